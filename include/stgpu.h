@@ -1,0 +1,218 @@
+/*
+ * stgpu.h -- C ABI of the B200 STRUCTURE sweep engine (libstgpu.so).
+ *
+ * Drop-in boundary for the per-sweep MCMC hot path of STRUCTURE 2.3.4 as
+ * shipped by pmelsted/structure.  In the reference each update is a pair of C
+ * functions, a CPU twin and an OpenCL twin taking a leading CLDict*
+ * (src/Updates/*.h); the device state lives in OpenCL buffers created by
+ * src/Kernels.c:576-635 and is the source of truth between host reads.  This
+ * header replaces that pair with one entry point per update on an opaque
+ * chain handle whose state lives in HBM.
+ *
+ * Conventions
+ *   - Every function returns an int status: ST_OK (0) or a negative ST_ERR_*.
+ *     Nothing calls exit() (the reference's handleCLErr exits,
+ *     src/Kernels.c:195-204).  st_last_error() gives the message.
+ *   - Buffers passed in are caller-owned host memory; the library copies.
+ *   - A context belongs to one host thread; chains of one context may be
+ *     driven from that thread only.  There are no process globals (the
+ *     reference keeps its model constants in globals, src/structure.h:70-121).
+ *   - Genotypes use the reference's layout Geno[ind][line][loc]
+ *     (src/structure.h:23 GenPos), alleles recoded to 0..k-1 and missing = -9
+ *     as produced by CountAlleles (src/datain.c:824-904).
+ */
+#ifndef STGPU_H
+#define STGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define STGPU_VERSION 10000
+
+enum st_status {
+    ST_OK = 0,
+    ST_ERR_ARG = -1,          /* invalid argument or size */
+    ST_ERR_CUDA = -2,         /* CUDA runtime error */
+    ST_ERR_NOMEM = -3,        /* allocation failed */
+    ST_ERR_ADMISSION = -4,    /* would exceed the context's HBM budget */
+    ST_ERR_STATE = -5,        /* operation not valid in the current state */
+    ST_ERR_DEVICE = -6,       /* a kernel raised a bit in the device error word */
+    ST_ERR_UNSUPPORTED = -7,  /* model option outside the implemented path */
+    ST_ERR_NODEVICE = -8      /* no CUDA device / library built without one */
+};
+
+enum st_layout {
+    ST_LAYOUT_AUTO = 0,       /* B2G when the data allow it, else U8 */
+    ST_LAYOUT_U8 = 1,         /* one byte per allele copy, any allele count */
+    ST_LAYOUT_B2G = 2         /* biallelic, 2 bits per genotype, locus-major */
+};
+
+/* Device error word bits (st_get_state ST_F_ERR). */
+enum st_device_error {
+    ST_DERR_GAMMA_CAP = 0x1,
+    ST_DERR_NAN = 0x2,
+    ST_DERR_BOUNDS = 0x4,
+    ST_DERR_FALLTHROUGH = 0x8
+};
+
+typedef struct st_ctx st_ctx;
+typedef struct st_data st_data;
+typedef struct st_chain st_chain;
+typedef struct st_batch st_batch;
+
+/* ---- context -------------------------------------------------------------
+ * Replaces InitCLDict / ReleaseCLDict (src/Kernels.c:641-751, Kernels.h:4-5).
+ * hbm_budget = 0: free device memory at creation minus 2 GiB.              */
+int st_version(void);
+int st_ctx_create(int device, size_t hbm_budget, st_ctx **out);
+int st_ctx_destroy(st_ctx *ctx);
+const char *st_last_error(const st_ctx *ctx);
+int st_ctx_memory(const st_ctx *ctx, size_t *in_use, size_t *budget);
+
+/* ---- data ----------------------------------------------------------------
+ * Replaces the Geno/NumAlleles/popflags uploads of src/structure.c:427-483.
+ * Give either geno (reference layout, recoded) or packed (ST_LAYOUT_B2G
+ * words [num_loci][ceil(num_inds/16)], 2 bits per individual: 0 = 0/0,
+ * 1 = 0/1 (allele 0 on line 0), 2 = 1/1, 3 = missing).                      */
+typedef struct st_data_desc {
+    int32_t num_inds;          /* NUMINDS */
+    int32_t num_loci;          /* NUMLOCI */
+    int32_t lines;             /* LINES; must be 2 */
+    int32_t layout;            /* enum st_layout */
+    const int32_t *geno;       /* [num_inds][lines][num_loci] or NULL */
+    const uint32_t *packed;    /* B2G words or NULL */
+    const int32_t *num_alleles;/* [num_loci] NumAlleles */
+    const int32_t *popflags;   /* [num_inds] Individual[].PopFlag or NULL */
+} st_data_desc;
+
+int st_data_upload(st_ctx *ctx, const st_data_desc *desc, st_data **out);
+int st_data_destroy(st_data *data);
+int st_data_layout(const st_data *data);
+
+/* ---- model ---------------------------------------------------------------
+ * The mainparams/extraparams keys the hot path reads (src/structure.h:70-121,
+ * defaults of src/params.c:571-670 via st_model_defaults).                 */
+typedef struct st_model {
+    int32_t maxpops;           /* MAXPOPS (K), 1..32 */
+    int32_t burnin, numreps;   /* BURNIN, NUMREPS */
+    int32_t noadmix;           /* NOADMIX: must be 0 */
+    int32_t linkage;           /* LINKAGE: must be 0 */
+    int32_t usepopinfo;        /* USEPOPINFO: must be 0 */
+    int32_t locprior;          /* LOCPRIOR: must be 0 */
+    int32_t freqscorr;         /* FREQSCORR */
+    int32_t onefst;            /* ONEFST */
+    int32_t inferalpha;        /* INFERALPHA */
+    int32_t popalphas;         /* POPALPHAS */
+    int32_t inferlambda;       /* INFERLAMBDA: must be 0 */
+    int32_t popspecificlambda; /* POPSPECIFICLAMBDA */
+    int32_t unifprioralpha;    /* UNIFPRIORALPHA */
+    int32_t computeprob;       /* COMPUTEPROB */
+    int32_t pfrompopflagonly;  /* PFROMPOPFLAGONLY */
+    int32_t ancestdist;        /* ANCESTDIST */
+    int32_t numboxes;          /* NUMBOXES */
+    int32_t metrofreq;         /* METROFREQ */
+    int32_t recessivealleles;  /* RECESSIVEALLELES: must be 0 */
+    double alpha;              /* ALPHA (initial) */
+    double alphamax;           /* ALPHAMAX */
+    double alphapropsd;        /* ALPHAPROPSD */
+    double alphapriora;        /* ALPHAPRIORA */
+    double alphapriorb;        /* ALPHAPRIORB */
+    double lambda;             /* LAMBDA */
+    double fpriormean;         /* FPRIORMEAN */
+    double fpriorsd;           /* FPRIORSD */
+    int32_t store_z;           /* keep Z in HBM (needed for st_get_state ST_F_Z) */
+    int32_t precision;         /* 0: FP32 Z/P/Q arithmetic; 1: FP64 Z (U8 data) */
+    int32_t tile_t, tile_w, tile_r; /* Z-pass tile (0 = choose); see DESIGN */
+    int32_t reserved[8];
+} st_model;
+
+int st_model_defaults(st_model *m);
+
+/* ---- chain ---------------------------------------------------------------
+ * Creates device state and runs the reference's Initialization
+ * (src/Init.c:329-444): alpha = ALPHA, lambda = LAMBDA, random Z
+ * (InitializeZ, Init.c:125-169), epsilon/F (InitFreqPriors, Init.c:173-240),
+ * Q = 1/K (src/structure.c:51-58), zeroed sums.                              */
+int st_chain_create(st_ctx *ctx, st_data *data, const st_model *model,
+                    uint64_t seed, st_chain **out);
+int st_chain_destroy(st_chain *chain);
+
+/* ---- per-update entry points: one per reference CL twin -------------------
+ * Each reads the chain's current state and writes the updated state; random
+ * draws come from Philox4x32-10 counters (seed, sweep, update, index).
+ * The sweep index is ST_F_REP (st_set_state), advanced only by st_sweep.    */
+int st_update_p(st_chain *c);      /* UpdatePCL      src/Updates/UpdateP.c:202-273 */
+int st_update_q(st_chain *c);      /* UpdateQCL      src/Updates/UpdateQ.c:894-929 */
+int st_update_z(st_chain *c);      /* UpdateZCL      src/Updates/UpdateZ.c:60-93   */
+int st_update_alpha(st_chain *c);  /* UpdateAlphaCL  src/Updates/UpdateAlpha.c:307-393 */
+int st_update_eps(st_chain *c);    /* UpdateEpsilonCL src/Updates/UpdateEpsilon.c:270-292 */
+int st_update_fst(st_chain *c);    /* UpdateFstCL    src/Updates/UpdateFst.c:100-140 */
+int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183         */
+/* UpdateZ (src/Updates/UpdateZ.c:13-56) fed an explicit uniform array laid out
+ * like the reference's randomArr: slot ind*L*2 + loc*2 + (draws so far at
+ * that locus).  precision 64 reproduces the reference's FP64 arithmetic.
+ * Needs U8 data.                                                             */
+int st_update_z_injected(st_chain *c, const double *uniforms, size_t n, int precision);
+
+/* ---- sweeps ----------------------------------------------------------------
+ * st_sweep: n sweeps in the order of src/structure.c:497-685 (P, Q, Z, alpha,
+ * eps, F, DataCollection after burn-in), fused into 3-5 launches per sweep.
+ * st_run: from the current sweep to BURNIN+NUMREPS.                          */
+int st_sweep(st_chain *c, int nsweeps);
+int st_run(st_chain *c);
+int st_sync(st_chain *c);          /* wait; ST_ERR_DEVICE if the error word is set */
+
+/* Many chains (any mix of data sets, N, L; same METROFREQ) advanced by one
+ * launch per update step.                                                    */
+int st_batch_create(st_ctx *ctx, st_chain **chains, int nchains, st_batch **out);
+int st_batch_sweep(st_batch *b, int nsweeps);
+int st_batch_destroy(st_batch *b);
+
+/* ---- state ---------------------------------------------------------------- */
+enum st_field {
+    ST_F_Q = 1,        /* float [N][K] */
+    ST_F_LOGQ,         /* float [N][K] */
+    ST_F_TESTQ,        /* float [N][K] Metropolis proposal */
+    ST_F_LOGTESTQ,     /* float [N][K] */
+    ST_F_P,            /* float [L][K][A] */
+    ST_F_LOGP,         /* float [L][K][A] */
+    ST_F_EPS,          /* double [L][A] */
+    ST_F_F,            /* double [K] */
+    ST_F_ALPHA,        /* double [K] */
+    ST_F_LAMBDA,       /* double [K] */
+    ST_F_Z,            /* uint8 [N][2][L], 0xFF = missing (needs store_z) */
+    ST_F_N,            /* int32 [L][K][A] allele counts from the last Z pass (get) */
+    ST_F_M,            /* int32 [N][K] ancestry counts from the last Z pass (get) */
+    ST_F_LOGDIFF,      /* double [N] last Metropolis log ratio (get) */
+    ST_F_QSUM,         /* double [N][K] */
+    ST_F_PSUM,         /* double [L][K][A] */
+    ST_F_SUMEPS,       /* double [L][A] */
+    ST_F_FSTSUM,       /* double [K] */
+    ST_F_SUMALPHA,     /* double [K] */
+    ST_F_SUMLAMBDA,    /* double [K] */
+    ST_F_ANCESTDIST,   /* int32 [N][K][NUMBOXES] */
+    ST_F_STATS,        /* double [256]: like, sumlikes, sumsqlikes, ... */
+    ST_F_REP,          /* int32: sweep counter */
+    ST_F_ERR,          /* int32: device error word */
+    ST_F_DIMS          /* int32 [8]: N, L, K, A, layout, G, nchunks, ngroups */
+};
+int st_get_state(st_chain *c, int field, void *host, size_t bytes);
+int st_set_state(st_chain *c, int field, const void *host, size_t bytes);
+size_t st_field_bytes(st_chain *c, int field);
+
+/* Per-chain timing of the last st_sweep / st_batch_sweep call (ms). */
+int st_get_timing(st_chain *c, double *ms_total);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

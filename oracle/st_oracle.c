@@ -1,0 +1,638 @@
+/*
+ * st_oracle.c -- CPU restatement of the STRUCTURE per-sweep hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product): loaded by tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg.  Built with
+ * -ffp-contract=off so that every a*b+c is two roundings unless written as
+ * fma()/fmaf(), exactly like the device code built with -fmad=false.
+ *
+ * Reference = pmelsted/structure (STRUCTURE 2.3.4 CPU code under src/).
+ * Random draws come from Philox4x32-10 counters (the device convention):
+ *   key = chain seed, ctr = {index, sub-index, sweep, stream << 24}.
+ */
+#include "st_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LOG_UNDERFLO_D   (-230.25850929940458)   /* log(1e-100): ran.c:1262 patch */
+#define SQRT_UNDERFLO    1e-50                   /* sqrt(UNDERFLO), CalcLike.c:107 */
+#define TWO_PI           6.283185307179586
+#define GAMMA_MAX_BLOCKS 64
+#define ERR_GAMMA_CAP    0x8
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10                                                            */
+/* ------------------------------------------------------------------------ */
+void orc_philox(const uint32_t ctr[4], uint64_t key, uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c1 = (uint32_t)p1;
+        c3 = (uint32_t)p0;
+        c0 = n0;
+        c2 = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static void philox4(uint32_t a, uint32_t b, uint32_t rep, uint32_t stream,
+                    uint64_t key, uint32_t out[4])
+{
+    uint32_t c[4] = {a, b, rep, stream << 24};
+    orc_philox(c, key, out);
+}
+
+double orc_u01(uint32_t hi, uint32_t lo)
+{
+    uint64_t x = ((uint64_t)(hi >> 6) << 26) | (uint64_t)(lo >> 6);   /* 52 bits */
+    return ((double)x + 0.5) * (1.0 / 4503599627370496.0);
+}
+
+/* ran.c:128-161: RandomReal/rnd on rand() in [0, 2^31); rnd() redraws on 0. */
+double orc_rnd31_block(const uint32_t w[4])
+{
+    for (int j = 0; j < 4; j++) {
+        uint32_t v = w[j] >> 1;
+        if (v != 0) return (double)v / 2147483648.0;
+    }
+    return 1.0 / 4294967296.0;
+}
+
+double orc_normal(uint32_t idx, uint32_t rep, uint32_t stream, uint64_t key)
+{
+    uint32_t w[4];
+    philox4(idx, 0, rep, stream, key, w);
+    double u1 = orc_u01(w[0], w[1]);
+    double u2 = orc_u01(w[2], w[3]);
+    return sqrt(-2.0 * log(u1)) * cos(TWO_PI * u2);
+}
+
+/* ------------------------------------------------------------------------ */
+/* ln Gamma: Lanczos (1964) g=7, n=9 series with the coefficient set used    */
+/* by mymath.c:382-429 (A. Miller 1988); same summation order.               */
+/* ------------------------------------------------------------------------ */
+double orc_lgamma(double z)
+{
+    static const double c[9] = {
+        0.9999999999995183, 676.5203681218835, -1259.139216722289,
+        771.3234287757674, -176.6150291498386, 12.50734324009056,
+        -0.1385710331296526, 9.934937113930748e-6, 1.659470187408462e-7};
+    double s = 0.0;
+    double t = z + 7.0;
+    for (int j = 8; j >= 1; j--) {
+        s += c[j] / t;
+        t -= 1.0;
+    }
+    s += c[0];
+    return log(s) + 0.9189385332046727 - (z + 6.5) + (z - 0.5) * log(z + 6.5);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Marsaglia & Tsang (2000) gamma, returned as log(draw).                    */
+/* Attempts come in pairs: block 2j gives two Box-Muller normals, block      */
+/* 2j+1 the two acceptance uniforms.  Shape < 1 uses G(a) = G(a+1) U^(1/a)   */
+/* with U from block 0xFFFFFFFF.                                             */
+/* ------------------------------------------------------------------------ */
+double orc_loggamma(double a, uint32_t e, uint32_t rep, uint32_t stream,
+                    uint64_t key, int *err)
+{
+    double aa = a < 1.0 ? a + 1.0 : a;
+    double d = aa - 1.0 / 3.0;
+    double c = 1.0 / sqrt(9.0 * d);
+    double lg = 0.0;
+    int done = 0;
+    for (uint32_t j = 0; j < GAMMA_MAX_BLOCKS && !done; j += 2) {
+        uint32_t b0[4], b1[4];
+        philox4(e, j, rep, stream, key, b0);
+        philox4(e, j + 1, rep, stream, key, b1);
+        double u1 = orc_u01(b0[0], b0[1]);
+        double u2 = orc_u01(b0[2], b0[3]);
+        double rad = sqrt(-2.0 * log(u1));
+        double ang = TWO_PI * u2;
+        double xs[2] = {rad * cos(ang), rad * sin(ang)};
+        double vs[2] = {orc_u01(b1[0], b1[1]), orc_u01(b1[2], b1[3])};
+        for (int h = 0; h < 2; h++) {
+            double x = xs[h];
+            double t = 1.0 + c * x;
+            if (t <= 0.0) continue;
+            double v = t * t * t;
+            double x2 = x * x;
+            double u = vs[h];
+            if (u < 1.0 - 0.0331 * x2 * x2 ||
+                log(u) < 0.5 * x2 + d * (1.0 - v + log(v))) {
+                lg = log(d * v);
+                done = 1;
+                break;
+            }
+        }
+    }
+    if (!done) {
+        if (err) *err |= ERR_GAMMA_CAP;
+        lg = log(d);
+    }
+    if (a < 1.0) {
+        uint32_t w[4];
+        philox4(e, 0xFFFFFFFFu, rep, stream, key, w);
+        lg += log(orc_u01(w[0], w[1])) / a;
+    }
+    return lg;
+}
+
+/* Pairwise tree over G (power of two) slots, the order of a xor-butterfly. */
+static double tree_sum(double *v, int G)
+{
+    for (int off = 1; off < G; off <<= 1)
+        for (int j = 0; j < G; j += 2 * off) v[j] = v[j] + v[j + off];
+    return v[0];
+}
+
+static int pow2_at_least(int k)
+{
+    int g = 1;
+    while (g < k) g <<= 1;
+    return g;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Z                                                                        */
+/* ------------------------------------------------------------------------ */
+/* Init.c:125-169 InitializeZ: RandomInteger(0,K-1) = (int)(d*K), d = rand()/2^31 */
+void orc_init_z(int N, int L, int K, const int32_t *geno, uint64_t key, int32_t *Z)
+{
+    for (int i = 0; i < N; i++)
+        for (int l = 0; l < L; l++) {
+            uint32_t w[4];
+            philox4((uint32_t)l, (uint32_t)(i >> 1), 0, ORC_S_INITZ, key, w);
+            for (int line = 0; line < 2; line++) {
+                size_t pos = ((size_t)i * 2 + line) * L + l;
+                if (geno[pos] < 0) {
+                    Z[pos] = ORC_UNASSIGNED;
+                } else {
+                    uint64_t v = w[2 * (i & 1) + line] >> 1;
+                    Z[pos] = (int32_t)((v * (uint64_t)K) >> 31);
+                }
+            }
+        }
+}
+
+/* Updates/UpdateZ.c:13-56 + mymath.c:105-129 in FP32: cumsum by fmaf,
+ * r = u*sum, z = first k with r <= cumsum_k  (= #{k<K-1 : cumsum_k < r}). */
+void orc_zupdate_f32(int N, int L, int K, int A, const int32_t *geno,
+                     const float *Q, const float *P, uint64_t key, uint32_t rep,
+                     int32_t *Z)
+{
+    float C[64];
+    for (int i = 0; i < N; i++) {
+        const float *q = Q + (size_t)i * K;
+        for (int l = 0; l < L; l++) {
+            uint32_t w[4];
+            philox4((uint32_t)l, (uint32_t)(i >> 1), rep, ORC_S_Z, key, w);
+            for (int line = 0; line < 2; line++) {
+                size_t pos = ((size_t)i * 2 + line) * L + l;
+                int a = geno[pos];
+                if (a < 0) { Z[pos] = ORC_UNASSIGNED; continue; }
+                const float *p = P + (size_t)l * K * A + a;
+                C[0] = q[0] * p[0];
+                for (int k = 1; k < K; k++) C[k] = fmaf(q[k], p[(size_t)k * A], C[k - 1]);
+                float u = (float)(w[2 * (i & 1) + line] >> 8) * (1.0f / 16777216.0f);
+                float r = u * C[K - 1];
+                int z = 0;
+                for (int k = 0; k < K - 1; k++) z += (C[k] < r);
+                Z[pos] = z;
+            }
+        }
+    }
+}
+
+/* The reference's UpdateZ arithmetic verbatim in FP64 (no contraction),
+ * reading uniforms from randomArr at slot i*L*2 + l*2 + (#draws so far).
+ * flags bit 0: a fall-through (option == K) was clamped to K-1. */
+void orc_zupdate_f64_injected(int N, int L, int K, int A, const int32_t *geno,
+                              const double *Q, const double *P,
+                              const double *randomArr, int32_t *Z, int32_t *flags)
+{
+    double W[64];
+    *flags = 0;
+    for (int i = 0; i < N; i++)
+        for (int l = 0; l < L; l++) {
+            int taken = 0;
+            for (int line = 0; line < 2; line++) {
+                size_t pos = ((size_t)i * 2 + line) * L + l;
+                int a = geno[pos];
+                if (a < 0) { Z[pos] = ORC_UNASSIGNED; continue; }
+                double sum = 0.0;
+                for (int k = 0; k < K; k++) {
+                    W[k] = Q[(size_t)i * K + k] * P[((size_t)l * K + k) * A + a];
+                    sum += W[k];
+                }
+                double u = randomArr[(size_t)i * L * 2 + (size_t)l * 2 + taken++];
+                double r = 0.0 + u * (sum - 0.0);
+                double so = 0.0;
+                int k;
+                for (k = 0; k < K; k++) {
+                    so += W[k];
+                    if (r <= so) break;
+                }
+                if (k == K) { k = K - 1; *flags |= 1; }
+                Z[pos] = k;
+            }
+        }
+}
+
+/* Updates/UpdateP.c:60-99 GetNumFromPops and Updates/UpdateQ.c:17-35 GetNumLociPop */
+void orc_counts(int N, int L, int K, int A, const int32_t *geno, const int32_t *Z,
+                int pfrompopflagonly, const int32_t *popflags,
+                int32_t *n, int32_t *m)
+{
+    memset(n, 0, sizeof(int32_t) * (size_t)L * K * A);
+    memset(m, 0, sizeof(int32_t) * (size_t)N * K);
+    for (int i = 0; i < N; i++)
+        for (int line = 0; line < 2; line++)
+            for (int l = 0; l < L; l++) {
+                size_t pos = ((size_t)i * 2 + line) * L + l;
+                int z = Z[pos], a = geno[pos];
+                if (z == ORC_UNASSIGNED) continue;
+                m[(size_t)i * K + z]++;
+                if (a >= 0 && (!pfrompopflagonly || popflags[i] == 1))
+                    n[((size_t)l * K + z) * A + a]++;
+            }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dirichlet from log-gamma draws (ran.c:1248-1272 incl. the 1e-100 patch)   */
+/* ------------------------------------------------------------------------ */
+static void dirichlet_seq(const double *lg, int n, int patch, float *P, float *logP)
+{
+    double M = lg[0];
+    for (int a = 1; a < n; a++) if (lg[a] > M) M = lg[a];
+    double S = 0.0;
+    for (int a = 0; a < n; a++) S += exp(lg[a] - M);
+    double ls = M + log(S);
+    if (patch && ls < LOG_UNDERFLO_D) {
+        for (int a = 0; a < n; a++) {
+            P[a] = (float)(1.0 / (double)n);
+            logP[a] = (float)(-log((double)n));
+        }
+        return;
+    }
+    for (int a = 0; a < n; a++) {
+        double lp = lg[a] - ls;
+        logP[a] = (float)lp;
+        P[a] = (float)exp(lp);
+    }
+}
+
+void orc_update_p(int L, int K, int A, const int32_t *numalleles, const int32_t *n,
+                  int freqscorr, const double *eps, const double *F,
+                  const double *lambda, uint64_t key, uint32_t rep,
+                  float *P, float *logP, int *err)
+{
+    double lg[256];
+    for (int l = 0; l < L; l++) {
+        int na = numalleles[l];
+        for (int k = 0; k < K; k++) {
+            size_t base = ((size_t)l * K + k) * A;
+            for (int a = 0; a < na; a++) {
+                double shape;
+                if (freqscorr)
+                    shape = eps[(size_t)l * A + a] * (1.0 - F[k]) / F[k] + (double)n[base + a];
+                else
+                    shape = lambda[k] + (double)n[base + a];
+                lg[a] = orc_loggamma(shape, (uint32_t)(base + a), rep, ORC_S_P, key, err);
+            }
+            if (na > 0) dirichlet_seq(lg, na, 1, P + base, logP + base);
+        }
+    }
+}
+
+/* Dirichlet over K populations with a G-lane butterfly normalisation. */
+static void dirichlet_tree(const double *lg, int K, float *Q, float *logQ)
+{
+    double v[64];
+    int G = pow2_at_least(K);
+    double M = lg[0];
+    for (int k = 1; k < K; k++) if (lg[k] > M) M = lg[k];
+    for (int k = 0; k < G; k++) v[k] = k < K ? exp(lg[k] - M) : 0.0;
+    double ls = M + log(tree_sum(v, G));
+    for (int k = 0; k < K; k++) {
+        double lq = lg[k] - ls;
+        logQ[k] = (float)lq;
+        Q[k] = (float)exp(lq);
+    }
+}
+
+void orc_update_q_gibbs(int N, int K, const int32_t *m, const double *alpha,
+                        uint64_t key, uint32_t rep, float *Q, float *logQ, int *err)
+{
+    double lg[64];
+    for (int i = 0; i < N; i++) {
+        for (int k = 0; k < K; k++)
+            lg[k] = orc_loggamma(alpha[k] + (double)m[(size_t)i * K + k],
+                                 (uint32_t)(i * K + k), rep, ORC_S_QG, key, err);
+        dirichlet_tree(lg, K, Q + (size_t)i * K, logQ + (size_t)i * K);
+    }
+}
+
+void orc_metro_propose(int N, int K, const double *alpha, uint64_t key,
+                       uint32_t rep, float *TestQ, float *logTestQ, int *err)
+{
+    double lg[64];
+    for (int i = 0; i < N; i++) {
+        for (int k = 0; k < K; k++)
+            lg[k] = orc_loggamma(alpha[k], (uint32_t)(i * K + k), rep, ORC_S_QM, key, err);
+        dirichlet_tree(lg, K, TestQ + (size_t)i * K, logTestQ + (size_t)i * K);
+    }
+}
+
+/* CalcLike.c:281-345 CalcLikeIndDiff, FP64, same loop order. */
+void orc_metro_logdiff(int N, int L, int K, int A, const int32_t *geno,
+                       const float *Q, const float *TestQ, const float *P,
+                       double *logdiff)
+{
+    for (int i = 0; i < N; i++) {
+        double lp = 0.0, lm = 0.0;
+        for (int line = 0; line < 2; line++)
+            for (int l = 0; l < L; l++) {
+                int a = geno[((size_t)i * 2 + line) * L + l];
+                if (a < 0) continue;
+                double tp = 0.0, tm = 0.0;
+                for (int k = 0; k < K; k++) {
+                    double p = P[((size_t)l * K + k) * A + a];
+                    tp += (double)TestQ[(size_t)i * K + k] * p;
+                    tm += (double)Q[(size_t)i * K + k] * p;
+                }
+                lp += log(tp);
+                lm += log(tm);
+            }
+        logdiff[i] = lp - lm;
+    }
+}
+
+/* Updates/UpdateQ.c:278-289: accept if u < exp(logdiff). */
+int orc_metro_accept(int N, int K, const double *logdiff, uint64_t key,
+                     uint32_t rep, float *Q, float *logQ, const float *TestQ,
+                     const float *logTestQ, uint8_t *accepted)
+{
+    int hits = 0;
+    for (int i = 0; i < N; i++) {
+        uint32_t w[4];
+        philox4((uint32_t)i, 0, rep, ORC_S_QMA, key, w);
+        double u = orc_u01(w[0], w[1]);
+        int acc = u < exp(logdiff[i]);
+        if (accepted) accepted[i] = (uint8_t)acc;
+        if (acc) {
+            hits++;
+            for (int k = 0; k < K; k++) {
+                Q[(size_t)i * K + k] = TestQ[(size_t)i * K + k];
+                logQ[(size_t)i * K + k] = logTestQ[(size_t)i * K + k];
+            }
+        }
+    }
+    return hits;
+}
+
+/* ------------------------------------------------------------------------ */
+/* alpha                                                                    */
+/* ------------------------------------------------------------------------ */
+/* S_k = sum_i log Q_ik (LogProbQonepop, UpdateAlpha.c:84-116, unclamped);
+ * T = sum_ik log max(Q_ik, sqrt(UNDERFLO)) (LogProbQ, UpdateAlpha.c:144-186). */
+void orc_alpha_sums(int N, int K, const float *logQ, double *S, double *T)
+{
+    const double lclamp = log(SQRT_UNDERFLO);
+    *T = 0.0;
+    for (int k = 0; k < K; k++) S[k] = 0.0;
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < K; k++) {
+            double lq = (double)logQ[(size_t)i * K + k];
+            S[k] += lq;
+            *T += lq > lclamp ? lq : lclamp;
+        }
+}
+
+/* Updates/UpdateAlpha.c:189-253, including its carry of logprobdiff from one
+ * population to the next when UNIFPRIORALPHA=1 and POPALPHAS=1. */
+void orc_update_alpha(const orc_alpha_params *p, const double *S, double T,
+                      double *alpha, uint64_t key, uint32_t rep, double *lpd_out)
+{
+    int K = p->K;
+    int numalphas = p->popalphas ? K : 1;
+    double logprobdiff = 0.0;
+    for (int pop = 0; pop < numalphas; pop++) {
+        double newalpha = alpha[pop] + p->alphapropsd * orc_normal((uint32_t)pop, rep, ORC_S_ALPHA, key);
+        if ((newalpha > 0) && ((newalpha < p->alphamax) || (!(p->unifprioralpha)))) {
+            if (!(p->unifprioralpha))
+                logprobdiff = (p->alphapriora - 1) * log(newalpha / alpha[pop]) +
+                              (alpha[pop] - newalpha) / p->alphapriorb;
+            if (p->popalphas) {
+                double sumalphas = 0.0;
+                for (int i = 0; i < K; i++) sumalphas += alpha[i];
+                logprobdiff -= (alpha[pop] - 1.0) * S[pop] +
+                               (orc_lgamma(sumalphas) - orc_lgamma(alpha[pop])) * p->N;
+                sumalphas += newalpha - alpha[pop];
+                logprobdiff += (newalpha - 1.0) * S[pop] +
+                               (orc_lgamma(sumalphas) - orc_lgamma(newalpha)) * p->N;
+            } else {
+                logprobdiff += (newalpha - 1.0) * T +
+                               (orc_lgamma(K * newalpha) - K * orc_lgamma(newalpha)) * p->N;
+                logprobdiff -= (alpha[pop] - 1.0) * T +
+                               (orc_lgamma(K * alpha[pop]) - K * orc_lgamma(alpha[pop])) * p->N;
+            }
+            uint32_t w[4];
+            philox4((uint32_t)pop, 1, rep, ORC_S_ALPHA, key, w);
+            double unifrv = orc_rnd31_block(w);
+            if (lpd_out) lpd_out[pop] = logprobdiff;
+            if (unifrv < exp(logprobdiff)) {
+                alpha[pop] = newalpha;
+                if (!(p->popalphas))
+                    for (int q = 1; q < K; q++) alpha[q] = newalpha;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* epsilon: Updates/UpdateEpsilon.c:71-145 NonIndependenceUpdateEpsilon      */
+/* ------------------------------------------------------------------------ */
+void orc_update_eps(int L, int K, int A, const int32_t *numalleles,
+                    const float *logP, double *eps, const double *F,
+                    double lambda0, double invsqrtnuminds, uint64_t key,
+                    uint32_t rep, uint8_t *accepted)
+{
+    double t[64];
+    int G = pow2_at_least(K);
+    for (int l = 0; l < L; l++) {
+        int na = numalleles[l];
+        if (accepted) accepted[l] = 0;
+        if (na <= 1) continue;
+        uint32_t w[4];
+        philox4((uint32_t)l, 0, rep, ORC_S_EPS, key, w);
+        int a1 = (int)(((double)(w[0] >> 1) / 2147483648.0) * na);
+        int a2 = (int)(((double)(w[1] >> 1) / 2147483648.0) * (na - 1));
+        if (a2 >= a1) a2 += 1;
+        double difference = 0.0 + ((double)(w[2] >> 1) / 2147483648.0) * (invsqrtnuminds - 0.0);
+        double e1 = eps[(size_t)l * A + a1], e2 = eps[(size_t)l * A + a2];
+        if (!((e1 + difference < 1.0) && (e2 - difference > 0.0))) continue;
+        for (int k = 0; k < G; k++) {
+            if (k >= K) { t[k] = 0.0; continue; }
+            double frac = (1.0 - F[k]) / F[k];
+            double lp1 = (double)logP[((size_t)l * K + k) * A + a1];
+            double lp2 = (double)logP[((size_t)l * K + k) * A + a2];
+            double s = orc_lgamma(frac * e1);
+            s += orc_lgamma(frac * e2);
+            s -= orc_lgamma(frac * (e1 + difference));
+            s -= orc_lgamma(frac * (e2 - difference));
+            s += frac * difference * lp1;
+            s -= frac * difference * lp2;
+            t[k] = s;
+        }
+        double sum = tree_sum(t, G);
+        if (lambda0 != 1.0)
+            sum += log(pow((e1 + difference) * (e2 - difference) / e1 / e2, lambda0 - 1.0));
+        philox4((uint32_t)l, 1, rep, ORC_S_EPS, key, w);
+        if (orc_rnd31_block(w) < exp(sum)) {
+            eps[(size_t)l * A + a1] += difference;
+            eps[(size_t)l * A + a2] -= difference;
+            if (accepted) accepted[l] = 1;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* F: Updates/UpdateFst.c                                                    */
+/* ------------------------------------------------------------------------ */
+/* diff[j] = sum over loci/alleles of the FlikeFreqs(new)-FlikeFreqs(old)
+ * terms for proposal j (UpdateFst.c:22-51), without the L*lgamma(frac) part. */
+void orc_fst_diffs(int L, int K, int A, const int32_t *numalleles,
+                   const float *logP, const double *eps, const double *F,
+                   int onefst, double fpriorsd, uint64_t key, uint32_t rep,
+                   double *newf, double *diff)
+{
+    int numfst = onefst ? 1 : K;
+    for (int j = 0; j < numfst; j++) {
+        newf[j] = F[j] + fpriorsd * orc_normal((uint32_t)j, rep, ORC_S_FST, key);
+        diff[j] = 0.0;
+        if (!(newf[j] > 0.0 && newf[j] < 1.0)) continue;
+        double nfr = (1.0 - newf[j]) / newf[j];
+        double ofr = (1.0 - F[j]) / F[j];
+        int k0 = onefst ? 0 : j, k1 = onefst ? K : j + 1;
+        for (int k = k0; k < k1; k++)
+            for (int l = 0; l < L; l++)
+                for (int a = 0; a < numalleles[l]; a++) {
+                    double e = eps[(size_t)l * A + a];
+                    double lp = (double)logP[((size_t)l * K + k) * A + a];
+                    diff[j] += (nfr - ofr) * e * lp - (orc_lgamma(nfr * e) - orc_lgamma(ofr * e));
+                }
+    }
+}
+
+/* UpdateFst.c:142-204 with FPriorDiff (10-18). */
+void orc_update_fst(int K, int onefst, double fpriormean, double fpriorsd,
+                    int Leff, const double *diff, const double *newf,
+                    double *F, uint64_t key, uint32_t rep, double *lpd_out)
+{
+    int numfst = onefst ? 1 : K;
+    for (int j = 0; j < numfst; j++) {
+        double oldf = F[j], nf = newf[j];
+        if (!(nf > 0.0 && nf < 1.0)) continue;
+        double logprobdiff = (fpriormean * fpriormean / (fpriorsd * fpriorsd) - 1) * log(nf / oldf) +
+                             (oldf - nf) * fpriormean / (fpriorsd * fpriorsd);
+        double nfr = (1.0 - nf) / nf, ofr = (1.0 - oldf) / oldf;
+        int npops = onefst ? K : 1;
+        logprobdiff += (double)Leff * npops * (orc_lgamma(nfr) - orc_lgamma(ofr)) + diff[j];
+        if (lpd_out) lpd_out[j] = logprobdiff;
+        int accept = 0;
+        if (logprobdiff >= 0.0) {
+            accept = 1;
+        } else {
+            uint32_t w[4];
+            philox4((uint32_t)j, 1, rep, ORC_S_FST, key, w);
+            if (orc_rnd31_block(w) < exp(logprobdiff)) accept = 1;
+        }
+        if (accept) {
+            if (onefst) { for (int k = 0; k < K; k++) F[k] = nf; }
+            else F[j] = nf;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* CalcLike.c:75-133 CalcLikeInd / 387-426 CalcLike (non-recessive branch)   */
+/* ------------------------------------------------------------------------ */
+double orc_calc_like(int N, int L, int K, int A, const int32_t *geno,
+                     const double *Q, const double *P)
+{
+    double like = 0.0;
+    for (int i = 0; i < N; i++) {
+        double rt = 1.0, ll = 0.0;
+        for (int line = 0; line < 2; line++)
+            for (int l = 0; l < L; l++) {
+                int a = geno[((size_t)i * 2 + line) * L + l];
+                if (a < 0) continue;
+                double term = 0.0;
+                for (int k = 0; k < K; k++)
+                    term += Q[(size_t)i * K + k] * P[((size_t)l * K + k) * A + a];
+                rt *= term > SQRT_UNDERFLO ? term : SQRT_UNDERFLO;
+                if (rt < SQRT_UNDERFLO) {
+                    ll += log(rt);
+                    rt = 1.0;
+                }
+            }
+        ll += log(rt);
+        like += ll;
+    }
+    return like;
+}
+
+double orc_calc_like_f(int N, int L, int K, int A, const int32_t *geno,
+                       const float *Q, const float *P)
+{
+    size_t nq = (size_t)N * K, np = (size_t)L * K * A;
+    double *q = (double *)malloc(sizeof(double) * nq);
+    double *p = (double *)malloc(sizeof(double) * np);
+    for (size_t j = 0; j < nq; j++) q[j] = Q[j];
+    for (size_t j = 0; j < np; j++) p[j] = P[j];
+    double r = orc_calc_like(N, L, K, A, geno, q, p);
+    free(q);
+    free(p);
+    return r;
+}
+
+/* Init.c:173-240 InitFreqPriors */
+void orc_init_eps(int N, int L, int A, const int32_t *geno,
+                  const int32_t *numalleles, int freqscorr, double lambda,
+                  double fpriormean, int K, double *eps, double *F)
+{
+    int cnt[256];
+    for (int l = 0; l < L; l++) {
+        int na = numalleles[l], total = 0;
+        for (int a = 0; a < na; a++) cnt[a] = 0;
+        if (freqscorr) {
+            for (int i = 0; i < N; i++)
+                for (int line = 0; line < 2; line++) {
+                    int v = geno[((size_t)i * 2 + line) * L + l];
+                    if (v >= 0) { total++; if (v < na) cnt[v]++; }
+                }
+        }
+        for (int a = 0; a < na; a++)
+            eps[(size_t)l * A + a] = freqscorr
+                ? (((double)lambda + (double)cnt[a]) / ((double)na * (double)lambda + (double)total))
+                : lambda;
+    }
+    for (int k = 0; k < K; k++) F[k] = freqscorr ? fpriormean : 0.5;
+}
+
+/* output.c:458-467 EstLogProb with mymath.c:52-62 SampleVar */
+double orc_est_logprob(double sumlikes, double sumsqlikes, int reps)
+{
+    double mean = sumlikes / reps;
+    double var = reps == 1 ? 0.0 : (sumsqlikes - sumlikes * sumlikes / reps) / (reps - 1);
+    return mean - var / 2.0;
+}

@@ -1,0 +1,1054 @@
+// st_api.cu -- the C ABI (include/stgpu.h): contexts with HBM admission,
+// genotype upload and packing, chain state, the per-update entry points, the
+// fused sweep and the batched sweep.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <cuda_runtime.h>
+#include "../../include/stgpu.h"
+#include "st_kernels.h"
+
+using namespace st;
+
+struct st_ctx {
+  int device = 0;
+  size_t budget = 0, in_use = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+};
+
+struct st_data {
+  st_ctx* ctx = nullptr;
+  int N = 0, L = 0, A = 1, layout = kLayoutU8, wpr = 0, Leff = 0;
+  uint32_t* g2 = nullptr;
+  uint8_t* g8 = nullptr;
+  int32_t* numalleles = nullptr;
+  int32_t* popflags = nullptr;
+  std::vector<int32_t> na_h;
+  std::vector<int64_t> cnt_h;    // [L][A] allele copies observed
+  std::vector<int64_t> tot_h;    // [L] non-missing copies
+  size_t bytes = 0;
+  int chains = 0;
+};
+
+struct st_chain {
+  st_ctx* ctx = nullptr;
+  st_data* data = nullptr;
+  st_model model{};
+  ChainDev h{};
+  ChainDev* d_chain = nullptr;
+  int* d_prefix = nullptr;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  int host_rep = 0;
+  bool fast = false;
+  int KT = 0;
+  size_t zsmem = 0;
+  double* d_injected = nullptr;
+  size_t injected_n = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  bool timed = false;
+};
+
+struct st_batch {
+  st_ctx* ctx = nullptr;
+  std::vector<st_chain*> chains;
+  ChainDev* d_table = nullptr;
+  int* d_pz = nullptr;     // prefix: Z pass
+  int* d_pl = nullptr;     // prefix: locus kernel
+  int* d_pi = nullptr;     // prefix: individual kernel
+  int tz = 0, tl = 0, ti = 0;
+  size_t zsmem = 0;
+  int KT = 0, W = 8, G = 1;
+  bool fast = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+constexpr int kBlockLoc = 256;
+constexpr int kBlockInd = 256;
+constexpr int kBlockCol = 256;
+const int kFastK[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 20, 24, 32};
+
+int seterr(st_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+int cuda_check(st_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return ST_OK;
+  return seterr(ctx, ST_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+#define ST_CUDA(ctx, call)                                            \
+  do {                                                                \
+    int _r = cuda_check((ctx), (call), #call);                        \
+    if (_r != ST_OK) return _r;                                       \
+  } while (0)
+
+int ctx_alloc(st_ctx* ctx, size_t bytes, void** p, std::vector<void*>* track, size_t* acc) {
+  *p = nullptr;
+  if (bytes == 0) return ST_OK;
+  if (ctx->in_use + bytes > ctx->budget)
+    return seterr(ctx, ST_ERR_ADMISSION,
+                  "admission: %zu bytes requested, %zu of %zu in use", bytes, ctx->in_use,
+                  ctx->budget);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return seterr(ctx, ST_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->in_use += bytes;
+  if (track) track->push_back(*p);
+  if (acc) *acc += bytes;
+  return ST_OK;
+}
+
+int pow2_at_least(int k) {
+  int g = 1;
+  while (g < k) g <<= 1;
+  return g;
+}
+
+int fast_kt(int K) {
+  for (int k : kFastK)
+    if (k >= K) return k;
+  return 0;
+}
+
+LaunchSet single(st_chain* c, int ctas) {
+  LaunchSet ls;
+  ls.chains = c->d_chain;
+  ls.prefix = c->d_prefix;
+  ls.nchains = 1;
+  ls.total_ctas = ctas;
+  ls.stream = c->ctx->stream;
+  return ls;
+}
+
+int upload_chain(st_chain* c) {
+  return cuda_check(c->ctx, cudaMemcpyAsync(c->d_chain, &c->h, sizeof(ChainDev),
+                                            cudaMemcpyHostToDevice, c->ctx->stream),
+                    "upload chain");
+}
+
+int set_rep(st_chain* c, int rep) {
+  c->host_rep = rep;
+  return cuda_check(c->ctx, cudaMemcpyAsync(c->h.rep, &c->host_rep, sizeof(int),
+                                            cudaMemcpyHostToDevice, c->ctx->stream),
+                    "set rep");
+}
+
+// Z-pass tiling heuristic: W warps of 32 loci, T individuals per chunk (a
+// multiple of 16), R locus blocks per CTA so that about two waves of CTAs
+// cover the data.
+void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R) {
+  int w = m->tile_w > 0 ? m->tile_w : 8;
+  if (w > 8) w = 8;
+  int t = m->tile_t > 0 ? m->tile_t : 512;
+  t = (t + 15) & ~15;
+  int np = (N + 15) & ~15;
+  if (t > np) t = np;
+  while (t > 16 && zpass_b2g_smem(fast_kt(K), K, t, w, kZMetro) > 160 * 1024) t -= 16;
+  int r = m->tile_r;
+  if (r <= 0) {
+    long lblocks = (L + 32 * w - 1) / (32 * w);
+    long nch = (N + t - 1) / t;
+    long target = 148L * 8;
+    r = (int)std::max(1L, (lblocks * nch) / target);
+    if (r > 64) r = 64;
+  }
+  *T = t;
+  *W = w;
+  *R = r;
+}
+
+int zpass(st_chain* c, int mode, int flags) {
+  if (c->fast) {
+    LaunchSet ls = single(c, ctas_zpass_b2g(c->h));
+    return cuda_check(c->ctx, launch_zpass_b2g(ls, c->KT, c->h.tileW, mode, flags, c->zsmem),
+                      "zpass_b2g");
+  }
+  st_ctx* ctx = c->ctx;
+  if (mode == kZNormal || mode == kZInit || mode == kZRecount) {
+    ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, ctx->stream));
+    ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, ctx->stream));
+  }
+  if (mode == kZMetro)
+    ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * (size_t)c->h.N, ctx->stream));
+  if (c->model.precision == 1) flags |= kZfF64;
+  LaunchSet ls = single(c, ctas_zpass_u8(c->h, 256));
+  return cuda_check(ctx, launch_zpass_u8(ls, mode, flags), "zpass_u8");
+}
+
+int locus(st_chain* c, int stages) {
+  LaunchSet ls = single(c, ctas_locus(c->h, kBlockLoc));
+  return cuda_check(c->ctx, launch_locus(ls, c->h.G, stages, kBlockLoc), "locus");
+}
+
+int ind(st_chain* c, int mode, int stages) {
+  LaunchSet ls = single(c, ctas_ind(c->h, kBlockInd));
+  return cuda_check(c->ctx, launch_ind(ls, c->h.G, mode, stages, kBlockInd), "ind");
+}
+
+int check_model(st_ctx* ctx, const st_model* m) {
+  if (m->maxpops < 1 || m->maxpops > kMaxPops)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "MAXPOPS=%d outside 1..%d", m->maxpops, kMaxPops);
+  if (m->noadmix) return seterr(ctx, ST_ERR_UNSUPPORTED, "NOADMIX=1 is not on the GPU path");
+  if (m->linkage) return seterr(ctx, ST_ERR_UNSUPPORTED, "LINKAGE=1 is not on the GPU path");
+  if (m->usepopinfo) return seterr(ctx, ST_ERR_UNSUPPORTED, "USEPOPINFO=1 is not on the GPU path");
+  if (m->locprior) return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR=1 is not on the GPU path");
+  if (m->inferlambda) return seterr(ctx, ST_ERR_UNSUPPORTED, "INFERLAMBDA=1 is not on the GPU path");
+  if (m->recessivealleles)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "RECESSIVEALLELES=1 is not on the GPU path");
+  if (m->freqscorr && (m->fpriormean <= 0 || m->fpriorsd <= 0))
+    return seterr(ctx, ST_ERR_ARG, "FPRIORMEAN/FPRIORSD must be positive");
+  if (m->burnin < 0 || m->numreps < 0) return seterr(ctx, ST_ERR_ARG, "negative BURNIN/NUMREPS");
+  if (m->ancestdist && m->numboxes < 1) return seterr(ctx, ST_ERR_ARG, "NUMBOXES < 1");
+  if (m->precision != 0 && m->precision != 1) return seterr(ctx, ST_ERR_ARG, "precision must be 0 or 1");
+  return ST_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// context
+// ===========================================================================
+extern "C" int st_version(void) { return STGPU_VERSION; }
+
+extern "C" int st_ctx_create(int device, size_t hbm_budget, st_ctx** out) {
+  if (!out) return ST_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return ST_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= n) return ST_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return ST_ERR_CUDA;
+  st_ctx* ctx = new st_ctx();
+  ctx->device = device;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  const size_t reserve = (size_t)2 << 30;
+  ctx->budget = hbm_budget ? hbm_budget : (fr > reserve ? fr - reserve : fr / 2);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return ST_ERR_CUDA;
+  }
+  *out = ctx;
+  return ST_OK;
+}
+
+extern "C" int st_ctx_destroy(st_ctx* ctx) {
+  if (!ctx) return ST_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return ST_OK;
+}
+
+extern "C" const char* st_last_error(const st_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" int st_ctx_memory(const st_ctx* ctx, size_t* in_use, size_t* budget) {
+  if (!ctx) return ST_ERR_ARG;
+  if (in_use) *in_use = ctx->in_use;
+  if (budget) *budget = ctx->budget;
+  return ST_OK;
+}
+
+// ===========================================================================
+// data
+// ===========================================================================
+extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out) {
+  if (!ctx || !d || !out) return ST_ERR_ARG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  if (d->lines != 2) return seterr(ctx, ST_ERR_UNSUPPORTED, "LINES=%d: only diploid data", d->lines);
+  if (d->num_inds < 1 || d->num_loci < 1 || !d->num_alleles)
+    return seterr(ctx, ST_ERR_ARG, "empty data set or missing num_alleles");
+  if (!d->geno && !d->packed) return seterr(ctx, ST_ERR_ARG, "need geno or packed");
+  const int N = d->num_inds, L = d->num_loci;
+  st_data* s = new st_data();
+  s->ctx = ctx;
+  s->N = N;
+  s->L = L;
+  s->na_h.assign(d->num_alleles, d->num_alleles + L);
+  int A = 1;
+  for (int l = 0; l < L; l++) {
+    if (s->na_h[l] < 0 || s->na_h[l] > 254) {
+      delete s;
+      return seterr(ctx, ST_ERR_ARG, "num_alleles[%d]=%d out of range", l, d->num_alleles[l]);
+    }
+    A = std::max(A, s->na_h[l]);
+    if (s->na_h[l] > 0) s->Leff++;
+  }
+  if (A > kMaxAlleles) {
+    delete s;
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "%d alleles at a locus (limit %d)", A, kMaxAlleles);
+  }
+  s->A = A;
+  s->cnt_h.assign((size_t)L * A, 0);
+  s->tot_h.assign(L, 0);
+
+  // decide the layout and validate the genotypes
+  bool b2g_ok = A <= 2;
+  if (d->geno) {
+    for (int i = 0; i < N; i++)
+      for (int l = 0; l < L; l++) {
+        int a0 = d->geno[((size_t)i * 2) * L + l], a1 = d->geno[((size_t)i * 2 + 1) * L + l];
+        for (int a : {a0, a1}) {
+          if (a >= 0) {
+            if (a >= s->na_h[l]) {
+              delete s;
+              return seterr(ctx, ST_ERR_ARG, "allele %d >= num_alleles[%d]=%d", a, l, s->na_h[l]);
+            }
+            s->cnt_h[(size_t)l * A + a]++;
+            s->tot_h[l]++;
+          } else if (a != kUnassigned) {
+            delete s;
+            return seterr(ctx, ST_ERR_ARG, "genotype value %d: expected 0..k-1 or -9", a);
+          }
+        }
+        if ((a0 < 0) != (a1 < 0)) b2g_ok = false;
+        if (a0 >= 0 && a1 >= 0 && a0 > a1) b2g_ok = false;
+      }
+  } else {
+    if (A > 2) {
+      delete s;
+      return seterr(ctx, ST_ERR_ARG, "packed genotypes need <= 2 alleles per locus");
+    }
+    const int wpr = (N + 15) / 16;
+    for (int l = 0; l < L; l++)
+      for (int i = 0; i < N; i++) {
+        uint32_t g = (d->packed[(size_t)l * wpr + (i >> 4)] >> (2 * (i & 15))) & 3u;
+        if (g == 3u) continue;
+        s->tot_h[l] += 2;
+        s->cnt_h[(size_t)l * A + 0] += (g == 0) ? 2 : (g == 1 ? 1 : 0);
+        if (A > 1) s->cnt_h[(size_t)l * A + 1] += (g == 2) ? 2 : (g == 1 ? 1 : 0);
+      }
+  }
+  int layout = d->layout;
+  if (layout == ST_LAYOUT_AUTO) layout = b2g_ok ? ST_LAYOUT_B2G : ST_LAYOUT_U8;
+  if (layout == ST_LAYOUT_B2G && !b2g_ok) {
+    delete s;
+    return seterr(ctx, ST_ERR_ARG, "data not representable at 2 bits/genotype (multi-allelic, "
+                  "half-missing or non-canonical heterozygote)");
+  }
+  if (layout == ST_LAYOUT_U8 && !d->geno) {
+    delete s;
+    return seterr(ctx, ST_ERR_ARG, "U8 layout needs geno");
+  }
+  s->layout = layout == ST_LAYOUT_B2G ? kLayoutB2G : kLayoutU8;
+
+  int rc;
+  void* p;
+  rc = ctx_alloc(ctx, sizeof(int32_t) * L, &p, nullptr, &s->bytes);
+  if (rc) { delete s; return rc; }
+  s->numalleles = (int32_t*)p;
+  rc = ctx_alloc(ctx, sizeof(int32_t) * N, &p, nullptr, &s->bytes);
+  if (rc) { cudaFree(s->numalleles); delete s; return rc; }
+  s->popflags = (int32_t*)p;
+  cudaMemcpy(s->numalleles, s->na_h.data(), sizeof(int32_t) * L, cudaMemcpyHostToDevice);
+  std::vector<int32_t> pf(N, 0);
+  if (d->popflags) pf.assign(d->popflags, d->popflags + N);
+  cudaMemcpy(s->popflags, pf.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice);
+
+  if (s->layout == kLayoutB2G) {
+    const int wpr = (N + 15) / 16;
+    s->wpr = wpr;
+    std::vector<uint32_t> words;
+    const uint32_t* src = d->packed;
+    if (!src) {
+      words.assign((size_t)L * wpr, 0xFFFFFFFFu);
+      for (int l = 0; l < L; l++)
+        for (int i = 0; i < N; i++) {
+          int a0 = d->geno[((size_t)i * 2) * L + l], a1 = d->geno[((size_t)i * 2 + 1) * L + l];
+          uint32_t g = (a0 < 0) ? 3u : (uint32_t)(a0 + a1);
+          uint32_t& w = words[(size_t)l * wpr + (i >> 4)];
+          w &= ~(3u << (2 * (i & 15)));
+          w |= g << (2 * (i & 15));
+        }
+      src = words.data();
+    }
+    rc = ctx_alloc(ctx, sizeof(uint32_t) * (size_t)L * wpr, &p, nullptr, &s->bytes);
+    if (rc) { st_data_destroy(s); return rc; }
+    s->g2 = (uint32_t*)p;
+    rc = cuda_check(ctx, cudaMemcpy(s->g2, src, sizeof(uint32_t) * (size_t)L * wpr,
+                                    cudaMemcpyHostToDevice), "upload packed");
+    if (rc) { st_data_destroy(s); return rc; }
+  } else {
+    const size_t n = (size_t)N * 2 * L;
+    rc = ctx_alloc(ctx, n, &p, nullptr, &s->bytes);
+    if (rc) { st_data_destroy(s); return rc; }
+    s->g8 = (uint8_t*)p;
+    // stage the int32 genotypes through a temporary device buffer in slices
+    const size_t slice = (size_t)1 << 26;
+    int32_t* tmp = nullptr;
+    rc = cuda_check(ctx, cudaMalloc(&tmp, sizeof(int32_t) * std::min(n, slice)), "staging");
+    if (rc) { st_data_destroy(s); return rc; }
+    for (size_t off = 0; off < n; off += slice) {
+      size_t m = std::min(slice, n - off);
+      cudaMemcpy(tmp, d->geno + off, sizeof(int32_t) * m, cudaMemcpyHostToDevice);
+      launch_pack_u8(tmp, s->g8 + off, m, 0);
+    }
+    cudaDeviceSynchronize();
+    cudaFree(tmp);
+    rc = cuda_check(ctx, cudaGetLastError(), "pack genotypes");
+    if (rc) { st_data_destroy(s); return rc; }
+  }
+  *out = s;
+  return ST_OK;
+}
+
+extern "C" int st_data_destroy(st_data* s) {
+  if (!s) return ST_ERR_ARG;
+  if (s->chains > 0) return seterr(s->ctx, ST_ERR_STATE, "data still used by %d chains", s->chains);
+  cudaSetDevice(s->ctx->device);
+  for (void* p : {(void*)s->g2, (void*)s->g8, (void*)s->numalleles, (void*)s->popflags})
+    if (p) cudaFree(p);
+  s->ctx->in_use -= s->bytes;
+  delete s;
+  return ST_OK;
+}
+
+extern "C" int st_data_layout(const st_data* s) {
+  if (!s) return ST_ERR_ARG;
+  return s->layout == kLayoutB2G ? ST_LAYOUT_B2G : ST_LAYOUT_U8;
+}
+
+// ===========================================================================
+// model / chain
+// ===========================================================================
+extern "C" int st_model_defaults(st_model* m) {
+  if (!m) return ST_ERR_ARG;
+  memset(m, 0, sizeof(*m));
+  // src/params.c:571-670 PresetValues
+  m->maxpops = 2;
+  m->burnin = 10000;
+  m->numreps = 20000;
+  m->freqscorr = 1;
+  m->onefst = 0;
+  m->inferalpha = 1;
+  m->popalphas = 0;
+  m->inferlambda = 0;
+  m->unifprioralpha = 1;
+  m->computeprob = 1;
+  m->pfrompopflagonly = 0;
+  m->ancestdist = 0;
+  m->numboxes = 1000;
+  m->metrofreq = 20;
+  m->alpha = 1.0;
+  m->alphamax = 10.0;
+  m->alphapropsd = 0.05;
+  m->alphapriora = 1.0;
+  m->alphapriorb = 2.0;
+  m->lambda = 1.0;
+  m->fpriormean = 0.1;
+  m->fpriorsd = 0.1;
+  return ST_OK;
+}
+
+extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model, uint64_t seed,
+                               st_chain** out) {
+  if (!ctx || !data || !model || !out) return ST_ERR_ARG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  int rc = check_model(ctx, model);
+  if (rc) return rc;
+  const int N = data->N, L = data->L, K = model->maxpops, A = data->A;
+  st_chain* c = new st_chain();
+  c->ctx = ctx;
+  c->data = data;
+  c->model = *model;
+  ChainDev& h = c->h;
+  h.N = N; h.L = L; h.K = K; h.A = A; h.G = pow2_at_least(K);
+  h.layout = data->layout; h.wpr = data->wpr; h.Leff = data->Leff;
+  h.freqscorr = model->freqscorr; h.onefst = model->onefst; h.inferalpha = model->inferalpha;
+  h.popalphas = model->popalphas; h.unifprioralpha = model->unifprioralpha;
+  h.computeprob = model->computeprob; h.pfrompopflagonly = model->pfrompopflagonly;
+  h.ancestdist = model->ancestdist; h.numboxes = model->numboxes > 0 ? model->numboxes : 1;
+  h.metrofreq = model->metrofreq; h.burnin = model->burnin;
+  h.alphamax = model->alphamax; h.alphapropsd = model->alphapropsd;
+  h.alphapriora = model->alphapriora; h.alphapriorb = model->alphapriorb;
+  h.fpriormean = model->fpriormean; h.fpriorsd = model->fpriorsd;
+  h.invsqrtnuminds = pow((double)N, -0.5);    // src/Updates/UpdateEpsilon.c:80
+  h.key = seed;
+  h.g2 = data->g2; h.g8 = data->g8; h.numalleles = data->numalleles; h.popflags = data->popflags;
+
+  c->fast = data->layout == kLayoutB2G && model->precision == 0 && fast_kt(K) > 0;
+  if (data->layout == kLayoutB2G && !c->fast) {
+    delete c;
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "FP64 Z arithmetic needs U8 data (ST_LAYOUT_U8)");
+  }
+  if (c->fast) {
+    c->KT = fast_kt(K);
+    int T, W, R;
+    choose_tile(model, N, L, K, &T, &W, &R);
+    h.tileT = T; h.tileW = W; h.tileR = R;
+    h.nchunks = (N + T - 1) / T;
+    const int lblocks = (L + 32 * W - 1) / (32 * W);
+    h.ngroups = (lblocks + R - 1) / R;
+    c->zsmem = 0;
+    for (int mode : {kZNormal, kZMetro, kZInit, kZRecount, kZLike})
+      c->zsmem = std::max(c->zsmem, zpass_b2g_smem(c->KT, K, T, W, mode));
+  } else {
+    h.tileT = N; h.tileW = 8; h.tileR = 1;
+    h.nchunks = 1;
+    h.ngroups = 1;
+  }
+  h.cnt_chunks = h.nchunks;
+  h.cnt_groups = h.ngroups;
+
+  const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A, LA = (size_t)L * A;
+  const int zctas = c->fast ? ctas_zpass_b2g(h) : ctas_zpass_u8(h, 256);
+  ChainDev hw = h;
+  hw.G = 32;  // scratch sized for the widest group a batch may impose
+  const int nred = std::max(ctas_locus(hw, kBlockLoc) * K, ctas_ind(hw, kBlockInd) * (K + 1));
+  struct Buf { void** p; size_t bytes; };
+  void *Q, *logQ, *TQ, *lTQ, *P, *logP, *eps, *F, *alpha, *lambda, *Z = nullptr, *npart, *mpart,
+      *ldpart, *QSum, *PSum, *SumEps, *FstSum, *sumAlpha, *sumlambda, *AD = nullptr, *stats,
+      *likepart, *redpart, *ctr, *rep, *err, *chain, *prefix;
+  std::vector<Buf> bufs = {
+      {&Q, NK * 4}, {&logQ, NK * 4}, {&TQ, NK * 4}, {&lTQ, NK * 4}, {&P, LKA * 4},
+      {&logP, LKA * 4}, {&eps, LA * 8}, {&F, (size_t)K * 8}, {&alpha, (size_t)K * 8},
+      {&lambda, (size_t)K * 8}, {&npart, (size_t)h.nchunks * LKA * 4},
+      {&mpart, (size_t)h.ngroups * NK * 4}, {&ldpart, (size_t)h.ngroups * N * 8},
+      {&QSum, NK * 8}, {&PSum, LKA * 8}, {&SumEps, LA * 8}, {&FstSum, (size_t)K * 8},
+      {&sumAlpha, (size_t)K * 8}, {&sumlambda, (size_t)K * 8}, {&stats, (size_t)kStSize * 8},
+      {&likepart, (size_t)zctas * 8}, {&redpart, (size_t)nred * 8},
+      {&ctr, (size_t)kCtrCount * 4}, {&rep, 4}, {&err, 4}, {&chain, sizeof(ChainDev)},
+      {&prefix, 16}};
+  if (model->store_z) bufs.push_back({&Z, (size_t)N * 2 * L});
+  if (model->ancestdist) bufs.push_back({&AD, NK * (size_t)h.numboxes * 4});
+  for (auto& b : bufs) {
+    rc = ctx_alloc(ctx, b.bytes, b.p, &c->allocs, &c->bytes);
+    if (rc) { st_chain_destroy(c); return rc; }
+  }
+  h.Q = (float*)Q; h.logQ = (float*)logQ; h.TestQ = (float*)TQ; h.logTestQ = (float*)lTQ;
+  h.P = (float*)P; h.logP = (float*)logP; h.eps = (double*)eps; h.F = (double*)F;
+  h.alpha = (double*)alpha; h.lambda = (double*)lambda; h.Z = (uint8_t*)Z;
+  h.npart = (int32_t*)npart; h.mpart = (int32_t*)mpart; h.ldpart = (double*)ldpart;
+  h.QSum = (double*)QSum; h.PSum = (double*)PSum; h.SumEps = (double*)SumEps;
+  h.FstSum = (double*)FstSum; h.sumAlpha = (double*)sumAlpha; h.sumlambda = (double*)sumlambda;
+  h.AncestDist = (int32_t*)AD; h.stats = (double*)stats; h.likepart = (double*)likepart;
+  h.redpart = (double*)redpart; h.ctr = (unsigned*)ctr; h.rep = (int*)rep; h.err = (int*)err;
+  c->d_chain = (ChainDev*)chain;
+  c->d_prefix = (int*)prefix;
+  data->chains++;
+
+  // ---- Initialization (src/Init.c:329-444, src/structure.c:51-58) ---------
+  cudaStream_t s = ctx->stream;
+  std::vector<float> q(NK, (float)(1.0 / K)), lq(NK, (float)log(1.0 / K));
+  std::vector<double> kv(K);
+  std::vector<double> ev(LA, 0.0);
+  for (int l = 0; l < L; l++)
+    for (int a = 0; a < data->na_h[l]; a++) {
+      // src/Init.c:173-240 InitFreqPriors
+      ev[(size_t)l * A + a] = model->freqscorr
+          ? (((double)model->lambda + (double)data->cnt_h[(size_t)l * A + a]) /
+             ((double)data->na_h[l] * (double)model->lambda + (double)data->tot_h[l]))
+          : model->lambda;
+    }
+  cudaMemcpyAsync(h.Q, q.data(), NK * 4, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(h.logQ, lq.data(), NK * 4, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(h.eps, ev.data(), LA * 8, cudaMemcpyHostToDevice, s);
+  std::fill(kv.begin(), kv.end(), model->freqscorr ? model->fpriormean : 0.5);
+  cudaMemcpyAsync(h.F, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
+  std::fill(kv.begin(), kv.end(), model->alpha);
+  cudaMemcpyAsync(h.alpha, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
+  std::fill(kv.begin(), kv.end(), model->lambda);
+  cudaMemcpyAsync(h.lambda, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(h.P, 0, LKA * 4, s);
+  cudaMemsetAsync(h.logP, 0, LKA * 4, s);
+  cudaMemsetAsync(h.TestQ, 0, NK * 4, s);
+  cudaMemsetAsync(h.logTestQ, 0, NK * 4, s);
+  cudaMemsetAsync(h.QSum, 0, NK * 8, s);
+  cudaMemsetAsync(h.PSum, 0, LKA * 8, s);
+  cudaMemsetAsync(h.SumEps, 0, LA * 8, s);
+  cudaMemsetAsync(h.FstSum, 0, K * 8, s);
+  cudaMemsetAsync(h.sumAlpha, 0, K * 8, s);
+  cudaMemsetAsync(h.sumlambda, 0, K * 8, s);
+  cudaMemsetAsync(h.stats, 0, kStSize * 8, s);
+  cudaMemsetAsync(h.ctr, 0, kCtrCount * 4, s);
+  cudaMemsetAsync(h.rep, 0, 4, s);
+  cudaMemsetAsync(h.err, 0, 4, s);
+  cudaMemsetAsync(h.ldpart, 0, (size_t)h.ngroups * N * 8, s);
+  if (h.AncestDist) cudaMemsetAsync(h.AncestDist, 0, NK * (size_t)h.numboxes * 4, s);
+  int zero = 0;
+  cudaMemcpyAsync(c->d_prefix, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+  rc = upload_chain(c);
+  if (!rc) rc = zpass(c, kZInit, model->store_z ? kZfStoreZ : 0);
+  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "chain init");
+  if (rc) { st_chain_destroy(c); return rc; }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  *out = c;
+  return ST_OK;
+}
+
+extern "C" int st_chain_destroy(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  cudaStreamSynchronize(c->ctx->stream);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->d_injected) { cudaFree(c->d_injected); c->ctx->in_use -= c->injected_n * 8; }
+  c->ctx->in_use -= c->bytes;
+  if (c->h.N) c->data->chains--;
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  delete c;
+  return ST_OK;
+}
+
+// ===========================================================================
+// per-update entry points
+// ===========================================================================
+extern "C" int st_update_p(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  return locus(c, kLocP);
+}
+
+extern "C" int st_update_eps(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.freqscorr) return seterr(c->ctx, ST_ERR_STATE, "UpdateEpsilon needs FREQSCORR=1");
+  cudaSetDevice(c->ctx->device);
+  return locus(c, kLocEps);
+}
+
+extern "C" int st_update_fst(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.freqscorr) return seterr(c->ctx, ST_ERR_STATE, "UpdateFst needs FREQSCORR=1");
+  cudaSetDevice(c->ctx->device);
+  return locus(c, kLocFst);
+}
+
+static int update_q_impl(st_chain* c, int stages) {
+  const int rep = c->host_rep;
+  if (c->h.metrofreq > 0 && rep % c->h.metrofreq == 0) {
+    int rc = ind(c, kIndPropose, 0);
+    if (!rc) rc = zpass(c, kZMetro, 0);
+    if (!rc) rc = ind(c, kIndAccept, stages);
+    return rc;
+  }
+  return ind(c, kIndGibbs, stages);
+}
+
+extern "C" int st_update_q(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  return update_q_impl(c, 0);
+}
+
+extern "C" int st_update_z(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  return zpass(c, kZNormal, c->model.store_z ? kZfStoreZ : 0);
+}
+
+extern "C" int st_update_alpha(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.inferalpha) return seterr(c->ctx, ST_ERR_STATE, "UpdateAlpha needs INFERALPHA=1");
+  cudaSetDevice(c->ctx->device);
+  return ind(c, kIndNone, kIndAlpha);
+}
+
+extern "C" int st_collect(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  int rc = ST_OK;
+  if (c->h.computeprob) rc = zpass(c, kZLike, kZfLikeAlways);
+  if (rc) return rc;
+  LaunchSet ls = single(c, ctas_collect(c->h, kBlockCol));
+  return cuda_check(c->ctx, launch_collect(ls, kBlockCol), "collect");
+}
+
+extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int precision) {
+  if (!c || !u) return ST_ERR_ARG;
+  if (c->fast || c->h.layout != kLayoutU8)
+    return seterr(c->ctx, ST_ERR_STATE, "injected uniforms need U8 data (ST_LAYOUT_U8)");
+  if (n != (size_t)c->h.N * c->h.L * 2)
+    return seterr(c->ctx, ST_ERR_ARG, "need N*L*2 = %zu uniforms", (size_t)c->h.N * c->h.L * 2);
+  if (precision != 32 && precision != 64) return seterr(c->ctx, ST_ERR_ARG, "precision 32 or 64");
+  cudaSetDevice(c->ctx->device);
+  if (c->injected_n != n) {
+    if (c->d_injected) { cudaFree(c->d_injected); c->ctx->in_use -= c->injected_n * 8; }
+    c->d_injected = nullptr;
+    c->injected_n = 0;
+    void* p;
+    int rc = ctx_alloc(c->ctx, n * 8, &p, nullptr, nullptr);
+    if (rc) return rc;
+    c->d_injected = (double*)p;
+    c->injected_n = n;
+  }
+  ST_CUDA(c->ctx, cudaMemcpyAsync(c->d_injected, u, n * 8, cudaMemcpyHostToDevice, c->ctx->stream));
+  c->h.injected = c->d_injected;
+  int rc = upload_chain(c);
+  if (rc) return rc;
+  const int saved = c->model.precision;
+  c->model.precision = 0;
+  int flags = kZfInjected | (c->model.store_z ? kZfStoreZ : 0) | (precision == 64 ? kZfF64 : 0);
+  rc = zpass(c, kZNormal, flags);
+  c->model.precision = saved;
+  return rc;
+}
+
+// ===========================================================================
+// sweeps
+// ===========================================================================
+static int sweep_once(st_chain* c) {
+  const int zflags = (c->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
+                     (c->model.store_z ? kZfStoreZ : 0);
+  int rc = locus(c, kLocP | kLocEps | kLocFst | kLocCollect);
+  if (!rc) rc = update_q_impl(c, kIndAlpha | kIndCollect);
+  if (!rc) rc = zpass(c, kZNormal, zflags);
+  if (!rc) c->host_rep++;
+  return rc;
+}
+
+extern "C" int st_sweep(st_chain* c, int nsweeps) {
+  if (!c || nsweeps < 0) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  cudaEventRecord(c->ev0, c->ctx->stream);
+  for (int s = 0; s < nsweeps; s++) {
+    int rc = sweep_once(c);
+    if (rc) return rc;
+  }
+  cudaEventRecord(c->ev1, c->ctx->stream);
+  c->timed = true;
+  return ST_OK;
+}
+
+extern "C" int st_run(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  int todo = c->model.burnin + c->model.numreps - c->host_rep;
+  if (todo <= 0) return ST_OK;
+  int rc = st_sweep(c, todo);
+  if (rc) return rc;
+  return st_sync(c);
+}
+
+extern "C" int st_sync(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  ST_CUDA(c->ctx, cudaStreamSynchronize(c->ctx->stream));
+  int e = 0;
+  ST_CUDA(c->ctx, cudaMemcpy(&e, c->h.err, 4, cudaMemcpyDeviceToHost));
+  if (c->timed) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->last_ms = ms;
+    cudaGetLastError();
+    c->timed = false;
+  }
+  if (e) return seterr(c->ctx, ST_ERR_DEVICE, "device error word 0x%x", e);
+  return ST_OK;
+}
+
+extern "C" int st_get_timing(st_chain* c, double* ms) {
+  if (!c || !ms) return ST_ERR_ARG;
+  *ms = c->last_ms;
+  return ST_OK;
+}
+
+// ===========================================================================
+// state
+// ===========================================================================
+extern "C" size_t st_field_bytes(st_chain* c, int f) {
+  if (!c) return 0;
+  const ChainDev& h = c->h;
+  const size_t NK = (size_t)h.N * h.K, LKA = (size_t)h.L * h.K * h.A, LA = (size_t)h.L * h.A;
+  switch (f) {
+    case ST_F_Q: case ST_F_LOGQ: case ST_F_TESTQ: case ST_F_LOGTESTQ: return NK * 4;
+    case ST_F_P: case ST_F_LOGP: return LKA * 4;
+    case ST_F_EPS: case ST_F_SUMEPS: return LA * 8;
+    case ST_F_F: case ST_F_ALPHA: case ST_F_LAMBDA: case ST_F_FSTSUM: case ST_F_SUMALPHA:
+    case ST_F_SUMLAMBDA: return (size_t)h.K * 8;
+    case ST_F_Z: return (size_t)h.N * 2 * h.L;
+    case ST_F_N: return LKA * 4;
+    case ST_F_M: return NK * 4;
+    case ST_F_LOGDIFF: return (size_t)h.N * 8;
+    case ST_F_QSUM: return NK * 8;
+    case ST_F_PSUM: return LKA * 8;
+    case ST_F_ANCESTDIST: return NK * (size_t)h.numboxes * 4;
+    case ST_F_STATS: return (size_t)kStSize * 8;
+    case ST_F_REP: case ST_F_ERR: return 4;
+    case ST_F_DIMS: return 32;
+  }
+  return 0;
+}
+
+static void* field_ptr(st_chain* c, int f) {
+  ChainDev& h = c->h;
+  switch (f) {
+    case ST_F_Q: return h.Q;
+    case ST_F_LOGQ: return h.logQ;
+    case ST_F_TESTQ: return h.TestQ;
+    case ST_F_LOGTESTQ: return h.logTestQ;
+    case ST_F_P: return h.P;
+    case ST_F_LOGP: return h.logP;
+    case ST_F_EPS: return h.eps;
+    case ST_F_F: return h.F;
+    case ST_F_ALPHA: return h.alpha;
+    case ST_F_LAMBDA: return h.lambda;
+    case ST_F_Z: return h.Z;
+    case ST_F_QSUM: return h.QSum;
+    case ST_F_PSUM: return h.PSum;
+    case ST_F_SUMEPS: return h.SumEps;
+    case ST_F_FSTSUM: return h.FstSum;
+    case ST_F_SUMALPHA: return h.sumAlpha;
+    case ST_F_SUMLAMBDA: return h.sumlambda;
+    case ST_F_ANCESTDIST: return h.AncestDist;
+    case ST_F_STATS: return h.stats;
+    case ST_F_ERR: return h.err;
+  }
+  return nullptr;
+}
+
+extern "C" int st_get_state(st_chain* c, int f, void* host, size_t bytes) {
+  if (!c || !host) return ST_ERR_ARG;
+  const size_t need = st_field_bytes(c, f);
+  if (need == 0 || bytes != need)
+    return seterr(c->ctx, ST_ERR_ARG, "field %d: %zu bytes given, %zu expected", f, bytes, need);
+  cudaSetDevice(c->ctx->device);
+  cudaStream_t s = c->ctx->stream;
+  ST_CUDA(c->ctx, cudaStreamSynchronize(s));
+  const ChainDev& h = c->h;
+  if (f == ST_F_REP) { memcpy(host, &c->host_rep, 4); return ST_OK; }
+  if (f == ST_F_DIMS) {
+    int32_t d[8] = {h.N, h.L, h.K, h.A, h.layout, h.G, h.nchunks, h.ngroups};
+    memcpy(host, d, 32);
+    return ST_OK;
+  }
+  if (f == ST_F_N) {
+    const size_t LKA = (size_t)h.L * h.K * h.A;
+    std::vector<int32_t> part((size_t)h.cnt_chunks * LKA);
+    ST_CUDA(c->ctx, cudaMemcpy(part.data(), h.npart, part.size() * 4, cudaMemcpyDeviceToHost));
+    int32_t* o = (int32_t*)host;
+    memset(o, 0, bytes);
+    for (int cc = 0; cc < h.cnt_chunks; cc++)
+      for (int k = 0; k < h.K; k++)
+        for (int a = 0; a < h.A; a++)
+          for (int l = 0; l < h.L; l++)
+            o[((size_t)l * h.K + k) * h.A + a] +=
+                part[(((size_t)cc * h.K + k) * h.A + a) * h.L + l];
+    return ST_OK;
+  }
+  if (f == ST_F_M) {
+    const size_t NK = (size_t)h.N * h.K;
+    std::vector<int32_t> part((size_t)h.cnt_groups * NK);
+    ST_CUDA(c->ctx, cudaMemcpy(part.data(), h.mpart, part.size() * 4, cudaMemcpyDeviceToHost));
+    int32_t* o = (int32_t*)host;
+    memset(o, 0, bytes);
+    for (int g = 0; g < h.cnt_groups; g++)
+      for (size_t j = 0; j < NK; j++) o[j] += part[(size_t)g * NK + j];
+    return ST_OK;
+  }
+  if (f == ST_F_LOGDIFF) {
+    std::vector<double> part((size_t)h.cnt_groups * h.N);
+    ST_CUDA(c->ctx, cudaMemcpy(part.data(), h.ldpart, part.size() * 8, cudaMemcpyDeviceToHost));
+    double* o = (double*)host;
+    for (int i = 0; i < h.N; i++) {
+      double s2 = 0.0;
+      for (int g = 0; g < h.cnt_groups; g++) s2 += part[(size_t)g * h.N + i];
+      o[i] = s2;
+    }
+    return ST_OK;
+  }
+  void* p = field_ptr(c, f);
+  if (!p) return seterr(c->ctx, ST_ERR_STATE, "field %d not held (store_z / ancestdist off?)", f);
+  ST_CUDA(c->ctx, cudaMemcpy(host, p, bytes, cudaMemcpyDeviceToHost));
+  return ST_OK;
+}
+
+extern "C" int st_set_state(st_chain* c, int f, const void* host, size_t bytes) {
+  if (!c || !host) return ST_ERR_ARG;
+  const size_t need = st_field_bytes(c, f);
+  if (need == 0 || bytes != need)
+    return seterr(c->ctx, ST_ERR_ARG, "field %d: %zu bytes given, %zu expected", f, bytes, need);
+  cudaSetDevice(c->ctx->device);
+  cudaStream_t s = c->ctx->stream;
+  ChainDev& h = c->h;
+  if (f == ST_F_REP) return set_rep(c, *(const int32_t*)host);
+  if (f == ST_F_DIMS || f == ST_F_LOGDIFF)
+    return seterr(c->ctx, ST_ERR_ARG, "field %d is read-only", f);
+  if (f == ST_F_N || f == ST_F_M) {
+    // counts become partial slice 0; the other slices are cleared
+    if (f == ST_F_N) {
+      const size_t LKA = (size_t)h.L * h.K * h.A;
+      std::vector<int32_t> part((size_t)h.cnt_chunks * LKA, 0);
+      const int32_t* in = (const int32_t*)host;
+      for (int k = 0; k < h.K; k++)
+        for (int a = 0; a < h.A; a++)
+          for (int l = 0; l < h.L; l++)
+            part[((size_t)k * h.A + a) * h.L + l] = in[((size_t)l * h.K + k) * h.A + a];
+      ST_CUDA(c->ctx, cudaMemcpy(h.npart, part.data(), part.size() * 4, cudaMemcpyHostToDevice));
+    } else {
+      const size_t NK = (size_t)h.N * h.K;
+      std::vector<int32_t> part((size_t)h.cnt_groups * NK, 0);
+      memcpy(part.data(), host, NK * 4);
+      ST_CUDA(c->ctx, cudaMemcpy(h.mpart, part.data(), part.size() * 4, cudaMemcpyHostToDevice));
+    }
+    return ST_OK;
+  }
+  void* p = field_ptr(c, f);
+  if (!p) return seterr(c->ctx, ST_ERR_STATE, "field %d not held (store_z / ancestdist off?)", f);
+  ST_CUDA(c->ctx, cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, s));
+  if (f == ST_F_Q || f == ST_F_P || f == ST_F_TESTQ) {
+    // keep the log companion consistent
+    const size_t n = bytes / 4;
+    std::vector<float> lg(n);
+    const float* v = (const float*)host;
+    for (size_t j = 0; j < n; j++) lg[j] = (float)log((double)v[j]);
+    void* lp = f == ST_F_Q ? (void*)h.logQ : (f == ST_F_P ? (void*)h.logP : (void*)h.logTestQ);
+    ST_CUDA(c->ctx, cudaMemcpyAsync(lp, lg.data(), bytes, cudaMemcpyHostToDevice, s));
+    ST_CUDA(c->ctx, cudaStreamSynchronize(s));
+  }
+  if (f == ST_F_Z) {
+    // counts follow Z (the reference's GetNumFromPops / GetNumLociPop)
+    int rc = zpass(c, kZRecount, 0);
+    if (rc) return rc;
+  }
+  ST_CUDA(c->ctx, cudaStreamSynchronize(s));
+  return ST_OK;
+}
+
+// ===========================================================================
+// batches
+// ===========================================================================
+extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch** out) {
+  if (!ctx || !chains || n < 1 || !out) return ST_ERR_ARG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  st_batch* b = new st_batch();
+  b->ctx = ctx;
+  b->chains.assign(chains, chains + n);
+  st_chain* c0 = chains[0];
+  b->fast = c0->fast;
+  b->W = c0->h.tileW;
+  int G = 1, KT = 0;
+  for (st_chain* c : b->chains) {
+    if (c->ctx != ctx || c->fast != b->fast || c->h.tileW != b->W ||
+        c->h.metrofreq != c0->h.metrofreq || c->host_rep != c0->host_rep ||
+        c->model.store_z != c0->model.store_z || c->model.precision != c0->model.precision) {
+      delete b;
+      return seterr(ctx, ST_ERR_ARG,
+                    "batched chains must share the context, data path, tile width, METROFREQ, "
+                    "sweep counter and Z storage");
+    }
+    G = std::max(G, c->h.G);
+    KT = std::max(KT, c->KT);
+    b->zsmem = std::max(b->zsmem, c->zsmem);
+  }
+  for (st_chain* c : b->chains)
+    if (c->fast && c->KT != KT) {
+      delete b;
+      return seterr(ctx, ST_ERR_ARG, "batched fast-path chains must share the K class");
+    }
+  b->G = G;
+  b->KT = KT;
+  std::vector<ChainDev> table(n);
+  std::vector<int> pz(n), pl(n), pi(n);
+  for (int j = 0; j < n; j++) {
+    table[j] = b->chains[j]->h;
+    pz[j] = b->tz; pl[j] = b->tl; pi[j] = b->ti;
+    b->tz += b->fast ? ctas_zpass_b2g(table[j]) : ctas_zpass_u8(table[j], 256);
+    b->tl += ctas_locus(table[j], kBlockLoc);
+    b->ti += ctas_ind(table[j], kBlockInd);
+  }
+  // every chain's kernels must index its groups by the batch-wide G
+  for (int j = 0; j < n; j++) table[j].G = G;
+  pl.clear(); pi.clear();
+  b->tl = b->ti = 0;
+  for (int j = 0; j < n; j++) {
+    pl.push_back(b->tl);
+    pi.push_back(b->ti);
+    b->tl += ctas_locus(table[j], kBlockLoc);
+    b->ti += ctas_ind(table[j], kBlockInd);
+  }
+  // per-chain reduction scratch is sized for G = 32 (st_chain_create).
+  auto alloc = [&](void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    return e == cudaSuccess ? ST_OK : seterr(ctx, ST_ERR_NOMEM, "batch table");
+  };
+  if (alloc((void**)&b->d_table, sizeof(ChainDev) * n) || alloc((void**)&b->d_pz, 4 * n) ||
+      alloc((void**)&b->d_pl, 4 * n) || alloc((void**)&b->d_pi, 4 * n)) {
+    st_batch_destroy(b);
+    return ST_ERR_NOMEM;
+  }
+  cudaMemcpy(b->d_table, table.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pz, pz.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pl, pl.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pi, pi.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  *out = b;
+  return ST_OK;
+}
+
+extern "C" int st_batch_destroy(st_batch* b) {
+  if (!b) return ST_ERR_ARG;
+  cudaSetDevice(b->ctx->device);
+  for (void* p : {(void*)b->d_table, (void*)b->d_pz, (void*)b->d_pl, (void*)b->d_pi})
+    if (p) cudaFree(p);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return ST_OK;
+}
+
+extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
+  if (!b || nsweeps < 0) return ST_ERR_ARG;
+  st_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  const int n = (int)b->chains.size();
+  st_chain* c0 = b->chains[0];
+  cudaStream_t s = ctx->stream;
+  LaunchSet lz{b->d_table, b->d_pz, n, b->tz, s};
+  LaunchSet ll{b->d_table, b->d_pl, n, b->tl, s};
+  LaunchSet li{b->d_table, b->d_pi, n, b->ti, s};
+  const int zflags = (c0->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
+                     (c0->model.store_z ? kZfStoreZ : 0);
+  cudaEventRecord(b->ev0, s);
+  for (int sw = 0; sw < nsweeps; sw++) {
+    const int rep = c0->host_rep;
+    const bool metro = c0->h.metrofreq > 0 && rep % c0->h.metrofreq == 0;
+    ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
+    if (metro) {
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndPropose, 0, kBlockInd));
+      if (!b->fast)
+        for (st_chain* c : b->chains)
+          ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * c->h.N, s));
+      ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZMetro, 0, b->zsmem)
+                           : launch_zpass_u8(lz, kZMetro, c0->model.precision ? kZfF64 : 0));
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndAccept, kIndAlpha | kIndCollect, kBlockInd));
+    } else {
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
+    }
+    if (!b->fast)
+      for (st_chain* c : b->chains) {
+        ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
+        ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
+      }
+    ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZNormal, zflags, b->zsmem)
+                         : launch_zpass_u8(lz, kZNormal, zflags | (c0->model.precision ? kZfF64 : 0)));
+    for (st_chain* c : b->chains) c->host_rep++;
+  }
+  cudaEventRecord(b->ev1, s);
+  return ST_OK;
+}

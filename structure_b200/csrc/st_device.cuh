@@ -1,0 +1,187 @@
+// st_device.cuh -- device-side building blocks shared by the sweep kernels:
+// Philox4x32-10 counters, uniform/normal conversions, the Lanczos ln-Gamma,
+// Marsaglia-Tsang log-gamma draws and warp-group reductions.
+//
+// Built with -fmad=false: every a*b+c below is two IEEE roundings unless it
+// is written as an explicit fma intrinsic, so the host restatement of the same
+// formulas (compiled with -ffp-contract=off) reproduces them exactly, up to
+// the last-ulp differences of log/exp/sin/cos between CUDA and libm.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "st_types.h"
+
+namespace st {
+
+// Random123 Philox4x32-10.  key = chain seed; counter = {index, sub-index,
+// sweep, stream << 24}.
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2,
+                                     uint32_t c3, uint64_t key) {
+  uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    uint32_t n0 = hi1 ^ c1 ^ k0;
+    uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return U4{c0, c1, c2, c3};
+}
+
+__device__ __forceinline__ U4 philox_s(uint32_t a, uint32_t b, uint32_t rep,
+                                       uint32_t stream, uint64_t key) {
+  return philox(a, b, rep, stream << 24, key);
+}
+
+// 52-bit uniform in (0,1).
+__device__ __forceinline__ double u01(uint32_t hi, uint32_t lo) {
+  uint64_t x = ((uint64_t)(hi >> 6) << 26) | (uint64_t)(lo >> 6);
+  return ((double)x + 0.5) * (1.0 / 4503599627370496.0);
+}
+
+// rnd() of ran.c:152 on a rand() stream w>>1 (31 bits), skipping zeros.
+__device__ __forceinline__ double rnd31(U4 w) {
+  uint32_t v[4] = {w.x >> 1, w.y >> 1, w.z >> 1, w.w >> 1};
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (v[j] != 0) return (double)v[j] / 2147483648.0;
+  return 1.0 / 4294967296.0;
+}
+
+// 24-bit uniform in [0,1) for the FP32 categorical draw.
+__device__ __forceinline__ float u24(uint32_t w) {
+  return (float)(w >> 8) * (1.0f / 16777216.0f);
+}
+
+constexpr double kTwoPi = 6.283185307179586;
+
+// Standard normal for MH proposals: Box-Muller on block {idx, 0, rep, stream}.
+__device__ __forceinline__ double normal_draw(uint32_t idx, uint32_t rep,
+                                              uint32_t stream, uint64_t key) {
+  U4 w = philox_s(idx, 0, rep, stream, key);
+  double u1 = u01(w.x, w.y), u2 = u01(w.z, w.w);
+  return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+}
+
+// ln Gamma(z), z > 0: Lanczos (1964) series, g = 7, nine terms, with the
+// coefficient set and summation order of the reference's mylgamma.
+__device__ __forceinline__ double lanczos_lgamma(double z) {
+  const double c1 = 676.5203681218835, c2 = -1259.139216722289,
+               c3 = 771.3234287757674, c4 = -176.6150291498386,
+               c5 = 12.50734324009056, c6 = -0.1385710331296526,
+               c7 = 9.934937113930748e-6, c8 = 1.659470187408462e-7;
+  double s = 0.0, t = z + 7.0;
+  s += c8 / t; t -= 1.0;
+  s += c7 / t; t -= 1.0;
+  s += c6 / t; t -= 1.0;
+  s += c5 / t; t -= 1.0;
+  s += c4 / t; t -= 1.0;
+  s += c3 / t; t -= 1.0;
+  s += c2 / t; t -= 1.0;
+  s += c1 / t;
+  s += 0.9999999999995183;
+  return log(s) + 0.9189385332046727 - (z + 6.5) + (z - 0.5) * log(z + 6.5);
+}
+
+// log of a Gamma(a, 1) draw by Marsaglia & Tsang (2000), "A simple method for
+// generating gamma variables", ACM TOMS 26(3).  Attempts come in pairs: block
+// 2j yields two Box-Muller normals, block 2j+1 their acceptance uniforms.
+// For a < 1, G(a) = G(a+1) * U^(1/a) (U from block 0xFFFFFFFF), in logs so that
+// tiny shapes never underflow.
+__device__ __forceinline__ double log_gamma_draw(double a, uint32_t e, uint32_t rep,
+                                                 uint32_t stream, uint64_t key,
+                                                 int* errbits) {
+  double aa = a < 1.0 ? a + 1.0 : a;
+  double d = aa - 1.0 / 3.0;
+  double c = 1.0 / sqrt(9.0 * d);
+  double lg = 0.0;
+  bool done = false;
+  for (uint32_t j = 0; j < kGammaMaxBlocks && !done; j += 2) {
+    U4 b0 = philox_s(e, j, rep, stream, key);
+    U4 b1 = philox_s(e, j + 1, rep, stream, key);
+    double u1 = u01(b0.x, b0.y), u2 = u01(b0.z, b0.w);
+    double rad = sqrt(-2.0 * log(u1));
+    double s, co;
+    sincos(kTwoPi * u2, &s, &co);
+    double xs[2] = {rad * co, rad * s};
+    double vs[2] = {u01(b1.x, b1.y), u01(b1.z, b1.w)};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (done) break;
+      double x = xs[h];
+      double t = 1.0 + c * x;
+      if (t <= 0.0) continue;
+      double v = t * t * t;
+      double x2 = x * x;
+      double u = vs[h];
+      if (u < 1.0 - 0.0331 * x2 * x2 || log(u) < 0.5 * x2 + d * (1.0 - v + log(v))) {
+        lg = log(d * v);
+        done = true;
+      }
+    }
+  }
+  if (!done) {
+    *errbits |= kErrGammaCap;
+    lg = log(d);
+  }
+  if (a < 1.0) {
+    U4 w = philox_s(e, 0xFFFFFFFFu, rep, stream, key);
+    lg += log(u01(w.x, w.y)) / a;
+  }
+  return lg;
+}
+
+// Butterfly over G lanes (G a power of two, width-G shuffles): every lane of
+// the group ends with the same pairwise-tree value.
+template <typename T>
+__device__ __forceinline__ T group_sum(T v, int G) {
+  for (int off = 1; off < G; off <<= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off, G);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T group_max(T v, int G) {
+  for (int off = 1; off < G; off <<= 1) {
+    T o = __shfl_xor_sync(0xffffffffu, v, off, G);
+    v = o > v ? o : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ void set_err(int* err, int bits) {
+  if (bits) atomicOr(err, bits);
+}
+
+// "Last CTA" protocol for per-chain reductions: each CTA writes its partial,
+// fences, and bumps a counter; the CTA that observes count == total-1 owns the
+// finalisation and resets the counter for the next launch.  No spinning.
+__device__ __forceinline__ bool last_cta_arrive(unsigned* ctr, unsigned total) {
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev = atomicAdd(ctr, 1u);
+    s_last = (prev == total - 1) ? 1u : 0u;
+    if (s_last) *ctr = 0u;
+  }
+  __syncthreads();
+  bool last = s_last != 0u;
+  if (last) __threadfence();
+  return last;
+}
+
+// Binary search of the owning chain for a flat tile index.
+__device__ __forceinline__ int find_chain(const int* prefix, int nchains, int t) {
+  int lo = 0, hi = nchains - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+}  // namespace st

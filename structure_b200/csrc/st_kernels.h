@@ -1,0 +1,53 @@
+// st_kernels.h -- host-side launchers of the sweep kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "st_types.h"
+
+namespace st {
+
+// Chains covered by one launch: a device table of ChainDev and, per launch
+// kind, the exclusive prefix of CTA counts (device array, nchains entries).
+struct LaunchSet {
+  ChainDev* chains;      // device pointer
+  const int* prefix;     // device pointer
+  int nchains;
+  int total_ctas;
+  cudaStream_t stream;
+};
+
+// Z-pass modes.
+enum ZMode : int { kZNormal = 0, kZInit = 1, kZRecount = 2, kZMetro = 3, kZLike = 4 };
+// Z-pass flags.
+enum : int {
+  kZfLikeIfCollect = 0x1,  // compute ln P(D) when the sweep collects
+  kZfLikeAlways = 0x2,     // compute ln P(D) regardless
+  kZfStoreZ = 0x4,         // write Z bytes
+  kZfCollect = 0x8,        // fold ln P(D) into sumlikes/sumsqlikes when collecting
+  kZfAdvance = 0x10,       // bump the device sweep counter at the end
+  kZfF64 = 0x20,           // generic path: FP64 arithmetic (reference bit-parity)
+  kZfInjected = 0x40       // generic path: uniforms from the injected array
+};
+
+// Locus-kernel stages.
+enum : int { kLocP = 0x1, kLocEps = 0x2, kLocFst = 0x4, kLocCollect = 0x8 };
+// Individual-kernel modes and stages.
+enum : int { kIndGibbs = 0, kIndPropose = 1, kIndAccept = 2, kIndNone = 3 };
+enum : int { kIndAlpha = 0x1, kIndCollect = 0x2 };
+
+size_t zpass_b2g_smem(int KT, int K, int T, int W, int mode);
+cudaError_t launch_zpass_b2g(const LaunchSet& ls, int KT, int W, int mode, int flags,
+                             size_t smem);
+cudaError_t launch_zpass_u8(const LaunchSet& ls, int mode, int flags);
+cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block);
+cudaError_t launch_ind(const LaunchSet& ls, int G, int mode, int stages, int block);
+cudaError_t launch_collect(const LaunchSet& ls, int block);
+cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
+
+// CTA counts per chain for each launch kind (host-side mirror of the tiling).
+int ctas_zpass_b2g(const ChainDev& c);
+int ctas_zpass_u8(const ChainDev& c, int block);
+int ctas_locus(const ChainDev& c, int block);
+int ctas_ind(const ChainDev& c, int block);
+int ctas_collect(const ChainDev& c, int block);
+
+}  // namespace st

@@ -1,0 +1,92 @@
+// st_types.h -- device-resident chain descriptor and the constants shared by
+// the sweep kernels and the C-ABI layer.
+#pragma once
+#include <cstdint>
+
+namespace st {
+
+constexpr int kMaxPops = 32;          // K limit of the fused kernels
+constexpr int kMaxAlleles = 64;       // per-locus allele limit (register arrays)
+constexpr uint32_t kGammaMaxBlocks = 64;
+constexpr int kUnassigned = -9;       // structure.h:8
+constexpr uint8_t kZMissing = 0xFF;   // Z byte for a missing copy
+constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
+
+// Philox stream ids (counter word 3 = id << 24).
+enum Stream : uint32_t {
+  kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
+  kSAlpha = 7, kSEps = 8, kSFst = 9
+};
+
+// Device error word bits.
+enum : int {
+  kErrGammaCap = 0x1,    // gamma rejection loop hit its attempt cap
+  kErrNaN = 0x2,         // non-finite value produced
+  kErrBounds = 0x4,      // out-of-range index caught and skipped
+  kErrFallThrough = 0x8  // categorical draw fell through (clamped)
+};
+
+// Genotype layouts on the device.
+enum Layout : int {
+  kLayoutU8 = 0,   // [N][2][L] bytes, allele code or 0xFF (reference order)
+  kLayoutB2G = 1   // [L][wpr] uint32, 16 genotypes/word, 2 bits each:
+                   // 0 = 0/0, 1 = 0/1, 2 = 1/1, 3 = missing
+};
+
+// Stats block (doubles) offsets.
+enum : int {
+  kStLike = 0, kStSumLikes = 1, kStSumSq = 2, kStNLike = 3, kStMetroHits = 4,
+  kStEpsAcc = 5, kStAlphaT = 6, kStCopies = 7,
+  kStAlphaS = 8,                       // K sums of log Q_ik
+  kStFstDiff = kStAlphaS + kMaxPops,   // F likelihood differences
+  kStFstNew = kStFstDiff + kMaxPops,   // F proposals
+  kStAlphaLpd = kStFstNew + kMaxPops,  // alpha log acceptance ratios
+  kStFstLpd = kStAlphaLpd + kMaxPops,  // F log acceptance ratios
+  kStAlphaNew = kStFstLpd + kMaxPops,  // alpha proposals
+  kStSize = 256
+};
+
+// Done-counter slots of the last-CTA protocol.
+enum : int { kCtrZ = 0, kCtrLocus = 1, kCtrInd = 2, kCtrMetro = 3, kCtrCount = 8 };
+
+struct ChainDev {
+  // dimensions
+  int N, L, K, A, G;        // G = power of two >= K (lanes per group)
+  int layout, wpr;          // genotype layout, B2G words per locus row
+  int Leff;                 // loci with at least one observed allele
+  // model (mainparams / extraparams)
+  int freqscorr, onefst, inferalpha, popalphas, unifprioralpha;
+  int computeprob, pfrompopflagonly, ancestdist, numboxes, metrofreq, burnin;
+  double alphamax, alphapropsd, alphapriora, alphapriorb;
+  double fpriormean, fpriorsd, invsqrtnuminds;
+  uint64_t key;
+  // Z-pass tiling: T individuals per chunk, W warps, R locus blocks per CTA
+  int tileT, tileW, tileR, nchunks, ngroups;
+  // count partials currently held (producer's decomposition)
+  int cnt_chunks, cnt_groups;
+  // data
+  const uint32_t* g2;
+  const uint8_t* g8;
+  const int32_t* numalleles;
+  const int32_t* popflags;
+  // state
+  float *Q, *logQ, *TestQ, *logTestQ;   // N*K
+  float *P, *logP;                      // L*K*A
+  double *eps;                          // L*A
+  double *F, *alpha, *lambda;           // K
+  uint8_t* Z;                           // N*2*L (optional)
+  int32_t* npart;                       // [chunks][K][A][L]
+  int32_t* mpart;                       // [groups][N][K]
+  double* ldpart;                       // [groups][N]
+  // accumulators
+  double *QSum, *PSum, *SumEps, *FstSum, *sumAlpha, *sumlambda;
+  int32_t* AncestDist;                  // N*K*numboxes
+  double* stats;                        // kStSize
+  double *likepart, *redpart;           // per-CTA partials
+  unsigned* ctr;                        // kCtrCount
+  int* rep;                             // device sweep counter
+  int* err;                             // device error word
+  const double* injected;               // parity uniforms (reference slots)
+};
+
+}  // namespace st

