@@ -1,0 +1,401 @@
+#!/usr/bin/env python3
+"""bench.py -- chain-sweeps/s of STRUCTURE's per-sweep MCMC on B200.
+
+Workload (the large SNP panel): N=2000 diploid individuals, L=50,000 biallelic
+SNPs packed 2 bits/genotype, 3% missing genotypes, K=5 correlated-frequency (F)
+model with Fst_k = {0.05..0.25}, Q_i ~ Dirichlet(0.3), alpha and F inferred,
+METROFREQ=10, FPRIORMEAN/SD = 0.01/0.05; 20 chains (seeds 2000+r) batched on
+one GPU.  A step is one batched sweep (20 chain-sweeps: P, Q, Z, alpha, eps, F,
+DataCollection).  Warm-up steps are the burn-in; timed steps collect.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own 20-chain batch (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WL = dict(N=2000, L=50000, K=5, chains=20, F=[0.05, 0.10, 0.15, 0.20, 0.25], qalpha=0.3,
+          missing=0.03, metrofreq=10, fpriormean=0.01, fpriorsd=0.05, alphapropsd=0.025)
+WORKLOAD_NAME = "snp-fmodel N=2000 L=50000 K=5, 20 chains batched"
+SLICE_L = 10000          # CPU legs time a 10,000-locus slice and scale by L
+METRIC = "chain-sweeps/s"
+
+
+def model_kwargs(burnin, numreps):
+    return dict(maxpops=WL["K"], burnin=burnin, numreps=numreps, freqscorr=1, onefst=0,
+                inferalpha=1, popalphas=0, unifprioralpha=1, alpha=1.0, alphamax=10.0,
+                alphapropsd=WL["alphapropsd"], fpriormean=WL["fpriormean"],
+                fpriorsd=WL["fpriorsd"], metrofreq=WL["metrofreq"], computeprob=1, store_z=0)
+
+
+def make_data():
+    from structure_b200 import synth
+    return synth.config2(N=WL["N"], L=WL["L"], want_int32=False)
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the reference's own CPU update functions (oracle/_ref) in
+# structure.c order, timed over one METROFREQ cycle (9 Gibbs + 1 Metropolis
+# sweep) of a 10,000-locus slice; time scales linearly in L.
+# ---------------------------------------------------------------------------
+def _ref_worker(q, path, N, L_slice, seed, core):
+    try:
+        if core is not None:
+            os.sched_setaffinity(0, {core})
+        from oracle.oracle import RefLib, ref_model
+        geno = np.load(path)
+        r = RefLib()
+        m = ref_model(N=N, L=L_slice, K=WL["K"], maxalleles=2, freqscorr=1,
+                      fpriormean=WL["fpriormean"], fpriorsd=WL["fpriorsd"],
+                      metrofreq=WL["metrofreq"], burnin=0, numreps=100,
+                      alphapropsd=WL["alphapropsd"])
+        ch = r.chain_new(m, geno, seed=seed)
+        r.lib.stref_chain_sweeps(ch, 1)                   # rep 0 (untimed warm-up)
+        t0 = time.perf_counter()
+        r.lib.stref_chain_sweeps(ch, 10)                  # reps 1..10: 9 Gibbs + 1 Metropolis
+        dt = time.perf_counter() - t0
+        r.lib.stref_chain_free(ch)
+        q.put(dt)
+    except Exception as e:  # pragma: no cover - reported to the parent
+        q.put(repr(e))
+
+
+def cpu_reference(packed, workers, pin=False):
+    """chain-sweeps/s of `workers` concurrent reference chains at full L."""
+    from structure_b200 import synth
+    geno = synth.unpack_int32(packed, WL["N"], 0, SLICE_L)
+    tmp = tempfile.NamedTemporaryFile(suffix=".npy", delete=False)
+    np.save(tmp.name, geno)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ref_worker,
+                         args=(q, tmp.name, WL["N"], SLICE_L, 1000 + w, (w if pin else None)))
+             for w in range(workers)]
+    for p in procs:
+        p.start()
+    res = []
+    while len(res) < len(procs):
+        try:
+            res.append(q.get(timeout=5))
+        except Exception:
+            dead = [p for p in procs if not p.is_alive() and p.exitcode not in (0, None)]
+            if dead:
+                for p in procs:
+                    p.kill()
+                raise RuntimeError(f"reference worker exited with code {dead[0].exitcode}")
+    for p in procs:
+        p.join()
+    os.unlink(tmp.name)
+    bad = [x for x in res if not isinstance(x, float)]
+    if bad:
+        raise RuntimeError(f"reference worker failed: {bad[0]}")
+    scale = SLICE_L / WL["L"]
+    rate = sum(10.0 / dt for dt in res) * scale
+    sample = (f"{workers} concurrent reference chain(s), each timed over sweeps 1-10 "
+              f"(9 Gibbs + 1 Metropolis) of a {SLICE_L}-locus slice (N={WL['N']}, K={WL['K']}, "
+              f"F model), scaled by {SLICE_L}/{WL['L']} loci; uniforms for the array-fed "
+              f"updates from xorshift128+")
+    return rate, sample, max(res)
+
+
+def usable_workers():
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        mem = psutil.virtual_memory().available
+        n = min(n, max(1, int(mem // (2 << 30))))
+    except Exception:
+        pass
+    return max(1, min(n, WL["chains"]))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.p is None:
+            return out
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j] == "Active"})
+        out.update(sm_mhz=float(np.median(sm)) if sm else None,
+                   sm_max_mhz=max(mx) if mx else None, reasons=reasons, samples=len(rows))
+        return out
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """DRAM bytes per Z-pass launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "zpass_b2g_snp2000x50000_k5_batch20.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from structure_b200 import api
+
+    d = make_data()
+    packed, na = d["packed"], d["numalleles"]
+    N, L, K, B = WL["N"], WL["L"], WL["K"], WL["chains"]
+    W, S = args.warmup, args.steps
+    codes = (packed[:, :, None] >> (2 * np.arange(16, dtype=np.uint32))[None, None, :]) & 3
+    copies = int(2 * (codes.reshape(L, -1)[:, :N] != 3).sum())
+
+    ctx = api.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    data = api.Data(ctx, na, packed=packed, num_inds=N, num_loci=L, layout=api.LAYOUT_B2G)
+    mk = model_kwargs(burnin=W, numreps=S + 10)
+    chains = [api.Chain(ctx, data, api.model_defaults(**mk), 2000 + 1000 * rank + r)
+              for r in range(B)]
+    batch = api.Batch(ctx, chains)
+
+    # warm-up = burn-in
+    batch.sweep(W)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ctx.profile(True)
+    ctx.profile_read()
+    clocks = ClockSampler(local)
+    l0 = ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.sweep(S)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launches() - l0
+    prof = ctx.profile_read()
+    clk = clocks.stop()
+    ctx.profile(False)
+    for c in chains:
+        assert c.sync() == 0, "device error word set"
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * B * S / (ms / 1e3)
+
+    # plain path: the same chains one at a time (one chain per launch)
+    plain_sweeps = max(2, min(S, 10))
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for c in chains:
+        c.sweep(plain_sweeps)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain = B * plain_sweeps / (p0.elapsed_time(p1) / 1e3)
+    like = [c.get(api.F_STATS)[api.ST_SUMLIKES] / max(1, c.get(api.F_STATS)[api.ST_NLIKE])
+            for c in chains]
+    batch.close()
+    for c in chains:
+        c.close()
+    data.close()
+
+    # end to end through the C ABI from pinned host memory
+    pinned = torch.from_numpy(packed).pin_memory()
+    ppk = pinned.numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    data2 = api.Data(ctx, na, packed=ppk, num_inds=N, num_loci=L, layout=api.LAYOUT_B2G)
+    mk2 = model_kwargs(burnin=0, numreps=S)
+    ch2 = [api.Chain(ctx, data2, api.model_defaults(**mk2), 9000 + r) for r in range(B)]
+    b2 = api.Batch(ctx, ch2)
+    b2.sweep(S)
+    d2h = 0
+    for c in ch2:
+        for f in (api.F_QSUM, api.F_PSUM, api.F_STATS, api.F_ALPHA, api.F_F):
+            d2h += c.get(f).nbytes
+    t_e2e = time.perf_counter() - t0
+    e2e = B * S / t_e2e
+    b2.close()
+    for c in ch2:
+        c.close()
+    data2.close()
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel (the Z pass)
+    zms, zn = prof["zpass"]
+    zavg = zms / max(1, zn)
+    G = packed.nbytes
+    per_chain = N * K * 4 + L * K * 2 * 4 + (L * K * 2 + N * K) * 4
+    alg_bytes = G + B * per_chain
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (zavg / 1e3) / 1e9
+    ops_per_copy = 2 * K + 2 + 10 + 0.5
+    alu_achieved = B * copies * ops_per_copy / (zavg / 1e3) / 1e12
+    sm_mhz = clk["sm_mhz"] or 1965.0
+    alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+    traffic = read_traffic()
+    total_ms = sum(v[0] for v in prof.values())
+
+    cpu_rate, cpu_sample, _ = (None, None, None)
+    if not args.no_cpu_baseline and world == 1:
+        cpu_rate, cpu_sample, _ = cpu_reference(packed, 1, pin=True)
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world,
+        "steps": S, "warmup": W, "ms_per_step": round(ms / S, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
+        "data": "synthetic, seeded (STRUCTURE's generative model; no public dataset is named)",
+        "config": {"workload": WORKLOAD_NAME, "N": N, "L": L, "K": K, "chains_per_gpu": B,
+                   "model": "admixture + F model, alpha and F inferred, METROFREQ=10",
+                   "genotypes": "2 bits/genotype, locus-major", "store_z": False,
+                   "l2": f"no flush: per-sweep working set {(G + B * (per_chain + L * K * 2 * 12)) / 1e9:.2f} GB > 126 MB L2",
+                   "parallelism": f"{world} GPU x {B} chains (replicas)"},
+        "z_updates_per_s": round(value * copies, 1),
+        "plain": {"value": round(plain, 3), "unit": METRIC,
+                  "path": "one chain per launch, same kernels"},
+        "batched_over_plain": round(value / world / plain, 3),
+        "mean_lnpd_over_chains": round(float(np.mean(like)), 2),
+        "e2e": {"value": round(e2e, 3), "unit": METRIC,
+                "h2d_bytes_per_step": int(math.ceil(packed.nbytes / S)),
+                "d2h_bytes_per_step": int(math.ceil(d2h / S)),
+                "includes": "st_data_upload from pinned host words, 20 x st_chain_create "
+                            "(initial Z pass), st_batch_sweep, st_get_state of QSum/PSum/"
+                            "stats/alpha/F"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
+                     "peak_source": peak_kind,
+                     "kernel": "zpass_b2g_kernel<8,kZNormal> (batched, 20 chains)",
+                     "avg_launch_ms": round(zavg, 4),
+                     "algorithmic_bytes_per_launch": int(alg_bytes)},
+        "roofline_alu": {"bound": "alu", "achieved": round(alu_achieved, 3),
+                         "peak": round(alu_peak, 2), "unit": "Top/s",
+                         "frac": round(alu_achieved / alu_peak, 4),
+                         "ops_per_copy": ops_per_copy,
+                         "note": "2K+2 FP32 + ~10 int (Philox/4) + 0.5 log per allele copy; "
+                                 "peak = 148 SM x 128 lanes x median SM clock"},
+        "kernels_ms": {k: round(v[0], 3) for k, v in prof.items()},
+        "kernel_share": {k: round(v[0] / total_ms, 4) for k, v in prof.items()} if total_ms else {},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu_rate is not None:
+        out["cpu_baseline"] = {"value": round(cpu_rate, 5), "unit": METRIC, "cores": 1,
+                               "kind": "reference", "sample": cpu_sample}
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    d = make_data()
+    workers = usable_workers()
+    rate, sample, tmax = cpu_reference(d["packed"], workers, pin=False)
+    out = {"metric": METRIC, "value": round(rate, 5), "unit": METRIC, "n_gpus": world,
+           "steps": 10, "warmup": 10, "ms_per_step": round(tmax * 1e3 / 10, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic, seeded (same generator and seed as the GPU arm)",
+           "config": {"workload": WORKLOAD_NAME, "N": WL["N"], "L": WL["L"], "K": WL["K"],
+                      "slice_loci": SLICE_L, "workers": workers},
+           "impl": "reference",
+           "cpu_baseline": {"value": round(rate, 5), "unit": METRIC, "cores": workers,
+                            "kind": "reference", "sample": sample},
+           "e2e": {"value": round(rate, 5), "unit": METRIC, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -74,6 +74,19 @@ int st_ctx_create(int device, size_t hbm_budget, st_ctx **out);
 int st_ctx_destroy(st_ctx *ctx);
 const char *st_last_error(const st_ctx *ctx);
 int st_ctx_memory(const st_ctx *ctx, size_t *in_use, size_t *budget);
+/* Launch on the caller's cudaStream_t (passed as void*) instead of the
+ * context's own stream; NULL restores the context stream.                   */
+int st_ctx_set_stream(st_ctx *ctx, void *cuda_stream);
+
+/* Per-kernel timing: when enabled, every launch is bracketed by CUDA events on
+ * the launching stream.  st_ctx_profile_read synchronises, returns total
+ * device milliseconds and launch counts per kind (ST_K_*), and clears them.
+ * st_ctx_launches counts every kernel launched by the context.              */
+enum st_kernel_kind { ST_K_LOCUS = 0, ST_K_IND = 1, ST_K_ZPASS = 2, ST_K_METRO = 3,
+                      ST_K_OTHER = 4, ST_K_COUNT = 5 };
+int st_ctx_profile(st_ctx *ctx, int enable);
+int st_ctx_profile_read(st_ctx *ctx, double ms[ST_K_COUNT], int64_t launches[ST_K_COUNT]);
+int64_t st_ctx_launches(const st_ctx *ctx);
 
 /* ---- data ----------------------------------------------------------------
  * Replaces the Geno/NumAlleles/popflags uploads of src/structure.c:427-483.

@@ -50,6 +50,23 @@ void writeBuffer(CLDict *d, void *p, size_t s, enum BUFFER b, char *m)
 { (void)d; (void)p; (void)s; (void)b; (void)m; }
 void finishCommands(CLDict *d, char *m) { (void)d; (void)m; }
 
+/* ---- uniform-array cursor --------------------------------------------------
+ * The CPU update functions read uniforms through a cursor over randomArr
+ * (randGen.c:23-36).  The reference version ends the process when one slot
+ * region is over-read; UpdateQMetro's gamma draws can do that with its
+ * 64-value budget per individual.  This cursor keeps reading the following
+ * values of the array and counts the overrun instead.                        */
+#include "randGen.h"
+static long g_guard_hits = 0;
+long stref_guard_hits(void) { return g_guard_hits; }
+double rndDisc(RndDiscState *s)
+{
+    double v = s->randomArr[s->baseOffset + s->randomValsTaken];
+    s->randomValsTaken += 1;
+    if (s->randomValsTaken > s->maxrandom) g_guard_hits++;
+    return v;
+}
+
 /* ---- controlled random streams ------------------------------------------ */
 static const int32_t *g_rq = NULL;
 static long g_rq_n = -1, g_rq_pos = 0, g_rq_over = 0;

@@ -71,6 +71,10 @@ def lib():
         "st_ctx_destroy": ([vp], C.c_int),
         "st_last_error": ([vp], C.c_char_p),
         "st_ctx_memory": ([vp, C.POINTER(sz), C.POINTER(sz)], C.c_int),
+        "st_ctx_set_stream": ([vp, vp], C.c_int),
+        "st_ctx_profile": ([vp, C.c_int], C.c_int),
+        "st_ctx_profile_read": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)], C.c_int),
+        "st_ctx_launches": ([vp], C.c_int64),
         "st_data_upload": ([vp, C.POINTER(DataDesc), C.POINTER(vp)], C.c_int),
         "st_data_destroy": ([vp], C.c_int),
         "st_data_layout": ([vp], C.c_int),
@@ -126,6 +130,25 @@ class Context:
         a, b = C.c_size_t(), C.c_size_t()
         lib().st_ctx_memory(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def set_stream(self, stream_handle):
+        """Launch on a caller's cudaStream_t (int handle, e.g. torch's
+        Stream.cuda_stream); None restores the context's own stream."""
+        self.check(lib().st_ctx_set_stream(self.h, stream_handle or None))
+
+    def profile(self, enable=True):
+        self.check(lib().st_ctx_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{kind: (ms, launches)} since the last read (kinds: locus, ind, zpass,
+        metro, other)."""
+        ms = (C.c_double * 5)()
+        n = (C.c_int64 * 5)()
+        self.check(lib().st_ctx_profile_read(self.h, ms, n))
+        return {k: (ms[j], n[j]) for j, k in enumerate(("locus", "ind", "zpass", "metro", "other"))}
+
+    def launches(self):
+        return lib().st_ctx_launches(self.h)
 
     def close(self):
         if self.h:

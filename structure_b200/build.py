@@ -19,8 +19,12 @@ SOURCES = ["st_zpass.cu", "st_update.cu", "st_api.cu"]
 HEADERS = ["st_device.cuh", "st_types.h", "st_kernels.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "-I" + os.path.join(ROOT, "include")]
+# The data pass must round every product and sum exactly like its host
+# restatement (bit-exact Z); the FP64 Metropolis/Dirichlet code may contract.
+PER_FILE = {"st_zpass.cu": ["-fmad=false"], "st_api.cu": ["-fmad=false"],
+            "st_update.cu": ["-fmad=true"]}
 
 
 def _stale(target, deps):
@@ -39,7 +43,7 @@ def build(force=False, verbose=False):
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+            cmd = [NVCC] + ARCH + FLAGS + PER_FILE.get(src, []) + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

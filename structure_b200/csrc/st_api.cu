@@ -17,8 +17,15 @@ using namespace st;
 struct st_ctx {
   int device = 0;
   size_t budget = 0, in_use = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // launch stream (own or caller's)
+  cudaStream_t own = nullptr;
   std::string err;
+  int64_t launches = 0;
+  bool profile = false;
+  struct Ev { cudaEvent_t a, b; int kind; };
+  std::vector<Ev> evs;
+  double prof_ms[ST_K_COUNT] = {0};
+  int64_t prof_n[ST_K_COUNT] = {0};
 };
 
 struct st_data {
@@ -128,6 +135,27 @@ int fast_kt(int K) {
   return 0;
 }
 
+// Bracket one launch with events when profiling; always count it.
+struct Bracket {
+  st_ctx* ctx;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Bracket(st_ctx* c, int k) : ctx(c), kind(k) {
+    ctx->launches++;
+    if (ctx->profile) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  ~Bracket() {
+    if (ctx->profile) {
+      cudaEventRecord(b, ctx->stream);
+      ctx->evs.push_back({a, b, kind});
+    }
+  }
+};
+
 LaunchSet single(st_chain* c, int ctas) {
   LaunchSet ls;
   ls.chains = c->d_chain;
@@ -152,21 +180,30 @@ int set_rep(st_chain* c, int rep) {
 }
 
 // Z-pass tiling heuristic: W warps of 32 loci, T individuals per chunk (a
-// multiple of 16), R locus blocks per CTA so that about two waves of CTAs
-// cover the data.
+// multiple of 16), R locus blocks per CTA.  Shared memory is kept under
+// 72 KB so three 256-thread CTAs fit on an SM (the kernel is built for 3).
+size_t zpass_smem_all(int KT, int K, int T, int W) {
+  size_t s = 0;
+  for (int mode : {kZNormal, kZMetro, kZInit, kZRecount, kZLike})
+    s = std::max(s, zpass_b2g_smem(KT, K, T, W, mode));
+  return s;
+}
+
 void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R) {
-  int w = m->tile_w > 0 ? m->tile_w : 8;
-  if (w > 8) w = 8;
-  int t = m->tile_t > 0 ? m->tile_t : 512;
+  const int KT = fast_kt(K);
+  int w = zpass_b2g_width(KT);
+  int t = m->tile_t > 0 ? m->tile_t : 256;
   t = (t + 15) & ~15;
-  int np = (N + 15) & ~15;
+  const int np = (N + 15) & ~15;
   if (t > np) t = np;
-  while (t > 16 && zpass_b2g_smem(fast_kt(K), K, t, w, kZMetro) > 160 * 1024) t -= 16;
+  const size_t budget = 72 * 1024;
+  while (m->tile_t <= 0 && t > 32 && zpass_smem_all(KT, K, t, w) > budget) t -= 16;
+  while (t > 16 && zpass_smem_all(KT, K, t, w) > 200 * 1024) t -= 16;
   int r = m->tile_r;
   if (r <= 0) {
-    long lblocks = (L + 32 * w - 1) / (32 * w);
-    long nch = (N + t - 1) / t;
-    long target = 148L * 8;
+    const long lblocks = (L + 32 * w - 1) / (32 * w);
+    const long nch = (N + t - 1) / t;
+    const long target = 148L * 3 * 2;
     r = (int)std::max(1L, (lblocks * nch) / target);
     if (r > 64) r = 64;
   }
@@ -176,6 +213,7 @@ void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R)
 }
 
 int zpass(st_chain* c, int mode, int flags) {
+  Bracket br(c->ctx, mode == kZMetro ? ST_K_METRO : (mode == kZNormal ? ST_K_ZPASS : ST_K_OTHER));
   if (c->fast) {
     LaunchSet ls = single(c, ctas_zpass_b2g(c->h));
     return cuda_check(c->ctx, launch_zpass_b2g(ls, c->KT, c->h.tileW, mode, flags, c->zsmem),
@@ -194,11 +232,13 @@ int zpass(st_chain* c, int mode, int flags) {
 }
 
 int locus(st_chain* c, int stages) {
+  Bracket br(c->ctx, ST_K_LOCUS);
   LaunchSet ls = single(c, ctas_locus(c->h, kBlockLoc));
   return cuda_check(c->ctx, launch_locus(ls, c->h.G, stages, kBlockLoc), "locus");
 }
 
 int ind(st_chain* c, int mode, int stages) {
+  Bracket br(c->ctx, ST_K_IND);
   LaunchSet ls = single(c, ctas_ind(c->h, kBlockInd));
   return cuda_check(c->ctx, launch_ind(ls, c->h.G, mode, stages, kBlockInd), "ind");
 }
@@ -244,10 +284,11 @@ extern "C" int st_ctx_create(int device, size_t hbm_budget, st_ctx** out) {
   cudaMemGetInfo(&fr, &tot);
   const size_t reserve = (size_t)2 << 30;
   ctx->budget = hbm_budget ? hbm_budget : (fr > reserve ? fr - reserve : fr / 2);
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
     return ST_ERR_CUDA;
   }
+  ctx->stream = ctx->own;
   *out = ctx;
   return ST_OK;
 }
@@ -256,10 +297,49 @@ extern "C" int st_ctx_destroy(st_ctx* ctx) {
   if (!ctx) return ST_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  cudaStreamDestroy(ctx->stream);
+  for (auto& e : ctx->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  cudaStreamDestroy(ctx->own);
   delete ctx;
   return ST_OK;
 }
+
+extern "C" int st_ctx_set_stream(st_ctx* ctx, void* stream) {
+  if (!ctx) return ST_ERR_ARG;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return ST_OK;
+}
+
+extern "C" int st_ctx_profile(st_ctx* ctx, int enable) {
+  if (!ctx) return ST_ERR_ARG;
+  ctx->profile = enable != 0;
+  return ST_OK;
+}
+
+extern "C" int st_ctx_profile_read(st_ctx* ctx, double* ms, int64_t* n) {
+  if (!ctx) return ST_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  ST_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto& e : ctx->evs) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, e.a, e.b) == cudaSuccess) {
+      ctx->prof_ms[e.kind] += t;
+      ctx->prof_n[e.kind] += 1;
+    }
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  cudaGetLastError();
+  ctx->evs.clear();
+  for (int k = 0; k < ST_K_COUNT; k++) {
+    if (ms) ms[k] = ctx->prof_ms[k];
+    if (n) n[k] = ctx->prof_n[k];
+    ctx->prof_ms[k] = 0.0;
+    ctx->prof_n[k] = 0;
+  }
+  return ST_OK;
+}
+
+extern "C" int64_t st_ctx_launches(const st_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
 extern "C" const char* st_last_error(const st_ctx* ctx) {
   return ctx ? ctx->err.c_str() : "null context";
@@ -504,9 +584,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     h.nchunks = (N + T - 1) / T;
     const int lblocks = (L + 32 * W - 1) / (32 * W);
     h.ngroups = (lblocks + R - 1) / R;
-    c->zsmem = 0;
-    for (int mode : {kZNormal, kZMetro, kZInit, kZRecount, kZLike})
-      c->zsmem = std::max(c->zsmem, zpass_b2g_smem(c->KT, K, T, W, mode));
+    c->zsmem = zpass_smem_all(c->KT, K, T, W);
   } else {
     h.tileT = N; h.tileW = 8; h.tileR = 1;
     h.nchunks = 1;
@@ -675,6 +753,7 @@ extern "C" int st_collect(st_chain* c) {
   int rc = ST_OK;
   if (c->h.computeprob) rc = zpass(c, kZLike, kZfLikeAlways);
   if (rc) return rc;
+  Bracket br(c->ctx, ST_K_OTHER);
   LaunchSet ls = single(c, ctas_collect(c->h, kBlockCol));
   return cuda_check(c->ctx, launch_collect(ls, kBlockCol), "collect");
 }
@@ -1028,16 +1107,27 @@ extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
   for (int sw = 0; sw < nsweeps; sw++) {
     const int rep = c0->host_rep;
     const bool metro = c0->h.metrofreq > 0 && rep % c0->h.metrofreq == 0;
-    ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
+    {
+      Bracket br(ctx, ST_K_LOCUS);
+      ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
+    }
     if (metro) {
-      ST_CUDA(ctx, launch_ind(li, b->G, kIndPropose, 0, kBlockInd));
+      {
+        Bracket br(ctx, ST_K_IND);
+        ST_CUDA(ctx, launch_ind(li, b->G, kIndPropose, 0, kBlockInd));
+      }
       if (!b->fast)
         for (st_chain* c : b->chains)
           ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * c->h.N, s));
-      ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZMetro, 0, b->zsmem)
-                           : launch_zpass_u8(lz, kZMetro, c0->model.precision ? kZfF64 : 0));
+      {
+        Bracket br(ctx, ST_K_METRO);
+        ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZMetro, 0, b->zsmem)
+                             : launch_zpass_u8(lz, kZMetro, c0->model.precision ? kZfF64 : 0));
+      }
+      Bracket br(ctx, ST_K_IND);
       ST_CUDA(ctx, launch_ind(li, b->G, kIndAccept, kIndAlpha | kIndCollect, kBlockInd));
     } else {
+      Bracket br(ctx, ST_K_IND);
       ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
     }
     if (!b->fast)
@@ -1045,8 +1135,11 @@ extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
         ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
         ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
       }
-    ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZNormal, zflags, b->zsmem)
-                         : launch_zpass_u8(lz, kZNormal, zflags | (c0->model.precision ? kZfF64 : 0)));
+    {
+      Bracket br(ctx, ST_K_ZPASS);
+      ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZNormal, zflags, b->zsmem)
+                           : launch_zpass_u8(lz, kZNormal, zflags | (c0->model.precision ? kZfF64 : 0)));
+    }
     for (st_chain* c : b->chains) c->host_rep++;
   }
   cudaEventRecord(b->ev1, s);

@@ -35,6 +35,7 @@ enum : int { kIndGibbs = 0, kIndPropose = 1, kIndAccept = 2, kIndNone = 3 };
 enum : int { kIndAlpha = 0x1, kIndCollect = 0x2 };
 
 size_t zpass_b2g_smem(int KT, int K, int T, int W, int mode);
+int zpass_b2g_width(int KT);   // CTA width (warps) of the fast path for a K class
 cudaError_t launch_zpass_b2g(const LaunchSet& ls, int KT, int W, int mode, int flags,
                              size_t smem);
 cudaError_t launch_zpass_u8(const LaunchSet& ls, int mode, int flags);

@@ -37,7 +37,7 @@ __device__ __forceinline__ void warp_slot_sums(double v, int G, double* s, int n
 // ---------------------------------------------------------------------------
 // Locus kernel
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
              int G, int stages) {
   __shared__ double sF[8 * kMaxPops];
@@ -60,32 +60,21 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
 
   // ---- P ------------------------------------------------------------------
   if ((stages & kLocP) && kvalid && na > 0) {
-    double lg[kMaxAlleles];
-    const int nac = na < kMaxAlleles ? na : kMaxAlleles;
-    if (na > kMaxAlleles) errb |= kErrBounds;
-    for (int a = 0; a < nac; a++) {
+    auto shape_of = [&](int a) {
       int n = 0;
       for (int cc = 0; cc < ch.cnt_chunks; cc++)
         n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
-      double shape;
       if (ch.freqscorr)
-        shape = ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
-      else
-        shape = ch.lambda[k] + (double)n;
-      lg[a] = log_gamma_draw(shape, (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
-    }
-    double M = lg[0];
-    for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
-    double S = 0.0;
-    for (int a = 0; a < nac; a++) S += exp(lg[a] - M);
-    const double ls = M + log(S);
-    for (int a = 0; a < nac; a++) {
+        return ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
+      return ch.lambda[k] + (double)n;
+    };
+    auto emit = [&](int a, double lg, double ls, int nac) {
       double lp, p;
       if (ls < kLogUnderflo) {
         p = 1.0 / (double)nac;
         lp = -log((double)nac);
       } else {
-        lp = lg[a] - ls;
+        lp = lg - ls;
         p = exp(lp);
       }
       const float pf = (float)p;
@@ -93,6 +82,31 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
       ch.logP[base + a] = (float)lp;
       if (collect) ch.PSum[base + a] += (double)pf;
       if (!(pf == pf)) errb |= kErrNaN;
+    };
+    if (na <= 2) {
+      // biallelic (and monomorphic) loci stay in registers
+      const double lg0 = log_gamma_draw(shape_of(0), (uint32_t)base, (uint32_t)rep, kSP, key, &errb);
+      const double lg1 = na > 1 ? log_gamma_draw(shape_of(1), (uint32_t)(base + 1), (uint32_t)rep,
+                                                 kSP, key, &errb)
+                                : -INFINITY;
+      const double M = (na > 1 && lg1 > lg0) ? lg1 : lg0;
+      double S = exp(lg0 - M);
+      if (na > 1) S += exp(lg1 - M);
+      const double ls = M + log(S);
+      emit(0, lg0, ls, na);
+      if (na > 1) emit(1, lg1, ls, na);
+    } else {
+      double lg[kMaxAlleles];
+      const int nac = na < kMaxAlleles ? na : kMaxAlleles;
+      if (na > kMaxAlleles) errb |= kErrBounds;
+      for (int a = 0; a < nac; a++)
+        lg[a] = log_gamma_draw(shape_of(a), (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+      double M = lg[0];
+      for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
+      double S = 0.0;
+      for (int a = 0; a < nac; a++) S += exp(lg[a] - M);
+      const double ls = M + log(S);
+      for (int a = 0; a < nac; a++) emit(a, lg[a], ls, nac);
     }
   }
 
@@ -115,10 +129,10 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         const double frac = (1.0 - ch.F[k]) / ch.F[k];
         const double lp1 = (double)ch.logP[base + a1];
         const double lp2 = (double)ch.logP[base + a2];
-        double s = lanczos_lgamma(frac * e1);
-        s += lanczos_lgamma(frac * e2);
-        s -= lanczos_lgamma(frac * (e1 + d));
-        s -= lanczos_lgamma(frac * (e2 - d));
+        double s = lanczos_lgamma_fast(frac * e1);
+        s += lanczos_lgamma_fast(frac * e2);
+        s -= lanczos_lgamma_fast(frac * (e1 + d));
+        s -= lanczos_lgamma_fast(frac * (e2 - d));
         s += frac * d * lp1;
         s -= frac * d * lp2;
         t = s;
@@ -154,7 +168,7 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         for (int a = 0; a < na; a++) {
           const double e = ch.eps[(size_t)l * A + a];
           const double lp = (double)ch.logP[base + a];
-          dsum += (nfr - ofr) * e * lp - (lanczos_lgamma(nfr * e) - lanczos_lgamma(ofr * e));
+          dsum += (nfr - ofr) * e * lp - (lanczos_lgamma_fast(nfr * e) - lanczos_lgamma_fast(ofr * e));
         }
       }
     }
@@ -193,7 +207,7 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
           double lpd = (m * m / (sd * sd) - 1) * log(nf / oldf) + (oldf - nf) * m / (sd * sd);
           const double nfr = (1.0 - nf) / nf, ofr = (1.0 - oldf) / oldf;
           const int npops = ch.onefst ? K : 1;
-          lpd += (double)ch.Leff * npops * (lanczos_lgamma(nfr) - lanczos_lgamma(ofr)) + sTot[jj];
+          lpd += (double)ch.Leff * npops * (lanczos_lgamma_fast(nfr) - lanczos_lgamma_fast(ofr)) + sTot[jj];
           ch.stats[kStFstLpd + jj] = lpd;
           bool acc = lpd >= 0.0;
           if (!acc) acc = rnd31(philox_s((uint32_t)jj, 1, (uint32_t)rep, kSFst, key)) < exp(lpd);
@@ -352,15 +366,15 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
               double sumalphas = 0.0;
               for (int q = 0; q < K; q++) sumalphas += alpha[q];
               logprobdiff -= (alpha[pop] - 1.0) * sTot[pop] +
-                             (lanczos_lgamma(sumalphas) - lanczos_lgamma(alpha[pop])) * N;
+                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(alpha[pop])) * N;
               sumalphas += newalpha - alpha[pop];
               logprobdiff += (newalpha - 1.0) * sTot[pop] +
-                             (lanczos_lgamma(sumalphas) - lanczos_lgamma(newalpha)) * N;
+                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(newalpha)) * N;
             } else {
               logprobdiff += (newalpha - 1.0) * T +
-                             (lanczos_lgamma(K * newalpha) - K * lanczos_lgamma(newalpha)) * N;
+                             (lanczos_lgamma_fast(K * newalpha) - K * lanczos_lgamma_fast(newalpha)) * N;
               logprobdiff -= (alpha[pop] - 1.0) * T +
-                             (lanczos_lgamma(K * alpha[pop]) - K * lanczos_lgamma(alpha[pop])) * N;
+                             (lanczos_lgamma_fast(K * alpha[pop]) - K * lanczos_lgamma_fast(alpha[pop])) * N;
             }
             ch.stats[kStAlphaLpd + pop] = logprobdiff;
             const double unifrv = rnd31(philox_s((uint32_t)pop, 1, (uint32_t)rep, kSAlpha, key));

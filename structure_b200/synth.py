@@ -88,7 +88,7 @@ def microsat(N=200, L=100, K=3, amin=2, amax=10, qalpha=0.5, missing=0.05, seed=
     return dict(geno_raw=geno, geno=rec, numalleles=na, Q=Q, K=K)
 
 
-def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=4096,
+def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=1024,
                want_int32=True):
     """Configs 2/3/5: biallelic SNPs under the F model; whole genotypes missing.
     Genotype code g = copies of allele 1 (0,1,2; 3 = missing).  At each locus the
@@ -101,6 +101,7 @@ def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=4096,
     Q = rng.dirichlet(np.full(K, qalpha), size=N)
     cq = np.cumsum(Q, axis=1)
     cq[:, -1] = 1.0
+    cq32 = cq.astype(np.float32)
     geno = np.empty((N, 2, L), np.int32) if want_int32 else None
     numalleles = np.zeros(L, np.int32)
     wpr = (N + 15) // 16
@@ -111,14 +112,14 @@ def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=4096,
         n = l1 - l0
         p = np.clip(rng.beta(p_beta[0], p_beta[1], size=n), 1e-4, 1 - 1e-4)
         P1 = rng.beta(p[None, :] * fr[:, None], (1 - p[None, :]) * fr[:, None])  # [K, n]
-        u = rng.random((N, 2, n))
+        u = rng.random((N, 2, n), dtype=np.float32)
         z = np.zeros((N, 2, n), np.int8)
         for k in range(K - 1):
-            z += (u > cq[:, k][:, None, None]).astype(np.int8)
-        v = rng.random((N, 2, n))
-        a = (v < P1[z, np.arange(n)[None, None, :]]).astype(np.int8)
-        g = a.sum(axis=1).astype(np.uint8)                    # [N, n]
-        g[rng.random((N, n)) < missing] = 3
+            z += u > cq32[:, k][:, None, None]
+        v = rng.random((N, 2, n), dtype=np.float32)
+        a = v < P1.astype(np.float32)[z, np.arange(n)[None, None, :]]
+        g = a.sum(axis=1, dtype=np.uint8)                     # [N, n]
+        g[rng.random((N, n), dtype=np.float32) < missing] = 3
         ok = g != 3
         first = np.where(ok.any(0), ok.argmax(0), 0)
         flip = ok.any(0) & (g[first, np.arange(n)] == 2)
@@ -152,6 +153,21 @@ def pack_codes(g):
     for j in range(16):
         w |= gp[:, j, :] << np.uint32(2 * j)
     return np.ascontiguousarray(w.T)
+
+
+def unpack_int32(packed, N, l0=0, l1=None):
+    """Inverse of pack_codes for loci [l0, l1): reference-layout int32 geno
+    [N][2][l1-l0] with -9 for missing."""
+    l1 = packed.shape[0] if l1 is None else l1
+    w = packed[l0:l1]                                      # [n, wpr]
+    j = np.arange(N)
+    g = (w[:, j >> 4] >> (2 * (j & 15)).astype(np.uint32)) & np.uint32(3)   # [n, N]
+    g = g.T.astype(np.int8)
+    lo = (g == 2).astype(np.int32)
+    hi = (g >= 1).astype(np.int32)
+    lo[g == 3] = MISSING
+    hi[g == 3] = MISSING
+    return np.ascontiguousarray(np.stack([lo, hi], axis=1))
 
 
 def repack_from_int32(geno):

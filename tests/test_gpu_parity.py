@@ -117,6 +117,26 @@ def test_updatez_f32_philox_bitexact(ctx, orc, layout):
     c.close(); d.close()
 
 
+def test_updatez_fast_path_many_draws_bitexact(ctx, orc):
+    """1.6e7 copies: ties u*T == cumsum_k occur a few times per pass; the fast
+    path must resolve them exactly as the reference's `r <= cumsum` does."""
+    geno, na, _ = _snp(N=1024, L=8192, K=3, seed=31)
+    N, _, L = geno.shape
+    K = 3
+    rng = np.random.default_rng(31)
+    Q, P = _rand_state(rng, N, L, K, na)
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    for rep in (1, 2):
+        c.set(api.F_REP, np.array([rep], np.int32))
+        c.UpdateZ()
+        zo = orc.zupdate_f32(geno, Q, P, SEED, rep)
+        zd = _zdev(c)
+        assert (zd == zo).all(), f"{(zd != zo).sum()} copies differ at rep {rep}"
+    c.close(); d.close()
+
+
 @pytest.mark.parametrize("K", [1, 2, 5, 7, 13])
 def test_fast_path_padded_k_bitexact(ctx, orc, K):
     geno, na, _ = _snp(N=130, L=300, K=3, seed=K)
