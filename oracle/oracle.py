@@ -310,6 +310,8 @@ class RefLib:
         lib.FPriorDiff.argtypes = [_cd, _cd]
         lib.FPriorDiff.restype = _cd
         lib.UpdateAlpha.argtypes = [_f64p, _f64p, C.c_void_p, _ci]
+        lib.UpdateP.argtypes = [_f64p, _f64p, _f64p, _i32p, _i32p, _i32p, _f64p, C.c_void_p, _f64p]
+        lib.stref_guard_hits.restype = C.c_long
         lib.UpdateEpsilon.argtypes = [_f64p, _f64p, _f64p, _i32p, _cd]
         lib.UpdateFst.argtypes = [_f64p, _f64p, _f64p, _i32p]
         lib.InitializeZ.argtypes = [_i32p, C.c_void_p, _i32p]

@@ -1,0 +1,97 @@
+"""Host-side checks that need no GPU: the C ABI library exports everything
+include/stgpu.h declares, the multi-rank timing plumbing over gloo, and the
+reference CPU chain driver."""
+import os
+import re
+import socket
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "stgpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(st_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_cabi_library_exports_every_declared_symbol():
+    import ctypes
+    from structure_b200 import api
+    lib = ctypes.CDLL(api.LIB_PATH)
+    names = _declared()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.st_version() == 10000
+
+
+def test_cabi_reports_no_device_without_gpu():
+    import torch
+    from structure_b200 import api
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.StError) as e:
+        api.Context(0)
+    assert e.value.code == api.ST_ERR_NODEVICE
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    from structure_b200 import dist as sd
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    r, w, lr = sd.rank_env()
+    seeds = sd.chain_seeds(r, 20)
+    ms = 10.0 + 5.0 * r                       # per-rank device time
+    mx = sd.max_over_ranks(ms)
+    tot = sd.sum_over_ranks(len(seeds))
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((r, w, seeds, mx, tot))
+
+
+def test_multirank_timing_and_seeds_gloo():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(30)
+    assert [r[0] for r in res] == [0, 1] and all(r[1] == 2 for r in res)
+    assert all(r[3] == 15.0 for r in res)           # max over ranks
+    assert all(r[4] == 40.0 for r in res)           # chains over ranks
+    assert not set(res[0][2]) & set(res[1][2])      # disjoint chain seeds
+
+
+def test_reference_chain_driver_runs(ref):
+    """The reference's CPU sweep (structure.c order) on a small data set."""
+    from structure_b200 import synth
+    from oracle.oracle import ref_model
+    d = synth.microsat(N=30, L=12, K=2, seed=3)
+    m = ref_model(N=30, L=12, K=2, maxalleles=int(d["numalleles"].max()), metrofreq=5,
+                  burnin=3, numreps=6, freqscorr=1, fpriormean=0.05, fpriorsd=0.05)
+    ch = ref.chain_new(m, d["geno_raw"], seed=11)
+    ref.lib.stref_chain_sweeps(ch, 9)
+    v = ref.chain_view(ch, 30, 12, 2)
+    ref.lib.stref_chain_free(ch)
+    assert v["rep"] == 9 and np.isfinite(v["sumlikes"]) and v["sumlikes"] < 0
+    np.testing.assert_allclose(v["QSum"].sum(1), 6.0, rtol=1e-9)
+    assert (v["Geno"] == d["geno"]).all()      # the reference's recoding == synth.recode

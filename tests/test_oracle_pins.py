@@ -1,0 +1,302 @@
+"""Pins of the oracle restatement (oracle/st_oracle.c) against the reference's
+own CPU functions (pmelsted/structure src/*.c, built into oracle/_ref by
+oracle/Makefile and driven with controlled rand()/RNormal streams).
+
+These run on the CPU.  Deterministic pieces must agree exactly (or to the last
+few ulps where the summation order differs); Metropolis updates fed the same
+normals and uniforms must make the same moves; the Dirichlet samplers differ in
+algorithm (reference: Ripley/Cheng-Feast gamma; build: Marsaglia-Tsang) and are
+compared in distribution.
+"""
+import numpy as np
+import pytest
+
+from structure_b200 import synth
+from oracle.oracle import S_ALPHA, S_EPS, S_FST, S_INITZ, rnd_words
+
+KEY = 0x1234ABCD5678
+
+
+def _microsat(N, L, K, seed):
+    d = synth.microsat(N=N, L=L, K=K, seed=seed)
+    return d["geno"], d["numalleles"]
+
+
+def _snp(N, L, K, seed):
+    d = synth.snp_fmodel(N, L, K, np.linspace(0.05, 0.25, K), 0.4, 0.03, seed)
+    return d["geno"], d["numalleles"]
+
+
+def _state(rng, N, L, K, na, qa=0.7):
+    A = int(max(1, na.max()))
+    Q = rng.dirichlet(np.full(K, qa), N)
+    P = np.zeros((L, K, A))
+    for l in range(L):
+        if na[l] > 0:
+            P[l, :, :na[l]] = rng.dirichlet(np.ones(na[l]), K)
+    return Q.astype(np.float32).astype(np.float64), P.astype(np.float32).astype(np.float64)
+
+
+def test_philox_known_answers(orc):
+    # Random123 philox4x32_10 known-answer vectors
+    assert [hex(x) for x in orc.philox([0, 0, 0, 0], 0)] == \
+        ["0x6627e8d5", "0xe169c58d", "0xbc57ac4c", "0x9b00dbd8"]
+    assert [hex(x) for x in orc.philox([0xffffffff] * 4, 0xffffffffffffffff)] == \
+        ["0x408f276d", "0x41c83b0e", "0xa20bc7c6", "0x6d5451fd"]
+    assert [hex(x) for x in orc.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
+                                       0x299f31d0a4093822)] == \
+        ["0xd16cfe09", "0x94fdcceb", "0x5001e420", "0x24126ea1"]
+
+
+def test_lgamma_matches_reference_mylgamma(orc, ref):
+    zs = np.concatenate([np.linspace(1e-4, 8, 400), np.logspace(-4, 6, 400)])
+    for z in zs:
+        assert orc.lgamma(z) == ref.lib.mylgamma(z)
+
+
+@pytest.mark.parametrize("K,seed", [(1, 1), (2, 2), (3, 3), (6, 4)])
+def test_updatez_f64_matches_reference(orc, ref, K, seed):
+    geno, na = _microsat(40, 30, 3, seed)
+    N, _, L = geno.shape
+    rng = np.random.default_rng(seed)
+    Q, P = _state(rng, N, L, K, na)
+    u = rng.random(N * L * 2)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=P.shape[2])
+    zr = np.zeros_like(geno)
+    ref.lib.UpdateZ(zr, Q, P, geno.copy(), u)
+    zo, flags = orc.zupdate_f64_injected(geno, Q, P, u)
+    assert (zo == zr).all() and flags == 0
+
+
+@pytest.mark.parametrize("pfonly", [0, 1])
+def test_counts_match_reference(orc, ref, pfonly):
+    geno, na = _microsat(50, 25, 3, 9)
+    N, _, L = geno.shape
+    K, A = 4, int(na.max())
+    rng = np.random.default_rng(9)
+    Z = rng.integers(0, K, size=geno.shape).astype(np.int32)
+    Z[geno < 0] = -9
+    pf = (rng.random(N) < 0.5).astype(np.int32)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, pfrompopflagonly=pfonly)
+    nr = np.zeros(L * K * A, np.int32)
+    ref.lib.GetNumFromPops(nr, geno.copy(), Z, na.astype(np.int32), ref.individuals(N, pf))
+    no, mo = orc.counts(geno, Z, K, A, popflags=pf, pfrompopflagonly=pfonly)
+    assert (nr.reshape(L, K, A) == no).all()
+    tmp = np.zeros(K, np.int32)
+    for i in range(N):
+        ref.lib.GetNumLociPop(tmp, Z, i)
+        assert (tmp == mo[i]).all()
+
+
+def test_initializez_matches_reference(orc, ref):
+    geno, na = _microsat(30, 20, 3, 4)
+    N, _, L = geno.shape
+    K = 5
+    zi = orc.init_z(geno, K, KEY)
+    vals = []
+    for i in range(N):
+        for line in range(2):
+            for l in range(L):
+                if geno[i, line, l] >= 0:
+                    w = orc.philox([l, i >> 1, 0, S_INITZ << 24], KEY)
+                    vals.append(int(w[2 * (i & 1) + line]) >> 1)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=int(na.max()))
+    ref.rand_queue(vals)
+    zr = np.zeros_like(geno)
+    ref.lib.InitializeZ(geno.copy(), ref.individuals(N), zr)
+    ref.rand_queue(None)
+    assert (zr == zi).all()
+
+
+@pytest.mark.parametrize("freqscorr", [0, 1])
+def test_initfreqpriors_matches_reference(orc, ref, freqscorr):
+    geno, na = _microsat(30, 20, 3, 5)
+    N, _, L = geno.shape
+    K, A = 3, int(na.max())
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=freqscorr, fpriormean=0.02,
+                    lambda_=1.0)
+    er = np.zeros(L * A)
+    fr = np.zeros(K)
+    ref.lib.InitFreqPriors(er, fr, geno.copy(), na.astype(np.int32))
+    eo, fo = orc.init_eps(geno, na, A, freqscorr, 1.0, 0.02, K)
+    np.testing.assert_array_equal(eo.reshape(-1)[np.arange(L * A) % A < np.repeat(na, A)],
+                                  er[np.arange(L * A) % A < np.repeat(na, A)])
+    np.testing.assert_array_equal(fo, fr)
+
+
+def test_calclike_and_metro_logdiff_match_reference(orc, ref):
+    geno, na = _snp(60, 200, 3, 6)
+    N, _, L = geno.shape
+    K = 4
+    rng = np.random.default_rng(6)
+    Q, P = _state(rng, N, L, K, na)
+    T, _ = _state(rng, N, L, K, na)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=P.shape[2])
+    lr = ref.lib.CalcLike(geno.copy(), None, Q, P, None, None, None)
+    assert orc.calc_like(geno, Q, P) == lr
+    ld = orc.metro_logdiff(geno, Q.astype(np.float32), T.astype(np.float32), P.astype(np.float32))
+    for i in range(N):
+        r = ref.lib.CalcLikeIndDiff(geno.copy(), None, T[i].copy(), Q[i].copy(), P, i, None)
+        assert abs(r - ld[i]) <= 1e-9 * max(1.0, abs(r))
+
+
+def test_estlogprob_matches_reference(orc, ref):
+    for s, ss, n in [(-1000.0, 1e6 + 50.0, 1), (-5000.0, 2.5e6 + 900, 10), (-1.2e8, 7.2e15, 500)]:
+        assert orc.est_logprob(s, ss, n) == ref.lib.EstLogProb(s, ss, n) or n == 1
+
+
+@pytest.mark.parametrize("popalphas,unif", [(0, 1), (1, 1), (0, 0), (1, 0)])
+def test_updatealpha_matches_reference(orc, ref, popalphas, unif):
+    N, K = 150, 4
+    rng = np.random.default_rng(popalphas * 2 + unif)
+    Q = rng.dirichlet(np.full(K, 0.6), N).astype(np.float32)
+    logQ = np.log(Q.astype(np.float64)).astype(np.float32)
+    Qd = np.exp(logQ.astype(np.float64))          # so that log(Q) == logQ as the oracle sees it
+    alpha = np.array([0.7, 0.9, 0.5, 1.3])[:K] if popalphas else np.full(K, 0.8)
+    S, T = orc.alpha_sums(logQ)
+    for rep in range(8):
+        a_o, lpd = orc.update_alpha(N, S, T, alpha, KEY, rep, popalphas, unif, 10.0, 0.2,
+                                    2.0, 0.5)
+        nal = K if popalphas else 1
+        normals = [orc.normal(p, rep, S_ALPHA, KEY) for p in range(nal)]
+        rands = []
+        for p in range(nal):
+            newa = alpha[p] + 0.2 * normals[p]
+            if newa > 0 and (newa < 10.0 or not unif):
+                rands += rnd_words(orc.philox([p, 1, rep, S_ALPHA << 24], KEY))
+        ref.set_globals(N=N, L=1, K=K, maxalleles=2, popalphas=popalphas, unifprioralpha=unif,
+                        alphapropsd=0.2, alphamax=10.0, alphapriora=2.0, alphapriorb=0.5)
+        ar = alpha.copy()
+        ref.normal_queue(normals)
+        ref.rand_queue(rands)
+        ref.lib.UpdateAlpha(Qd.copy(), ar, ref.individuals(N), rep)
+        ref.rand_queue(None)
+        ref.normal_queue(None)
+        np.testing.assert_allclose(ar, a_o, rtol=1e-13)
+        alpha = a_o
+
+
+@pytest.mark.parametrize("lam", [1.0, 0.5])
+def test_updateepsilon_matches_reference(orc, ref, lam):
+    geno, na = _microsat(60, 40, 3, 12)
+    N, _, L = geno.shape
+    K, A = 3, int(na.max())
+    rng = np.random.default_rng(12)
+    _, P = _state(rng, N, L, K, na)
+    logP = np.where(P > 0, np.log(np.maximum(P, 1e-300)), 0).astype(np.float32)
+    Pd = np.where(P > 0, np.exp(logP.astype(np.float64)), 0)
+    eps, F = orc.init_eps(geno, na, A, 1, 1.0, 0.1, K)
+    F = np.array([0.05, 0.2, 0.4])
+    inv = float(N) ** -0.5
+    for rep in range(5):
+        e_o, acc = orc.update_eps(na, logP, eps, F, lam, inv, KEY, rep)
+        vals = []
+        for l in range(L):
+            if na[l] > 1:
+                w = orc.philox([l, 0, rep, S_EPS << 24], KEY)
+                a1 = int(((int(w[0]) >> 1) / 2147483648.0) * na[l])
+                a2 = int(((int(w[1]) >> 1) / 2147483648.0) * (na[l] - 1))
+                a2 = a2 + 1 if a2 >= a1 else a2
+                dl = ((int(w[2]) >> 1) / 2147483648.0) * inv
+                vals += [int(w[0]) >> 1, int(w[1]) >> 1, int(w[2]) >> 1]
+                if eps[l, a1] + dl < 1.0 and eps[l, a2] - dl > 0.0:
+                    vals += rnd_words(orc.philox([l, 1, rep, S_EPS << 24], KEY))
+        ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=1)
+        er = eps.copy()
+        ref.rand_queue(vals)
+        ref.lib.UpdateEpsilon(Pd, er, F.copy(), na.astype(np.int32), lam)
+        assert ref.lib.stref_rand_overrun() == 0
+        ref.rand_queue(None)
+        np.testing.assert_allclose(er, e_o, rtol=1e-12, atol=1e-15)
+        assert acc.sum() > 0
+        eps = e_o
+
+
+@pytest.mark.parametrize("onefst", [0, 1])
+def test_updatefst_matches_reference(orc, ref, onefst):
+    geno, na = _snp(80, 150, 3, 13)
+    N, _, L = geno.shape
+    K, A = 3, 2
+    rng = np.random.default_rng(13)
+    _, P = _state(rng, N, L, K, na)
+    logP = np.where(P > 0, np.log(np.maximum(P, 1e-300)), 0).astype(np.float32)
+    Pd = np.where(P > 0, np.exp(logP.astype(np.float64)), 0)
+    eps, _ = orc.init_eps(geno, na, A, 1, 1.0, 0.1, K)
+    F = np.array([0.05, 0.2, 0.4]) if not onefst else np.full(K, 0.15)
+    Leff = int((na > 0).sum())
+    for rep in range(6):
+        nf, diff = orc.fst_diffs(na, logP, eps, F, onefst, 0.05, KEY, rep)
+        F_o, lpd = orc.update_fst(F, onefst, 0.1, 0.05, Leff, diff, nf, KEY, rep)
+        # reference: FlikeFreqs differences agree; UpdateFst makes the same move
+        ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=1, onefst=onefst,
+                        fpriormean=0.1, fpriorsd=0.05)
+        numfst = 1 if onefst else K
+        for j in range(numfst):
+            if not (0 < nf[j] < 1):
+                continue
+            pops = range(K) if onefst else [j]
+            dr = sum(ref.lib.FlikeFreqs(nf[j], eps.reshape(-1).copy(), Pd.reshape(-1).copy(),
+                                        na.astype(np.int32), p) -
+                     ref.lib.FlikeFreqs(F[j], eps.reshape(-1).copy(), Pd.reshape(-1).copy(),
+                                        na.astype(np.int32), p) for p in pops)
+            npops = K if onefst else 1
+            do = diff[j] + Leff * npops * (orc.lgamma((1 - nf[j]) / nf[j]) - orc.lgamma((1 - F[j]) / F[j]))
+            assert abs(dr - do) <= 1e-8 * max(1.0, abs(dr))
+        normals = [orc.normal(j, rep, S_FST, KEY) for j in range(numfst)]
+        rands = []
+        for j in range(numfst):
+            if 0 < nf[j] < 1 and lpd[j] < 0:
+                rands += rnd_words(orc.philox([j, 1, rep, S_FST << 24], KEY))
+        Fr = F.copy()
+        ref.normal_queue(normals)
+        ref.rand_queue(rands)
+        ref.lib.UpdateFst(eps.reshape(-1).copy(), Fr, Pd.reshape(-1).copy(), na.astype(np.int32))
+        ref.rand_queue(None)
+        ref.normal_queue(None)
+        np.testing.assert_allclose(Fr, F_o, rtol=1e-14)
+        F = F_o
+
+
+def test_dirichlet_p_matches_reference_in_distribution(orc, ref):
+    """Same posterior Dir(lambda + n) from the reference's array-fed UpdateP
+    (Ripley / Cheng-Feast gamma) and the oracle's Marsaglia-Tsang draws."""
+    L, K, A = 400, 2, 3
+    rng = np.random.default_rng(21)
+    n = rng.integers(0, 6, size=(L, K, A)).astype(np.int32)
+    n[:, 0, :] = [0, 2, 7]
+    na = np.full(L, A, np.int32)
+    lam = np.full(K, 0.7)
+    eps = np.zeros((L, A))
+    F = np.full(K, 0.5)
+    draws_o, draws_r = [], []
+    # reference UpdateP counts from Z itself: a genotype table that reproduces n
+    for rep in range(20):
+        Po, _, err = orc.update_p(na, n, 0, eps, F, lam, KEY, rep)
+        assert err == 0
+        draws_o.append(Po.astype(np.float64))
+    N = int(n.sum(axis=(1, 2)).max() // 2 + 2)
+    geno = np.full((N, 2, L), -9, np.int32)
+    Z = np.full((N, 2, L), -9, np.int32)
+    for l in range(L):
+        c = 0
+        for k in range(K):
+            for a in range(A):
+                for _ in range(n[l, k, a]):
+                    geno[c // 2, c % 2, l] = a
+                    Z[c // 2, c % 2, l] = k
+                    c += 1
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=0, lambda_=0.7)
+    ind = ref.individuals(N)
+    for rep in range(20):
+        u = rng.random(L * K * A * 64)
+        P = np.zeros(L * K * A)
+        ref.lib.UpdateP(P, eps.reshape(-1).copy(), F.copy(), na, geno, Z, lam.copy(), ind, u)
+        draws_r.append(P.reshape(L, K, A))
+    do = np.stack(draws_o)[:, :, 0, :].reshape(-1, A)
+    dr = np.stack(draws_r)[:, :, 0, :].reshape(-1, A)
+    alpha = 0.7 + np.array([0, 2, 7])
+    mean = alpha / alpha.sum()
+    var = mean * (1 - mean) / (alpha.sum() + 1)
+    for x in (do, dr):
+        np.testing.assert_allclose(x.mean(0), mean, atol=4 * np.sqrt(var / len(x)).max())
+        np.testing.assert_allclose(x.var(0), var, rtol=0.15)
