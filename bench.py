@@ -54,6 +54,9 @@ def make_data():
 # ---------------------------------------------------------------------------
 def _ref_worker(q, path, N, L_slice, seed, core):
     try:
+        # the reference prints progress on stdout; keep the bench's stdout to one line
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
         if core is not None:
             os.sched_setaffinity(0, {core})
         from oracle.oracle import RefLib, ref_model

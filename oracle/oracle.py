@@ -57,6 +57,9 @@ class Oracle:
     def __init__(self):
         lib = self.lib = _load(os.path.join(HERE, "liboracle.so"))
         lib.orc_philox.argtypes = [_u32p, _cu64, _u32p]
+        lib.orc_stream.argtypes = [_cu32, _cu32, _cu32, _cu32, _cu64, _u32p]
+        lib.orc_seed32.argtypes = [_cu64]
+        lib.orc_seed32.restype = _cu32
         lib.orc_lgamma.argtypes = [_cd]
         lib.orc_lgamma.restype = _cd
         lib.orc_loggamma.argtypes = [_cd, _cu32, _cu32, _cu32, _cu64, C.POINTER(_ci)]
@@ -91,6 +94,12 @@ class Oracle:
     def philox(self, ctr, key):
         out = np.zeros(4, np.uint32)
         self.lib.orc_philox(np.ascontiguousarray(ctr, np.uint32), key, out)
+        return out
+
+    def stream(self, a, b, rep, stream, seed):
+        """Four words of block (a, b) of a chain's stream at a sweep."""
+        out = np.zeros(4, np.uint32)
+        self.lib.orc_stream(a, b, rep, stream, seed, out)
         return out
 
     def lgamma(self, z):

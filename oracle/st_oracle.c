@@ -8,7 +8,7 @@
  *
  * Reference = pmelsted/structure (STRUCTURE 2.3.4 CPU code under src/).
  * Random draws come from Philox4x32-10 counters (the device convention):
- *   key = chain seed, ctr = {index, sub-index, sweep, stream << 24}.
+ *   fixed key, ctr = {index, (stream << 24) | sub-index, sweep, seed32}.
  */
 #include "st_oracle.h"
 #include <math.h>
@@ -43,11 +43,32 @@ void orc_philox(const uint32_t ctr[4], uint64_t key, uint32_t out[4])
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
+/* Stream layout shared with the device: a fixed Philox key, and the counter
+ *   {a, (stream << 24) | (b & 0xFFFFFF), sweep, seed32},
+ * seed32 = low word of splitmix64(chain seed) (Steele, Lea & Flood 2014). */
+#define ORC_KEY0 0xA511E9B3u
+#define ORC_KEY1 0x3C6EF372u
+
+uint32_t orc_seed32(uint64_t seed)
+{
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (uint32_t)z;
+}
+
+void orc_stream(uint32_t a, uint32_t b, uint32_t rep, uint32_t stream, uint64_t seed,
+                uint32_t out[4])
+{
+    uint32_t c[4] = {a, (stream << 24) | (b & 0xFFFFFFu), rep, orc_seed32(seed)};
+    orc_philox(c, ((uint64_t)ORC_KEY1 << 32) | ORC_KEY0, out);
+}
+
 static void philox4(uint32_t a, uint32_t b, uint32_t rep, uint32_t stream,
                     uint64_t key, uint32_t out[4])
 {
-    uint32_t c[4] = {a, b, rep, stream << 24};
-    orc_philox(c, key, out);
+    orc_stream(a, b, rep, stream, key, out);
 }
 
 double orc_u01(uint32_t hi, uint32_t lo)
@@ -99,7 +120,7 @@ double orc_lgamma(double z)
 /* Marsaglia & Tsang (2000) gamma, returned as log(draw).                    */
 /* Attempts come in pairs: block 2j gives two Box-Muller normals, block      */
 /* 2j+1 the two acceptance uniforms.  Shape < 1 uses G(a) = G(a+1) U^(1/a)   */
-/* with U from block 0xFFFFFFFF.                                             */
+/* with U from block 0xFFFFFF.                                               */
 /* ------------------------------------------------------------------------ */
 double orc_loggamma(double a, uint32_t e, uint32_t rep, uint32_t stream,
                     uint64_t key, int *err)
@@ -140,7 +161,7 @@ double orc_loggamma(double a, uint32_t e, uint32_t rep, uint32_t stream,
     }
     if (a < 1.0) {
         uint32_t w[4];
-        philox4(e, 0xFFFFFFFFu, rep, stream, key, w);
+        philox4(e, 0xFFFFFFu, rep, stream, key, w);
         lg += log(orc_u01(w[0], w[1])) / a;
     }
     return lg;

@@ -33,6 +33,10 @@ enum {
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
 void orc_philox(const uint32_t ctr[4], uint64_t key, uint32_t out[4]);
+/* The streams of one chain: fixed key, ctr = {a, stream<<24 | b, sweep, seed32}. */
+uint32_t orc_seed32(uint64_t seed);
+void orc_stream(uint32_t a, uint32_t b, uint32_t rep, uint32_t stream, uint64_t seed,
+                uint32_t out[4]);
 double orc_u01(uint32_t hi, uint32_t lo);      /* 52-bit uniform in (0,1) */
 double orc_rnd31_block(const uint32_t w[4]);  /* ran.c:152 rnd() on rand()=w>>1 */
 double orc_normal(uint32_t idx, uint32_t rep, uint32_t stream, uint64_t key);

@@ -568,7 +568,14 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   h.alphapriora = model->alphapriora; h.alphapriorb = model->alphapriorb;
   h.fpriormean = model->fpriormean; h.fpriorsd = model->fpriorsd;
   h.invsqrtnuminds = pow((double)N, -0.5);    // src/Updates/UpdateEpsilon.c:80
-  h.key = seed;
+  {
+    // splitmix64 (Steele, Lea & Flood 2014): seed32 = low word
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    h.key = (uint32_t)z;
+  }
   h.g2 = data->g2; h.g8 = data->g8; h.numalleles = data->numalleles; h.popflags = data->popflags;
 
   c->fast = data->layout == kLayoutB2G && model->precision == 0 && fast_kt(K) > 0;

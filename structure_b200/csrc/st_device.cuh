@@ -13,29 +13,31 @@
 
 namespace st {
 
-// Random123 Philox4x32-10.  key = chain seed; counter = {index, sub-index,
-// sweep, stream << 24}.
+// Random123 Philox4x32-10 with a fixed key, so the ten round keys are
+// compile-time immediates; a chain's identity is the counter word seed32.
+// Streams: counter = {a, (stream << 24) | (b & 0xFFFFFF), sweep, seed32},
+// seed32 = low word of splitmix64(chain seed).
 struct U4 { uint32_t x, y, z, w; };
 
-__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2,
-                                     uint32_t c3, uint64_t key) {
-  uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+constexpr uint32_t kPhiloxKey0 = 0xA511E9B3u, kPhiloxKey1 = 0x3C6EF372u;
+
+__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
 #pragma unroll
   for (int r = 0; r < 10; r++) {
+    const uint32_t k0 = kPhiloxKey0 + (uint32_t)r * 0x9E3779B9u;
+    const uint32_t k1 = kPhiloxKey1 + (uint32_t)r * 0xBB67AE85u;
     const uint64_t p0 = (uint64_t)0xD2511F53u * c0;   // one 32x32->64 multiply each
     const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
     const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
     const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
     c0 = n0; c1 = (uint32_t)p1; c2 = n2; c3 = (uint32_t)p0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
   }
   return U4{c0, c1, c2, c3};
 }
 
 __device__ __forceinline__ U4 philox_s(uint32_t a, uint32_t b, uint32_t rep,
-                                       uint32_t stream, uint64_t key) {
-  return philox(a, b, rep, stream << 24, key);
+                                       uint32_t stream, uint32_t seed32) {
+  return philox(a, (stream << 24) | (b & 0xFFFFFFu), rep, seed32);
 }
 
 // 52-bit uniform in (0,1).
@@ -62,7 +64,7 @@ constexpr double kTwoPi = 6.283185307179586;
 
 // Standard normal for MH proposals: Box-Muller on block {idx, 0, rep, stream}.
 __device__ __forceinline__ double normal_draw(uint32_t idx, uint32_t rep,
-                                              uint32_t stream, uint64_t key) {
+                                              uint32_t stream, uint32_t key) {
   U4 w = philox_s(idx, 0, rep, stream, key);
   double u1 = u01(w.x, w.y), u2 = u01(w.z, w.w);
   return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
@@ -109,10 +111,10 @@ __device__ __forceinline__ double lanczos_lgamma_fast(double z) {
 // log of a Gamma(a, 1) draw by Marsaglia & Tsang (2000), "A simple method for
 // generating gamma variables", ACM TOMS 26(3).  Attempts come in pairs: block
 // 2j yields two Box-Muller normals, block 2j+1 their acceptance uniforms.
-// For a < 1, G(a) = G(a+1) * U^(1/a) (U from block 0xFFFFFFFF), in logs so that
+// For a < 1, G(a) = G(a+1) * U^(1/a) (U from block 0xFFFFFF), in logs so that
 // tiny shapes never underflow.
 static __device__ __noinline__ double log_gamma_draw(double a, uint32_t e, uint32_t rep,
-                                                 uint32_t stream, uint64_t key,
+                                                 uint32_t stream, uint32_t key,
                                                  int* errbits) {
   double aa = a < 1.0 ? a + 1.0 : a;
   double d = aa - 1.0 / 3.0;
@@ -148,7 +150,7 @@ static __device__ __noinline__ double log_gamma_draw(double a, uint32_t e, uint3
     lg = log(d);
   }
   if (a < 1.0) {
-    U4 w = philox_s(e, 0xFFFFFFFFu, rep, stream, key);
+    U4 w = philox_s(e, 0xFFFFFFu, rep, stream, key);
     lg += log(u01(w.x, w.y)) / a;
   }
   return lg;

@@ -59,7 +59,7 @@ struct ChainDev {
   int computeprob, pfrompopflagonly, ancestdist, numboxes, metrofreq, burnin;
   double alphamax, alphapropsd, alphapriora, alphapriorb;
   double fpriormean, fpriorsd, invsqrtnuminds;
-  uint64_t key;
+  uint32_t key;             // seed32: low word of splitmix64(chain seed)
   // Z-pass tiling: T individuals per chunk, W warps, R locus blocks per CTA
   int tileT, tileW, tileR, nchunks, ngroups;
   // count partials currently held (producer's decomposition)

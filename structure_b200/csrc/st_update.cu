@@ -52,7 +52,7 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   const bool lvalid = l < L;
   const bool kvalid = lvalid && k < K;
   const int rep = *ch.rep;
-  const uint64_t key = ch.key;
+  const uint32_t key = ch.key;
   const bool collect = (stages & kLocCollect) && (rep + 1 > ch.burnin);
   const int na = lvalid ? ch.numalleles[l] : 0;
   const size_t base = ((size_t)(lvalid ? l : 0) * K + (k < K ? k : 0)) * A;
@@ -255,7 +255,7 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
   const bool ivalid = i < N;
   const bool kvalid = ivalid && k < K;
   const int rep = *ch.rep;
-  const uint64_t key = ch.key;
+  const uint32_t key = ch.key;
   const bool collect = (stages & kIndCollect) && (rep + 1 > ch.burnin);
   const size_t qi = (size_t)(ivalid ? i : 0) * K + (k < K ? k : 0);
   int errb = 0;

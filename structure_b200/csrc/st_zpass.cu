@@ -121,7 +121,7 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   const int nT16 = (nT + 15) & ~15;  // whole words; padding genotypes are "missing"
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rep = *ch.rep;
-  const uint64_t key = ch.key;
+  const uint32_t key = ch.key;
   const bool collect = rep + 1 > ch.burnin;
   const bool want_like = (MODE == kZLike) ||
       (MODE == kZNormal && ((flags & kZfLikeAlways) || ((flags & kZfLikeIfCollect) && collect)));
@@ -205,7 +205,7 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
         const int ib = i0 + row0;
         U4 r4;
         if (MODE == kZNormal || MODE == kZInit)
-          r4 = philox((uint32_t)l, (uint32_t)(ib >> 1), prep, stream << 24, key);
+          r4 = philox_s((uint32_t)l, (uint32_t)(ib >> 1), prep, stream, key);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int row = row0 + h;
@@ -486,8 +486,8 @@ zpass_u8_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, i
     const float* Pl = ch.P + (size_t)l * K * A;
     U4 r4 = {0, 0, 0, 0};
     if (!injected && (mode == kZNormal || mode == kZInit))
-      r4 = philox((uint32_t)l, (uint32_t)(i >> 1), mode == kZInit ? 0u : (uint32_t)rep,
-                  (mode == kZInit ? (uint32_t)kSInitZ : (uint32_t)kSZ) << 24, ch.key);
+      r4 = philox_s((uint32_t)l, (uint32_t)(i >> 1), mode == kZInit ? 0u : (uint32_t)rep,
+                    mode == kZInit ? (uint32_t)kSInitZ : (uint32_t)kSZ, ch.key);
     const uint32_t wsel[2] = {(i & 1) ? r4.z : r4.x, (i & 1) ? r4.w : r4.y};
     int taken = 0;
     double ld = 0.0;

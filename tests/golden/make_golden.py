@@ -55,7 +55,7 @@ def main():
         for line in range(2):
             for l in range(L):
                 if geno[i, line, l] >= 0:
-                    w = orc.philox([l, i >> 1, 0, S_INITZ << 24], KEY)
+                    w = orc.stream(l, i >> 1, 0, S_INITZ, KEY)
                     zi_vals.append(int(w[2 * (i & 1) + line]) >> 1)
     ref.rand_queue(zi_vals)
     Zi = np.zeros_like(geno)
@@ -76,7 +76,7 @@ def main():
     for p in range(Kq):
         na_ = alpha0[p] + 0.2 * normals[p]
         if 0 < na_ < 10.0:
-            rands += rnd_words(orc.philox([p, 1, 5, S_ALPHA << 24], KEY))
+            rands += rnd_words(orc.stream(p, 1, 5, S_ALPHA, KEY))
     ref.set_globals(N=Nq, L=1, K=Kq, maxalleles=2, popalphas=1, alphapropsd=0.2, alphamax=10.0)
     ar = alpha0.copy()
     ref.normal_queue(normals)
@@ -105,14 +105,14 @@ def main():
     vals = []
     for l in range(Le):
         if nae[l] > 1:
-            w = orc.philox([l, 0, 2, S_EPS << 24], KEY)
+            w = orc.stream(l, 0, 2, S_EPS, KEY)
             a1 = int(((int(w[0]) >> 1) / 2147483648.0) * nae[l])
             a2 = int(((int(w[1]) >> 1) / 2147483648.0) * (nae[l] - 1))
             a2 = a2 + 1 if a2 >= a1 else a2
             dl = ((int(w[2]) >> 1) / 2147483648.0) * inv
             vals += [int(w[0]) >> 1, int(w[1]) >> 1, int(w[2]) >> 1]
             if eps0[l, a1] + dl < 1.0 and eps0[l, a2] - dl > 0.0:
-                vals += rnd_words(orc.philox([l, 1, 2, S_EPS << 24], KEY))
+                vals += rnd_words(orc.stream(l, 1, 2, S_EPS, KEY))
     ref.set_globals(N=N, L=Le, K=Ke, maxalleles=Ae, freqscorr=1)
     er = eps0.copy()
     ref.rand_queue(vals)

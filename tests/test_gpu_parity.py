@@ -169,7 +169,7 @@ def test_initial_z_matches_reference_initializez(ctx, ref, orc, layout):
         for line in range(2):
             for l in range(L):
                 if geno[i, line, l] >= 0:
-                    w = orc.philox([l, i >> 1, 0, 1 << 24], SEED)
+                    w = orc.stream(l, i >> 1, 0, 1, SEED)
                     vals.append(int(w[2 * (i & 1) + line]) >> 1)
     ref.set_globals(N=N, L=L, K=K, maxalleles=2)
     ref.rand_queue(vals)
@@ -285,7 +285,7 @@ def test_updatealpha_matches_oracle_and_reference(ctx, orc, ref, popalphas):
         # reference UpdateAlpha with the same normals and uniforms
         nalph = K if popalphas else 1
         normals = [orc.normal(p, rep, S_ALPHA, SEED) for p in range(nalph)]
-        rands = [rnd_words(orc.philox([p, 1, rep, S_ALPHA << 24], SEED)) for p in range(nalph)]
+        rands = [rnd_words(orc.stream(p, 1, rep, S_ALPHA, SEED)) for p in range(nalph)]
         ref.set_globals(N=N, L=geno.shape[2], K=K, maxalleles=2, popalphas=popalphas,
                         alphapropsd=0.2, alphamax=10.0)
         ar = a_before.copy()
@@ -346,14 +346,14 @@ def test_updateeps_and_fst_match_oracle_and_reference(ctx, orc, ref):
     vals = []
     for l in range(L):
         if na[l] > 1:
-            w = orc.philox([l, 0, rep, S_EPS << 24], SEED)
+            w = orc.stream(l, 0, rep, S_EPS, SEED)
             a1 = int(((int(w[0]) >> 1) / 2147483648.0) * na[l])
             a2 = int(((int(w[1]) >> 1) / 2147483648.0) * (na[l] - 1))
             a2 = a2 + 1 if a2 >= a1 else a2
             dlt = ((int(w[2]) >> 1) / 2147483648.0) * inv
             vals += [int(w[0]) >> 1, int(w[1]) >> 1, int(w[2]) >> 1]
             if eps0[l, a1] + dlt < 1.0 and eps0[l, a2] - dlt > 0.0:
-                vals += rnd_words(orc.philox([l, 1, rep, S_EPS << 24], SEED))
+                vals += rnd_words(orc.stream(l, 1, rep, S_EPS, SEED))
     er = eps0.copy()
     ref.rand_queue(vals)
     ref.lib.UpdateEpsilon(Pr_for_eps, er, F0.copy(), na.astype(np.int32), 1.0)

@@ -98,7 +98,7 @@ def test_initializez_matches_reference(orc, ref):
         for line in range(2):
             for l in range(L):
                 if geno[i, line, l] >= 0:
-                    w = orc.philox([l, i >> 1, 0, S_INITZ << 24], KEY)
+                    w = orc.stream(l, i >> 1, 0, S_INITZ, KEY)
                     vals.append(int(w[2 * (i & 1) + line]) >> 1)
     ref.set_globals(N=N, L=L, K=K, maxalleles=int(na.max()))
     ref.rand_queue(vals)
@@ -163,7 +163,7 @@ def test_updatealpha_matches_reference(orc, ref, popalphas, unif):
         for p in range(nal):
             newa = alpha[p] + 0.2 * normals[p]
             if newa > 0 and (newa < 10.0 or not unif):
-                rands += rnd_words(orc.philox([p, 1, rep, S_ALPHA << 24], KEY))
+                rands += rnd_words(orc.stream(p, 1, rep, S_ALPHA, KEY))
         ref.set_globals(N=N, L=1, K=K, maxalleles=2, popalphas=popalphas, unifprioralpha=unif,
                         alphapropsd=0.2, alphamax=10.0, alphapriora=2.0, alphapriorb=0.5)
         ar = alpha.copy()
@@ -193,14 +193,14 @@ def test_updateepsilon_matches_reference(orc, ref, lam):
         vals = []
         for l in range(L):
             if na[l] > 1:
-                w = orc.philox([l, 0, rep, S_EPS << 24], KEY)
+                w = orc.stream(l, 0, rep, S_EPS, KEY)
                 a1 = int(((int(w[0]) >> 1) / 2147483648.0) * na[l])
                 a2 = int(((int(w[1]) >> 1) / 2147483648.0) * (na[l] - 1))
                 a2 = a2 + 1 if a2 >= a1 else a2
                 dl = ((int(w[2]) >> 1) / 2147483648.0) * inv
                 vals += [int(w[0]) >> 1, int(w[1]) >> 1, int(w[2]) >> 1]
                 if eps[l, a1] + dl < 1.0 and eps[l, a2] - dl > 0.0:
-                    vals += rnd_words(orc.philox([l, 1, rep, S_EPS << 24], KEY))
+                    vals += rnd_words(orc.stream(l, 1, rep, S_EPS, KEY))
         ref.set_globals(N=N, L=L, K=K, maxalleles=A, freqscorr=1)
         er = eps.copy()
         ref.rand_queue(vals)
@@ -246,7 +246,7 @@ def test_updatefst_matches_reference(orc, ref, onefst):
         rands = []
         for j in range(numfst):
             if 0 < nf[j] < 1 and lpd[j] < 0:
-                rands += rnd_words(orc.philox([j, 1, rep, S_FST << 24], KEY))
+                rands += rnd_words(orc.stream(j, 1, rep, S_FST, KEY))
         Fr = F.copy()
         ref.normal_queue(normals)
         ref.rand_queue(rands)
