@@ -1,0 +1,455 @@
+// st_zpass_fast.cuh -- the biallelic fast path of the data pass (templates).
+// Instantiated per K class in st_zpass_k*.cu so the classes compile in
+// parallel; st_zpass.cu holds the dispatcher and the generic path.
+//
+// Fast path (biallelic, 2 bits per genotype, locus-major rows):
+//   CTA = W warps; lane = one locus; each warp walks the T individuals of its
+//   chunk, 16 genotypes per 32-bit word.  P[l][k][0..1] lives in a per-lane
+//   shared-memory table, Q rows of the chunk in shared memory (broadcast
+//   reads).  n[l][k][a] is a lane-private shared-memory histogram (lane-minor,
+//   conflict-free); m[i][k] is reduced across the warp's 32 loci with
+//   redux.sync on 7-bit packed fields.  Counts leave as per-CTA partials
+//   (plain stores, no global atomics): npart[chunk][k][a][l] and
+//   mpart[group][i][k], summed by the consumers.
+#pragma once
+#include "st_device.cuh"
+#include "st_kernels.h"
+
+namespace st {
+namespace zfast {
+
+
+constexpr float kLikeTinyF = 1e-30f;
+
+// Deterministic block sum of one double per thread (fixed tree order).
+__device__ __forceinline__ double block_sum_d(double v, double* sred) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sred[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; w++) s += sred[w];
+  }
+  return s;  // valid in thread 0
+}
+
+// Last CTA of a chain: sum the per-CTA ln-likelihood partials in order and
+// fold them into the chain's stats.
+static __device__ void finish_like(ChainDev& ch, int ntiles, bool collect, double* sred) {
+  double v = 0.0;
+  for (int j = threadIdx.x; j < ntiles; j += blockDim.x) v += ch.likepart[j];
+  double s = block_sum_d(v, sred);
+  if (threadIdx.x == 0) {
+    ch.stats[kStLike] = s;
+    if (collect) {
+      ch.stats[kStSumLikes] += s;
+      ch.stats[kStSumSq] += s * s;
+      ch.stats[kStNLike] += 1.0;
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fast path
+// ---------------------------------------------------------------------------
+// Shared-memory layout of one CTA (byte offsets; every piece 16-aligned).
+struct ZLayout {
+  size_t q2, t2, x, ld, inc, m, n, total;
+};
+
+__host__ __device__ inline size_t zalign16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+__host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int mode) {
+  const bool useP = (mode == kZNormal || mode == kZMetro || mode == kZLike);
+  const bool counts = (mode == kZNormal || mode == kZInit || mode == kZRecount);
+  const int KT2 = (KT + 1) & ~1;
+  ZLayout z;
+  size_t o = 0;
+  z.q2 = o; if (useP) o = zalign16(o + (size_t)T * KT2 * 8);            // (q,q) pairs
+  z.t2 = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * KT2 * 8);  // (t,t) pairs
+  z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT2 * nw32 * 8);      // allele table
+  z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * 8);
+  z.inc = o; if (counts && KT <= 8) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * 8);
+  z.m = o;  if (counts) o = zalign16(o + (size_t)T * KT * 4);
+  z.n = o;  if (counts) o = zalign16(o + (size_t)(2 * K + 1) * nw32 * 4);
+  z.total = o;
+  return z;
+}
+
+// One CTA = W warps x 32 loci (one locus per lane) x R locus blocks, over a
+// chunk of T individuals that every warp walks in the same order, so Q_i is a
+// shared-memory broadcast.  Per genotype both allele copies are handled as
+// one packed FP32x2 lane pair (sm_100 FFMA2/FADD2):
+//   X_k   = (P[l][k][a0], P[l][k][a1]) from a per-lane table indexed by the
+//           genotype class, so no per-copy select is executed;
+//   C_k   = fma(q_k, X_k, C_{k-1})  -- the cumulative mixture weights;
+//   r     = u * C_{K-1};  z = sum_k signbit(C_k - r) for k < K-1.
+// sign(C_k - r) is exactly (C_k < r) in IEEE arithmetic without flush to zero,
+// so z is the reference's "first k with r <= cumsum_k" on FP32 weights.
+// The genotype loop of one lane (one locus) over the chunk's individuals,
+// specialised on the likelihood and Z-store flags so no per-genotype branch
+// tests them; the 16 genotypes of a word are fully unrolled so every shift and
+// shared-memory offset is an immediate.
+struct ZArgs {
+  ChainDev* chp;
+  const uint32_t* grow;
+  const float2* Xlane;
+  const float2* sQ2;
+  const float2* sT2;
+  double* sLD;
+  const uint2* sInc;
+  int* sM;
+  int* mycol;
+  int i0, i1, nT16, l, K, L, lane, my_word, my_shift;
+  uint32_t prep, key, stream;
+  bool valid, pfonly;
+};
+
+template <int KT, int MODE, int W, bool LIKE, bool SZ>
+__device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, int& errb) {
+  constexpr int NW32 = 32 * W;
+  constexpr int KT2 = (KT + 1) & ~1;
+  constexpr int NWM = (KT + 3) / 4;
+  constexpr bool kUseP = (MODE == kZNormal || MODE == kZMetro || MODE == kZLike);
+  constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
+  constexpr bool kLut = kCounts && KT <= 8;
+  ChainDev& ch = *za.chp;
+  const uint32_t* grow = za.grow;
+  const float2* Xlane = za.Xlane;
+  const float2* sQ2 = za.sQ2;
+  const float2* sT2 = za.sT2;
+  double* sLD = za.sLD;
+  const uint2* sInc = za.sInc;
+  int* sM = za.sM;
+  int* mycol = za.mycol;
+  const int i0 = za.i0, i1 = za.i1, nT16 = za.nT16, l = za.l, K = za.K, L = za.L;
+  const int lane = za.lane, my_word = za.my_word, my_shift = za.my_shift;
+  const uint32_t prep = za.prep, key = za.key, stream = za.stream;
+  const bool valid = za.valid, pfonly = za.pfonly;
+    for (int wi = 0; wi < (nT16 >> 4); wi++) {
+      const uint32_t word = valid ? __ldg(grow + (i0 >> 4) + wi) : 0xFFFFFFFFu;
+      float wlike = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 16; j += 2) {
+        const int row0 = (wi << 4) + j;              // chunk-relative individual
+        const int ib = i0 + row0;
+        U4 r4;
+        if (MODE == kZNormal || MODE == kZInit)
+          r4 = philox_s((uint32_t)l, (uint32_t)(ib >> 1), prep, stream, key);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int row = row0 + h;
+          const uint32_t g = (word >> (2 * (j + h))) & 3u;
+          const bool miss = (g == 3u);
+          const uint32_t a0 = g >> 1, a1 = (g | (g >> 1)) & 1u;
+          int z0 = 0, z1 = 0;
+          if (kUseP) {
+            const float4* q4 = reinterpret_cast<const float4*>(sQ2 + row * KT2);
+            const float4* X4 = reinterpret_cast<const float4*>(Xlane) + (miss ? 0u : g) * ((KT2 / 2) * NW32);
+            float2 Cs[KT];
+            float2 Q2[KT2], X[KT2];
+#pragma unroll
+            for (int k = 0; k < KT2; k += 2) {
+              const float4 v = q4[k >> 1];
+              Q2[k] = make_float2(v.x, v.y);
+              Q2[k + 1] = make_float2(v.z, v.w);
+              const float4 xv = X4[(k >> 1) * NW32];
+              X[k] = make_float2(xv.x, xv.y);
+              X[k + 1] = make_float2(xv.z, xv.w);
+            }
+            Cs[0] = mul2_rn(Q2[0], X[0]);
+#pragma unroll
+            for (int k = 1; k < KT; k++) Cs[k] = fma2_rn(Q2[k], X[k], Cs[k - 1]);
+            const float2 Tp = Cs[KT - 1];
+            if (MODE == kZNormal) {
+              const float2 U = make_float2(u24(h ? r4.z : r4.x), u24(h ? r4.w : r4.y));
+              // r = round(u*T), negated by flipping sign bits in the integer
+              // domain so the rounded product can never be fused into the add
+              const float2 NR =
+                  bits_f2(f2_bits(mul2_rn(U, Tp)) ^ 0x8000000080000000ull);
+              uint32_t s0 = 0, s1 = 0;
+#pragma unroll
+              for (int k = 0; k < KT - 1; k++) {
+                const float2 D = add2_rn(Cs[k], NR);
+                s0 += __float_as_uint(D.x) >> 31;
+                s1 += __float_as_uint(D.y) >> 31;
+              }
+              z0 = (int)s0;
+              z1 = (int)s1;
+            }
+            if (MODE == kZMetro) {
+              const float4* t4 = reinterpret_cast<const float4*>(sT2 + row * KT2);
+              float2 T2[KT2];
+#pragma unroll
+              for (int k = 0; k < KT2; k += 2) {
+                const float4 v = t4[k >> 1];
+                T2[k] = make_float2(v.x, v.y);
+                T2[k + 1] = make_float2(v.z, v.w);
+              }
+              float2 S = mul2_rn(T2[0], X[0]);
+#pragma unroll
+              for (int k = 1; k < KT; k++) S = fma2_rn(T2[k], X[k], S);
+              const float tp = S.x * S.y, tm = Tp.x * Tp.y;
+              const bool tiny = !miss && !(tp > kLikeTinyF && tm > kLikeTinyF);
+              float term = miss ? 0.0f : __logf(tp) - __logf(tm);
+              if (__any_sync(0xffffffffu, tiny)) {
+                if (tiny)
+                  term = (float)(log((double)S.x) + log((double)S.y) - log((double)Tp.x) -
+                                 log((double)Tp.y));
+              }
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
+              if (lane == 0) atomicAdd(&sLD[row], (double)term);
+            }
+            if (LIKE) {
+              const float pr = Tp.x * Tp.y;
+              const bool tiny = !miss && !(pr > kLikeTinyF);
+              float lt = miss ? 0.0f : __logf(pr);
+              if (__any_sync(0xffffffffu, tiny)) {
+                if (tiny)
+                  lt = (float)(log(fmax((double)Tp.x, 1e-50)) + log(fmax((double)Tp.y, 1e-50)));
+              }
+              wlike += lt;
+            }
+          } else if (MODE == kZInit) {
+            z0 = (int)(((uint64_t)((h ? r4.z : r4.x) >> 1) * (uint64_t)K) >> 31);
+            z1 = (int)(((uint64_t)((h ? r4.w : r4.y) >> 1) * (uint64_t)K) >> 31);
+          } else if (MODE == kZRecount) {
+            if (valid && !miss) {
+              const int ii = i0 + row;
+              z0 = ch.Z[((size_t)ii * 2) * L + l];
+              z1 = ch.Z[((size_t)ii * 2 + 1) * L + l];
+              if (z0 >= K || z1 >= K) errb |= kErrBounds;
+            }
+          }
+          if (kCounts) {
+            // invalid lanes read all-missing words, so !miss implies valid
+            bool cnt = !miss;
+            if (MODE == kZRecount) cnt = cnt && z0 < K && z1 < K;
+            bool ncnt = cnt;
+            if (pfonly) ncnt = ncnt && ch.popflags[i0 + row] == 1;
+            const int trash = 2 * K;
+            atomicAdd(&mycol[(ncnt ? 2 * z0 + (int)a0 : trash) * NW32], 1);
+            atomicAdd(&mycol[(ncnt ? 2 * z1 + (int)a1 : trash) * NW32], 1);
+            uint32_t s_lo, s_hi = 0;
+            if (kLut) {
+              const uint2 v = sInc[cnt ? z0 * (KT + 1) + z1 : KT * (KT + 1) + KT];
+              s_lo = __reduce_add_sync(0xffffffffu, v.x);
+              if (KT > 4) s_hi = __reduce_add_sync(0xffffffffu, v.y);
+            } else {
+              uint32_t mw[NWM];
+#pragma unroll
+              for (int q = 0; q < NWM; q++) {
+                uint32_t v = 0;
+                if (cnt) {
+                  v += (z0 >> 2) == q ? (1u << (7 * (z0 & 3))) : 0u;
+                  v += (z1 >> 2) == q ? (1u << (7 * (z1 & 3))) : 0u;
+                }
+                mw[q] = __reduce_add_sync(0xffffffffu, v);
+              }
+              s_lo = 0;
+#pragma unroll
+              for (int q = 0; q < NWM; q++) s_lo = my_word == q ? mw[q] : s_lo;
+            }
+            const uint32_t s = kLut ? (my_word == 0 ? s_lo : s_hi) : s_lo;
+            const int f = (int)((s >> my_shift) & 127u);
+            if (lane < K) atomicAdd(&sM[row * KT + lane], f);
+          }
+          if (SZ && valid && i0 + row < i1) {
+            const size_t zi = (size_t)(i0 + row) * 2 * L + l;
+            ch.Z[zi] = miss ? kZMissing : (uint8_t)z0;
+            ch.Z[zi + L] = miss ? kZMissing : (uint8_t)z1;
+          }
+        }
+      }
+      if (LIKE) like_acc += (double)wlike;
+    }
+}
+
+template <int KT, int MODE, int W>
+__global__ void __launch_bounds__(32 * W, (KT <= 12 ? 768 : 512) / (32 * W))
+zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
+                 int nchains, int flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double sred[8];
+  constexpr int NW32 = 32 * W;
+  constexpr int KT2 = (KT + 1) & ~1;
+  constexpr int NWM = (KT + 3) / 4;
+  constexpr bool kUseP = (MODE == kZNormal || MODE == kZMetro || MODE == kZLike);
+  constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
+  constexpr bool kLut = kCounts && KT <= 8;
+
+  const int c = find_chain(prefix, nchains, blockIdx.x);
+  ChainDev& ch = chains[c];
+  const int tile = blockIdx.x - prefix[c];
+  const int T = ch.tileT, R = ch.tileR;
+  const int ichunk = tile % ch.nchunks, grp = tile / ch.nchunks;
+  const int N = ch.N, L = ch.L, A = ch.A, K = ch.K;
+  const int i0 = ichunk * T;
+  const int i1 = min(N, i0 + T);
+  const int nT = i1 - i0;
+  const int nT16 = (nT + 15) & ~15;  // whole words; padding genotypes are "missing"
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rep = *ch.rep;
+  const uint32_t key = ch.key;
+  const bool collect = rep + 1 > ch.burnin;
+  const bool want_like = (MODE == kZLike) ||
+      (MODE == kZNormal && ((flags & kZfLikeAlways) || ((flags & kZfLikeIfCollect) && collect)));
+  const bool store_z = (MODE == kZNormal || MODE == kZInit) && (flags & kZfStoreZ) && ch.Z;
+  const bool pfonly = ch.pfrompopflagonly != 0;
+
+  const ZLayout lay = zlayout(KT, K, T, NW32, MODE);
+  float2* sQ2 = reinterpret_cast<float2*>(smem + lay.q2);
+  float2* sT2 = reinterpret_cast<float2*>(smem + lay.t2);
+  float2* sX = reinterpret_cast<float2*>(smem + lay.x);
+  double* sLD = reinterpret_cast<double*>(smem + lay.ld);
+  uint2* sInc = reinterpret_cast<uint2*>(smem + lay.inc);
+  int* sM = reinterpret_cast<int*>(smem + lay.m);
+  int* sN = reinterpret_cast<int*>(smem + lay.n);
+
+  if (kUseP) {
+    for (int idx = threadIdx.x; idx < nT16 * KT2; idx += NW32) {
+      const int ii = idx / KT2, k = idx - ii * KT2;
+      const bool in = ii < nT && k < K;
+      const float q = in ? ch.Q[(size_t)(i0 + ii) * K + k] : 0.0f;
+      sQ2[idx] = make_float2(q, q);
+      if (MODE == kZMetro) {
+        const float t = in ? ch.TestQ[(size_t)(i0 + ii) * K + k] : 0.0f;
+        sT2[idx] = make_float2(t, t);
+      }
+    }
+  }
+  if (kCounts)
+    for (int idx = threadIdx.x; idx < nT16 * KT; idx += NW32) sM[idx] = 0;
+  if (kLut) {
+    // packed one-hot increments of two copies: 7-bit field per population,
+    // four fields per 32-bit half; index KT = "no copy"
+    for (int idx = threadIdx.x; idx < (KT + 1) * (KT + 1); idx += NW32) {
+      const int za = idx / (KT + 1), zb = idx - za * (KT + 1);
+      uint64_t v = 0;
+      if (za < KT) v += 1ull << (7 * (za & 3) + 32 * (za >> 2));
+      if (zb < KT) v += 1ull << (7 * (zb & 3) + 32 * (zb >> 2));
+      sInc[idx] = make_uint2((uint32_t)v, (uint32_t)(v >> 32));
+    }
+  }
+  if (MODE == kZMetro)
+    for (int idx = threadIdx.x; idx < nT16; idx += NW32) sLD[idx] = 0.0;
+  __syncthreads();
+
+  // lane k < K extracts population k's field from the reduced words
+  const int my_word = lane >> 2, my_shift = 7 * (lane & 3);
+
+  double like_acc = 0.0;
+  int errb = 0;
+  const uint32_t stream = (MODE == kZInit) ? (uint32_t)kSInitZ : (uint32_t)kSZ;
+  const uint32_t prep = (MODE == kZInit) ? 0u : (uint32_t)rep;
+  int* mycol = sN + threadIdx.x;   // this lane's n[l][k][a] column: stride NW32
+
+  for (int rb = 0; rb < R; rb++) {
+    const int lbase = ((grp * R + rb) * W + warp) * 32;
+    if (lbase >= L) break;  // warp-uniform
+    const int l = lbase + lane;
+    const bool valid = l < L;
+    if (kUseP) {
+      // allele table of this lane's locus, per class g in {0/0, 0/1, 1/1}:
+      // float4 (P[a0][k], P[a1][k], P[a0][k+1], P[a1][k+1]) per pair of k
+      float4* X4w = reinterpret_cast<float4*>(sX) + threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < KT2; k += 2) {
+        float p0[2], p1[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int kk = k + e;
+          p0[e] = (valid && kk < K) ? ch.P[((size_t)l * K + kk) * A] : 0.0f;
+          p1[e] = (valid && kk < K && A > 1) ? ch.P[((size_t)l * K + kk) * A + 1] : 0.0f;
+        }
+        X4w[(0 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
+        X4w[(1 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
+        X4w[(2 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p1[0], p1[0], p1[1], p1[1]);
+      }
+    }
+    if (kCounts)
+      for (int q = 0; q < 2 * K + 1; q++) mycol[q * NW32] = 0;   // row 2K: missing copies
+    __syncwarp();
+    const uint32_t* grow = ch.g2 + (size_t)(valid ? l : 0) * ch.wpr;
+    const float2* Xlane = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
+    {
+      ZArgs za{&ch, grow, Xlane, sQ2, sT2, sLD, sInc, sM, mycol, i0, i1, nT16, l, K, L, lane,
+               my_word, my_shift, prep, key, stream, valid, pfonly};
+      if (want_like) {
+        if (store_z) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb);
+        else zword_loop<KT, MODE, W, true, false>(za, like_acc, errb);
+      } else {
+        if (store_z) zword_loop<KT, MODE, W, false, true>(za, like_acc, errb);
+        else zword_loop<KT, MODE, W, false, false>(za, like_acc, errb);
+      }
+    }
+    if (kCounts) {
+      __syncwarp();
+      if (valid) {
+        const size_t cbase = (size_t)ichunk * K * A;
+        for (int k = 0; k < K; k++) {
+          ch.npart[((cbase + (size_t)k * A) + 0) * L + l] = mycol[(k * 2) * NW32];
+          if (A > 1) ch.npart[((cbase + (size_t)k * A) + 1) * L + l] = mycol[(k * 2 + 1) * NW32];
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  if (kCounts) {
+    int* dst = ch.mpart + ((size_t)grp * N + i0) * K;
+    for (int idx = threadIdx.x; idx < nT * K; idx += NW32) {
+      const int ii = idx / K;
+      dst[idx] = sM[ii * KT + (idx - ii * K)];
+    }
+  }
+  if (MODE == kZMetro) {
+    double* dst = ch.ldpart + (size_t)grp * N + i0;
+    for (int idx = threadIdx.x; idx < nT; idx += NW32) dst[idx] = sLD[idx];
+  }
+  if (errb) set_err(ch.err, errb);
+
+  const int ntiles = ch.nchunks * ch.ngroups;
+  if (want_like) {
+    double sres = block_sum_d(like_acc, sred);
+    if (threadIdx.x == 0) ch.likepart[tile] = sres;
+  }
+  const bool advance = (flags & kZfAdvance) != 0;
+  if (want_like || advance) {
+    if (last_cta_arrive(&ch.ctr[kCtrZ], (unsigned)ntiles)) {
+      if (want_like) finish_like(ch, ntiles, collect && (flags & kZfCollect), sred);
+      if (advance && threadIdx.x == 0) *ch.rep = rep + 1;
+    }
+  }
+}
+
+template <int KT, int W>
+cudaError_t launch_b2g_kw(const LaunchSet& ls, int mode, int flags, size_t smem) {
+  dim3 grid(ls.total_ctas), block(32 * W);
+  switch (mode) {
+#define ST_ZCASE(M)                                                                        \
+  case M: {                                                                                \
+    auto fn = zpass_b2g_kernel<KT, M, W>;                                                   \
+    if (smem > 48 * 1024)                                                                  \
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
+    fn<<<grid, block, smem, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, flags);         \
+    return cudaGetLastError();                                                             \
+  }
+    ST_ZCASE(kZNormal)
+    ST_ZCASE(kZInit)
+    ST_ZCASE(kZRecount)
+    ST_ZCASE(kZMetro)
+    ST_ZCASE(kZLike)
+#undef ST_ZCASE
+  }
+  return cudaErrorInvalidValue;
+}
+
+
+}  // namespace zfast
+}  // namespace st
