@@ -141,7 +141,7 @@ typedef struct st_model {
     double fpriorsd;           /* FPRIORSD */
     int32_t store_z;           /* keep Z in HBM (needed for st_get_state ST_F_Z) */
     int32_t precision;         /* 0: FP32 Z/P/Q arithmetic; 1: FP64 Z (U8 data) */
-    int32_t tile_t, tile_w, tile_r; /* Z-pass tile (0 = choose); see DESIGN */
+    int32_t tile_t, tile_w, tile_r; /* Z-pass tile (0 = choose): individuals per chunk, warps, locus blocks per CTA */
     int32_t reserved[8];
 } st_model;
 
