@@ -173,6 +173,35 @@ int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183     
  * Needs U8 data.                                                             */
 int st_update_z_injected(st_chain *c, const double *uniforms, size_t n, int precision);
 
+/* One Z update with its counts and ln P(D) that allocates no device memory.
+ * No counterpart in the reference: it serves callers that own every device
+ * allocation themselves (a pool allocator that forbids outside cudaMalloc, a
+ * fixed device-memory budget, a path where an allocation would synchronise
+ * the device) and so cannot create a chain.
+ *   g2        device, B2G words [num_loci][wpr], wpr >= ceil(num_inds/16);
+ *             padding individuals coded 3 (missing)
+ *   Q         device, float [num_inds][maxpops]
+ *   P         device, float [num_loci][maxpops][2]
+ *   seed, rep the chain seed (as given to st_chain_create) and sweep index;
+ *             the draws equal st_update_z's on a chain with that seed at ST_F_REP = rep
+ *   n_out     device, int32 [num_loci][maxpops][2]  (ST_F_N after st_update_z)
+ *   m_out     device, int32 [num_inds][maxpops]     (ST_F_M after st_update_z)
+ *   like_out  device double, ln P(D|Q,P), or NULL to skip it
+ *   err_out   device int32 error word (ST_DERR_* bits), or NULL
+ *   scratch_bytes (host, may be NULL) receives the scratch the call needs.
+ * The count partials live in one static device array of
+ * ST_NOALLOC_SCRATCH_BYTES per GPU (held until exit); a call that needs more
+ * returns ST_ERR_ADMISSION.  Calls are asynchronous on cuda_stream (NULL =
+ * default stream) and share that array: calls that overlap on the GPU race.
+ * The first call on a device looks the array up (and may load the library's
+ * device code); make it before any stream capture.                           */
+#define ST_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int st_update_z_noalloc(int device, const uint32_t *g2, int32_t wpr, int32_t num_inds,
+                        int32_t num_loci, int32_t maxpops, const float *Q, const float *P,
+                        uint64_t seed, int32_t rep, int32_t *n_out, int32_t *m_out,
+                        double *like_out, int32_t *err_out, void *cuda_stream,
+                        size_t *scratch_bytes);
+
 /* ---- sweeps ----------------------------------------------------------------
  * st_sweep: n sweeps in the order of src/structure.c:497-685 (P, Q, Z, alpha,
  * eps, F, DataCollection after burn-in), fused into 3-5 launches per sweep.
