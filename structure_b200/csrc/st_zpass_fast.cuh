@@ -20,6 +20,11 @@ namespace zfast {
 
 
 constexpr float kLikeTinyF = 1e-30f;
+// ln P(D) fast path: the genotype terms Q.P(copy 0) * Q.P(copy 1) of four
+// genotypes are multiplied in FP32 and logged once.  Each factor above this
+// bound keeps the product of four a normal float (>= 1e-36 > FLT_MIN); a word
+// holding a smaller term is recomputed exactly (word_like_exact).
+constexpr float kLikeFastMin = 1e-9f;
 
 // Deterministic block sum of one double per thread (fixed tree order).
 __device__ __forceinline__ double block_sum_d(double v, double* sred) {
@@ -109,6 +114,35 @@ struct ZArgs {
   bool valid, pfonly;
 };
 
+// ln P(D) terms of one lane's 16 genotypes of a word in FP64 with the
+// reference's per-copy clamp (CalcLike.c:75-133: log of max(Q.P, sqrt(1e-100))),
+// from the same FP32 mixture sums as the draw.  Taken only for words that hold
+// a term below kLikeFastMin.
+template <int KT, int W>
+__device__ __noinline__ double word_like_exact(uint32_t word, int row_base, const float2* Xlane,
+                                               const float2* sQ2) {
+  constexpr int NW32 = 32 * W;
+  constexpr int KT2 = (KT + 1) & ~1;
+  double s = 0.0;
+  for (int gi = 0; gi < 16; gi++) {
+    const uint32_t g = (word >> (2 * gi)) & 3u;
+    if (g == 3u) continue;
+    const float4* q4 = reinterpret_cast<const float4*>(sQ2 + (row_base + gi) * KT2);
+    const float4* X4 = reinterpret_cast<const float4*>(Xlane) + g * ((KT2 / 2) * NW32);
+    float2 C = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int k = 0; k < KT2; k += 2) {
+      const float4 v = q4[k >> 1];
+      const float4 xv = X4[(k >> 1) * NW32];
+      if (k == 0) C = mul2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y));
+      else C = fma2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y), C);
+      if (k + 1 < KT) C = fma2_rn(make_float2(v.z, v.w), make_float2(xv.z, xv.w), C);
+    }
+    s += log(fmax((double)C.x, 1e-50)) + log(fmax((double)C.y, 1e-50));
+  }
+  return s;
+}
+
 template <int KT, int MODE, int W, bool LIKE, bool SZ>
 __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, int& errb) {
   constexpr int NW32 = 32 * W;
@@ -132,7 +166,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   const bool valid = za.valid, pfonly = za.pfonly;
     for (int wi = 0; wi < (nT16 >> 4); wi++) {
       const uint32_t word = valid ? __ldg(grow + (i0 >> 4) + wi) : 0xFFFFFFFFu;
-      float wlike = 0.0f;
+      float wlike = 0.0f, wprod = 1.0f, wmin = 1.0f;
 #pragma unroll
       for (int j = 0; j < 16; j += 2) {
         const int row0 = (wi << 4) + j;              // chunk-relative individual
@@ -206,14 +240,11 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               if (lane == 0) atomicAdd(&sLD[row], (double)term);
             }
             if (LIKE) {
-              const float pr = Tp.x * Tp.y;
-              const bool tiny = !miss && !(pr > kLikeTinyF);
-              float lt = miss ? 0.0f : __logf(pr);
-              if (__any_sync(0xffffffffu, tiny)) {
-                if (tiny)
-                  lt = (float)(log(fmax((double)Tp.x, 1e-50)) + log(fmax((double)Tp.y, 1e-50)));
-              }
-              wlike += lt;
+              // j + h is a compile-time constant after unrolling
+              const float pr = miss ? 1.0f : Tp.x * Tp.y;
+              wmin = fminf(wmin, pr);
+              wprod = ((j + h) & 3) == 0 ? pr : wprod * pr;
+              if (((j + h) & 3) == 3) wlike += __logf(wprod);
             }
           } else if (MODE == kZInit) {
             z0 = (int)(((uint64_t)((h ? r4.z : r4.x) >> 1) * (uint64_t)K) >> 31);
@@ -266,7 +297,14 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
           }
         }
       }
-      if (LIKE) like_acc += (double)wlike;
+      if (LIKE) {
+        double wl = (double)wlike;
+        if (__any_sync(0xffffffffu, !(wmin > kLikeFastMin))) {   // once per word, rare
+          if (!(wmin > kLikeFastMin))
+            wl = word_like_exact<KT, W>(word, wi << 4, Xlane, sQ2);
+        }
+        like_acc += wl;
+      }
     }
 }
 

@@ -386,6 +386,58 @@ def test_calclike_matches_reference(ctx, orc, ref, layout):
     c.close(); d.close()
 
 
+def test_calclike_tiny_terms_take_the_exact_path(ctx, orc, ref):
+    """Genotype terms below the FP32 fast-path bound (Q.P products under 1e-9)
+    are recomputed in FP64 with the reference's clamp; the total still matches
+    the reference's CalcLike."""
+    geno, na, _ = _snp(N=200, L=1200, K=4, seed=17)
+    N, _, L = geno.shape
+    K = 4
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G)
+    rng = np.random.default_rng(9)
+    Q, P = _rand_state(rng, N, L, K, na)
+    tiny = (rng.random(L) < 0.3) & (na == 2)
+    P[tiny, :, 1] = 1e-20
+    P[tiny, :, 0] = 1.0
+    small = (rng.random(L) < 0.1) & (na == 2) & ~tiny
+    P[small, :, 1] = 3e-6          # terms 9e-12 (1/1) and 3e-6 (0/1)
+    P[small, :, 0] = 1.0 - 3e-6
+    hit = np.isin(np.arange(L), np.flatnonzero(tiny | small)) & (geno[:, 1, :] == 1).any(0)
+    assert hit.sum() > 50
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    c.DataCollection()
+    like = c.get(api.F_STATS)[api.ST_LIKE]
+    lo = orc.calc_like(geno, Q, P)
+    ref.set_globals(N=N, L=L, K=K, maxalleles=c.A)
+    lr = ref.lib.CalcLike(geno.copy(), None, Q.astype(np.float64), P.astype(np.float64), None,
+                          None, None)
+    assert abs(lo - lr) <= 1e-12 * abs(lr)
+    assert abs(like - lr) <= 1e-6 * abs(lr), (like, lr)
+    assert c.get(api.F_ERR) == 0
+    c.close(); d.close()
+
+
+def test_sweep_lnpd_matches_oracle(ctx, orc):
+    """ln P(D) folded in by the sweep's Z pass equals CalcLike of the Q and P
+    that pass drew with, and sumlikes/sumsqlikes accumulate it."""
+    geno, na, _ = _snp(N=160, L=900, K=5, seed=29)
+    K = 5
+    d, c = _chain(ctx, geno, na, K, layout=api.LAYOUT_B2G, freqscorr=1, burnin=0)
+    likes = []
+    for _ in range(3):
+        c.sweep(1)
+        st = c.get(api.F_STATS)
+        lo = orc.calc_like(geno, c.get(api.F_Q), c.get(api.F_P))
+        assert abs(st[api.ST_LIKE] - lo) <= 1e-6 * abs(lo)
+        likes.append(st[api.ST_LIKE])
+    st = c.get(api.F_STATS)
+    assert st[api.ST_NLIKE] == 3
+    np.testing.assert_allclose(st[api.ST_SUMLIKES], sum(likes), rtol=1e-13)
+    np.testing.assert_allclose(st[api.ST_SUMSQ], sum(x * x for x in likes), rtol=1e-13)
+    c.close(); d.close()
+
+
 def test_sweeps_match_oracle_composition(ctx, orc):
     """Three full sweeps on the device == the oracle's updates composed in
     structure.c order, with each stochastic stage fed the device's inputs."""
