@@ -215,6 +215,12 @@ int st_sync(st_chain *c);          /* wait; ST_ERR_DEVICE if the error word is s
 int st_batch_create(st_ctx *ctx, st_chain **chains, int nchains, st_batch **out);
 int st_batch_sweep(st_batch *b, int nsweeps);
 int st_batch_destroy(st_batch *b);
+/* Replay each kind of sweep (Gibbs, Metropolis) from a CUDA graph captured on
+ * first use (default on).  Used only when profiling is off and the context's
+ * stream is not the legacy default stream; otherwise launches are direct.
+ * No reference counterpart (the reference enqueues every kernel per sweep,
+ * src/structure.c:497-685).                                                  */
+int st_batch_graphs(st_batch *b, int enable);
 
 /* ---- state ---------------------------------------------------------------- */
 enum st_field {

@@ -90,6 +90,7 @@ def lib():
         "st_sync": ([vp], C.c_int),
         "st_batch_create": ([vp, C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
         "st_batch_sweep": ([vp, C.c_int], C.c_int),
+        "st_batch_graphs": ([vp, C.c_int], C.c_int),
         "st_batch_destroy": ([vp], C.c_int),
         "st_get_state": ([vp, C.c_int, vp, sz], C.c_int),
         "st_set_state": ([vp, C.c_int, vp, sz], C.c_int),
@@ -102,6 +103,14 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+FAST_K_CLASSES = (1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 20, 24, 32)
+
+
+def fast_class(K):
+    """K capacity class of the biallelic Z pass (K is zero-padded up to it)."""
+    return next(k for k in FAST_K_CLASSES if k >= K)
 
 
 def model_defaults(**kw):
@@ -286,6 +295,10 @@ class Batch:
 
     def sweep(self, n=1):
         self.ctx.check(lib().st_batch_sweep(self.h, n))
+
+    def graphs(self, enable=True):
+        """Replay captured CUDA graphs of the sweep (default on)."""
+        self.ctx.check(lib().st_batch_graphs(self.h, int(enable)))
 
     def close(self):
         if self.h:

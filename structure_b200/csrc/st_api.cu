@@ -62,17 +62,29 @@ struct st_chain {
   bool timed = false;
 };
 
+// Chains of one K capacity class: a contiguous slice of the batch table,
+// advanced by one Z-pass launch per step.
+struct ZGroup {
+  int first = 0, n = 0;    // slice of the batch table
+  int KT = 0, W = 8;
+  size_t zsmem = 0;
+  int tz = 0;              // CTAs of the slice
+};
+
 struct st_batch {
   st_ctx* ctx = nullptr;
-  std::vector<st_chain*> chains;
+  std::vector<st_chain*> chains;   // sorted by K class
   ChainDev* d_table = nullptr;
-  int* d_pz = nullptr;     // prefix: Z pass
+  int* d_pz = nullptr;     // prefix: Z pass (restarting at 0 in every group)
   int* d_pl = nullptr;     // prefix: locus kernel
   int* d_pi = nullptr;     // prefix: individual kernel
   int tz = 0, tl = 0, ti = 0;
-  size_t zsmem = 0;
-  int KT = 0, W = 8, G = 1;
+  std::vector<ZGroup> zg;  // fast path: one Z launch per K class
+  int G = 1;
   bool fast = false;
+  bool graphs = true;                          // replay captured sweeps
+  cudaGraphExec_t gx[2] = {nullptr, nullptr};  // [Gibbs sweep, Metropolis sweep]
+  int glaunches[2] = {0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -1020,50 +1032,60 @@ extern "C" int st_set_state(st_chain* c, int f, const void* host, size_t bytes) 
 extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch** out) {
   if (!ctx || !chains || n < 1 || !out) return ST_ERR_ARG;
   *out = nullptr;
+  for (int j = 0; j < n; j++)
+    if (!chains[j]) return ST_ERR_ARG;
   cudaSetDevice(ctx->device);
   st_batch* b = new st_batch();
   b->ctx = ctx;
   b->chains.assign(chains, chains + n);
-  st_chain* c0 = chains[0];
+  // one Z launch per K class: keep each class contiguous in the table
+  std::stable_sort(b->chains.begin(), b->chains.end(),
+                   [](const st_chain* a, const st_chain* c) { return a->KT < c->KT; });
+  st_chain* c0 = b->chains[0];
   b->fast = c0->fast;
-  b->W = c0->h.tileW;
-  int G = 1, KT = 0;
+  int G = 1;
   for (st_chain* c : b->chains) {
-    if (c->ctx != ctx || c->fast != b->fast || c->h.tileW != b->W ||
-        c->h.metrofreq != c0->h.metrofreq || c->host_rep != c0->host_rep ||
-        c->model.store_z != c0->model.store_z || c->model.precision != c0->model.precision) {
+    if (c->ctx != ctx || c->fast != b->fast || c->h.metrofreq != c0->h.metrofreq ||
+        c->host_rep != c0->host_rep || c->model.store_z != c0->model.store_z ||
+        c->model.precision != c0->model.precision ||
+        c->h.computeprob != c0->h.computeprob) {
       delete b;
       return seterr(ctx, ST_ERR_ARG,
-                    "batched chains must share the context, data path, tile width, METROFREQ, "
+                    "batched chains must share the context, data path, METROFREQ, COMPUTEPROB, "
                     "sweep counter and Z storage");
     }
     G = std::max(G, c->h.G);
-    KT = std::max(KT, c->KT);
-    b->zsmem = std::max(b->zsmem, c->zsmem);
   }
-  for (st_chain* c : b->chains)
-    if (c->fast && c->KT != KT) {
-      delete b;
-      return seterr(ctx, ST_ERR_ARG, "batched fast-path chains must share the K class");
-    }
   b->G = G;
-  b->KT = KT;
   std::vector<ChainDev> table(n);
   std::vector<int> pz(n), pl(n), pi(n);
   for (int j = 0; j < n; j++) {
-    table[j] = b->chains[j]->h;
-    pz[j] = b->tz; pl[j] = b->tl; pi[j] = b->ti;
-    b->tz += b->fast ? ctas_zpass_b2g(table[j]) : ctas_zpass_u8(table[j], 256);
-    b->tl += ctas_locus(table[j], kBlockLoc);
-    b->ti += ctas_ind(table[j], kBlockInd);
-  }
-  // every chain's kernels must index its groups by the batch-wide G
-  for (int j = 0; j < n; j++) table[j].G = G;
-  pl.clear(); pi.clear();
-  b->tl = b->ti = 0;
-  for (int j = 0; j < n; j++) {
-    pl.push_back(b->tl);
-    pi.push_back(b->ti);
+    st_chain* c = b->chains[j];
+    table[j] = c->h;
+    table[j].G = G;   // every chain's kernels index their groups by the batch-wide G
+    if (b->fast && (b->zg.empty() || b->zg.back().KT != c->KT)) {
+      ZGroup g;
+      g.first = j;
+      g.KT = c->KT;
+      g.W = c->h.tileW;
+      b->zg.push_back(g);
+    }
+    if (b->fast) {
+      ZGroup& g = b->zg.back();
+      if (c->h.tileW != g.W) {
+        delete b;
+        return seterr(ctx, ST_ERR_ARG, "chains of one K class must share the Z-pass width");
+      }
+      pz[j] = g.tz;
+      g.tz += ctas_zpass_b2g(table[j]);
+      g.zsmem = std::max(g.zsmem, c->zsmem);
+      g.n++;
+    } else {
+      pz[j] = b->tz;
+      b->tz += ctas_zpass_u8(table[j], 256);
+    }
+    pl[j] = b->tl;
+    pi[j] = b->ti;
     b->tl += ctas_locus(table[j], kBlockLoc);
     b->ti += ctas_ind(table[j], kBlockInd);
   }
@@ -1094,7 +1116,123 @@ extern "C" int st_batch_destroy(st_batch* b) {
     if (p) cudaFree(p);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  for (cudaGraphExec_t x : b->gx)
+    if (x) cudaGraphExecDestroy(x);
   delete b;
+  return ST_OK;
+}
+
+// The launches of one batched sweep in src/structure.c:497-685 order: P, eps
+// and F (locus kernel); Q and alpha (individual kernel, with the Metropolis
+// data pass on METROFREQ sweeps); the Z pass with counts and ln P(D).  The
+// sweep index lives on the device, so the sequence depends on the host only
+// through `metro`.
+static int enqueue_batch_sweep(st_batch* b, bool metro) {
+  st_ctx* ctx = b->ctx;
+  const int n = (int)b->chains.size();
+  st_chain* c0 = b->chains[0];
+  cudaStream_t s = ctx->stream;
+  LaunchSet lz{b->d_table, b->d_pz, n, b->tz, s};
+  // one fast Z launch per K class over its slice of the table
+  auto zfast = [&](int mode, int flags) -> int {
+    for (const ZGroup& g : b->zg) {
+      LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, s};
+      ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags, g.zsmem));
+    }
+    ctx->launches += (int64_t)b->zg.size() - 1;   // the bracket counted one
+    return ST_OK;
+  };
+  LaunchSet ll{b->d_table, b->d_pl, n, b->tl, s};
+  LaunchSet li{b->d_table, b->d_pi, n, b->ti, s};
+  const int zflags = (c0->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
+                     (c0->model.store_z ? kZfStoreZ : 0);
+  {
+    Bracket br(ctx, ST_K_LOCUS);
+    ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
+  }
+  if (metro) {
+    {
+      Bracket br(ctx, ST_K_IND);
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndPropose, 0, kBlockInd));
+    }
+    if (!b->fast)
+      for (st_chain* c : b->chains)
+        ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * c->h.N, s));
+    {
+      Bracket br(ctx, ST_K_METRO);
+      if (b->fast) {
+        if (int rc = zfast(kZMetro, 0)) return rc;
+      } else {
+        ST_CUDA(ctx, launch_zpass_u8(lz, kZMetro, c0->model.precision ? kZfF64 : 0));
+      }
+    }
+    Bracket br(ctx, ST_K_IND);
+    ST_CUDA(ctx, launch_ind(li, b->G, kIndAccept, kIndAlpha | kIndCollect, kBlockInd));
+  } else {
+    Bracket br(ctx, ST_K_IND);
+    ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
+  }
+  if (!b->fast)
+    for (st_chain* c : b->chains) {
+      ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
+      ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
+    }
+  {
+    Bracket br(ctx, ST_K_ZPASS);
+    if (b->fast) {
+      if (int rc = zfast(kZNormal, zflags)) return rc;
+    } else {
+      ST_CUDA(ctx, launch_zpass_u8(lz, kZNormal, zflags | (c0->model.precision ? kZfF64 : 0)));
+    }
+  }
+  return ST_OK;
+}
+
+// Captures the sweep of kind `metro` into a CUDA graph on first use.  Returns
+// false (and leaves graphs off for this batch) when capture is not possible.
+static bool batch_graph(st_batch* b, bool metro) {
+  st_ctx* ctx = b->ctx;
+  const int j = metro ? 1 : 0;
+  if (b->gx[j]) return true;
+  cudaStream_t s = ctx->stream;
+  const int64_t l0 = ctx->launches;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const int rc = enqueue_batch_sweep(b, metro);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  ctx->launches = l0;
+  if (rc != ST_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return false;
+  }
+  cudaGraphExec_t x = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  std::vector<cudaGraphNode_t> list(nodes);
+  int kernels = 0;
+  if (nodes && cudaGraphGetNodes(g, list.data(), &nodes) == cudaSuccess)
+    for (cudaGraphNode_t nd : list) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kernels++;
+    }
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess || !x) {
+    cudaGetLastError();
+    return false;
+  }
+  b->gx[j] = x;
+  b->glaunches[j] = kernels;
+  return true;
+}
+
+extern "C" int st_batch_graphs(st_batch* b, int enable) {
+  if (!b) return ST_ERR_ARG;
+  b->graphs = enable != 0;
   return ST_OK;
 }
 
@@ -1102,50 +1240,21 @@ extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
   if (!b || nsweeps < 0) return ST_ERR_ARG;
   st_ctx* ctx = b->ctx;
   cudaSetDevice(ctx->device);
-  const int n = (int)b->chains.size();
   st_chain* c0 = b->chains[0];
   cudaStream_t s = ctx->stream;
-  LaunchSet lz{b->d_table, b->d_pz, n, b->tz, s};
-  LaunchSet ll{b->d_table, b->d_pl, n, b->tl, s};
-  LaunchSet li{b->d_table, b->d_pi, n, b->ti, s};
-  const int zflags = (c0->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
-                     (c0->model.store_z ? kZfStoreZ : 0);
+  // graphs replay the same launches; per-launch profiling events need the
+  // direct path, and the legacy default stream cannot be captured
+  const bool graphs = b->graphs && !ctx->profile && s != nullptr;
   cudaEventRecord(b->ev0, s);
   for (int sw = 0; sw < nsweeps; sw++) {
     const int rep = c0->host_rep;
     const bool metro = c0->h.metrofreq > 0 && rep % c0->h.metrofreq == 0;
-    {
-      Bracket br(ctx, ST_K_LOCUS);
-      ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
-    }
-    if (metro) {
-      {
-        Bracket br(ctx, ST_K_IND);
-        ST_CUDA(ctx, launch_ind(li, b->G, kIndPropose, 0, kBlockInd));
-      }
-      if (!b->fast)
-        for (st_chain* c : b->chains)
-          ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * c->h.N, s));
-      {
-        Bracket br(ctx, ST_K_METRO);
-        ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZMetro, 0, b->zsmem)
-                             : launch_zpass_u8(lz, kZMetro, c0->model.precision ? kZfF64 : 0));
-      }
-      Bracket br(ctx, ST_K_IND);
-      ST_CUDA(ctx, launch_ind(li, b->G, kIndAccept, kIndAlpha | kIndCollect, kBlockInd));
+    if (graphs && batch_graph(b, metro)) {
+      ST_CUDA(ctx, cudaGraphLaunch(b->gx[metro ? 1 : 0], s));
+      ctx->launches += b->glaunches[metro ? 1 : 0];
     } else {
-      Bracket br(ctx, ST_K_IND);
-      ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
-    }
-    if (!b->fast)
-      for (st_chain* c : b->chains) {
-        ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
-        ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
-      }
-    {
-      Bracket br(ctx, ST_K_ZPASS);
-      ST_CUDA(ctx, b->fast ? launch_zpass_b2g(lz, b->KT, b->W, kZNormal, zflags, b->zsmem)
-                           : launch_zpass_u8(lz, kZNormal, zflags | (c0->model.precision ? kZfF64 : 0)));
+      if (graphs) b->graphs = false;
+      if (int rc = enqueue_batch_sweep(b, metro)) return rc;
     }
     for (st_chain* c : b->chains) c->host_rep++;
   }
