@@ -75,7 +75,8 @@ int st_ctx_destroy(st_ctx *ctx);
 const char *st_last_error(const st_ctx *ctx);
 int st_ctx_memory(const st_ctx *ctx, size_t *in_use, size_t *budget);
 /* Launch on the caller's cudaStream_t (passed as void*) instead of the
- * context's own stream; NULL restores the context stream.                   */
+ * context's own stream; NULL restores the context stream.  The legacy default
+ * stream is passed as cudaStreamLegacy ((void*)1).                          */
 int st_ctx_set_stream(st_ctx *ctx, void *cuda_stream);
 
 /* Per-kernel timing: when enabled, every launch is bracketed by CUDA events on
@@ -221,6 +222,23 @@ int st_batch_destroy(st_batch *b);
  * No reference counterpart (the reference enqueues every kernel per sweep,
  * src/structure.c:497-685).                                                  */
 int st_batch_graphs(st_batch *b, int enable);
+
+/* ---- gradient of ln P(D|Q,P) -----------------------------------------------
+ * No reference counterpart (the reference evaluates the likelihood only,
+ * src/CalcLike.c:75-133 CalcLikeInd).  With Z summed out,
+ *   ln P(D|Q,P) = sum_i sum_l sum_copy log sum_k Q_ik P_lk,allele(copy),
+ * taken without CalcLikeInd's underflow clamps, Q_i = softmax(q_logits_i)
+ * over K and P_lk = softmax(p_logits_lk) over the two alleles.  Biallelic
+ * 2-bit data (ST_LAYOUT_B2G), K = 1..16.  precision 32 (float buffers) or 64
+ * (double buffers).  Every pointer is DEVICE memory owned by the caller:
+ * q_logits, dq [N][K]; p_logits, dp [L][K][2]; loglik (double scalar) and
+ * ll_ind (double [N], per individual) may be NULL.  Asynchronous on the
+ * context's stream.                                                          */
+typedef struct st_grad st_grad;
+int st_grad_create(st_ctx *ctx, st_data *data, int maxpops, int precision, st_grad **out);
+int st_grad_destroy(st_grad *g);
+int st_loglik_grad(st_grad *g, const void *q_logits, const void *p_logits, void *dq, void *dp,
+                   double *loglik, double *ll_ind);
 
 /* ---- state ---------------------------------------------------------------- */
 enum st_field {

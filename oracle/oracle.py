@@ -89,6 +89,9 @@ class Oracle:
         lib.orc_init_eps.argtypes = [_ci, _ci, _ci, _i32p, _i32p, _ci, _cd, _cd, _ci, _f64p, _f64p]
         lib.orc_est_logprob.argtypes = [_cd, _cd, _ci]
         lib.orc_est_logprob.restype = _cd
+        lib.orc_loglik_grad.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f64p, _f64p, _f64p, _f64p,
+                                        _f64p]
+        lib.orc_loglik_grad.restype = _cd
 
     # -- RNG ---------------------------------------------------------------
     def philox(self, ctr, key):
@@ -245,6 +248,18 @@ class Oracle:
 
     def est_logprob(self, s, ss, reps):
         return self.lib.orc_est_logprob(s, ss, reps)
+
+    def loglik_grad(self, geno, qlog, plog):
+        """ln P(D|softmax(qlog), softmax(plog)) and its gradient w.r.t. the
+        logits, FP64, no clamps.  qlog [N][K], plog [L][K][A]."""
+        N, _, L = geno.shape
+        K, A = qlog.shape[1], plog.shape[2]
+        qlog = np.ascontiguousarray(qlog, np.float64)
+        plog = np.ascontiguousarray(plog, np.float64)
+        dq, dp, lli = np.zeros_like(qlog), np.zeros_like(plog), np.zeros(N)
+        ll = self.lib.orc_loglik_grad(N, L, K, A, np.ascontiguousarray(geno, np.int32), qlog,
+                                      plog, dq, dp, lli)
+        return ll, dq, dp, lli
 
 
 class RefModel(C.Structure):

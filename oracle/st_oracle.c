@@ -657,3 +657,68 @@ double orc_est_logprob(double sumlikes, double sumsqlikes, int reps)
     double var = reps == 1 ? 0.0 : (sumsqlikes - sumlikes * sumlikes / reps) / (reps - 1);
     return mean - var / 2.0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Gradient of the Z-marginalised log-likelihood (CalcLike.c:75-133          */
+/* CalcLikeInd summed over individuals, without the underflow clamps) with   */
+/* respect to softmax logits: Q_i = softmax(qlog_i) over K, P_lk =           */
+/* softmax(plog_lk) over the A alleles.                                      */
+/*   ll = sum_i sum_l sum_copy log S,  S = sum_k Q_ik P_lk,a(copy)            */
+/*   dll/dQ_ik = sum_l sum_copy P_lk,a / S;  dll/dP_lka = sum_i sum_copy Q_ik/S */
+/*   d/dlogit = p * (g - <p, g>)  (softmax Jacobian)                          */
+/* ------------------------------------------------------------------------ */
+static void softmax_rows(const double *x, double *y, size_t rows, int n)
+{
+    for (size_t r = 0; r < rows; r++) {
+        const double *a = x + r * n;
+        double *b = y + r * n, m = a[0], s = 0.0;
+        for (int j = 1; j < n; j++) m = a[j] > m ? a[j] : m;
+        for (int j = 0; j < n; j++) { b[j] = exp(a[j] - m); s += b[j]; }
+        for (int j = 0; j < n; j++) b[j] /= s;
+    }
+}
+
+double orc_loglik_grad(int N, int L, int K, int A, const int32_t *geno,
+                       const double *qlog, const double *plog,
+                       double *dq, double *dp, double *ll_ind)
+{
+    size_t nq = (size_t)N * K, np = (size_t)L * K * A;
+    double *Q = (double *)malloc(sizeof(double) * nq);
+    double *P = (double *)malloc(sizeof(double) * np);
+    double *gq = (double *)calloc(nq, sizeof(double));
+    double *gp = (double *)calloc(np, sizeof(double));
+    softmax_rows(qlog, Q, (size_t)N, K);
+    softmax_rows(plog, P, (size_t)L * K, A);
+    double total = 0.0;
+    for (int i = 0; i < N; i++) {
+        double lli = 0.0;
+        for (int line = 0; line < 2; line++)
+            for (int l = 0; l < L; l++) {
+                int a = geno[((size_t)i * 2 + line) * L + l];
+                if (a < 0) continue;
+                double S = 0.0;
+                for (int k = 0; k < K; k++)
+                    S += Q[(size_t)i * K + k] * P[((size_t)l * K + k) * A + a];
+                lli += log(S);
+                for (int k = 0; k < K; k++) {
+                    gq[(size_t)i * K + k] += P[((size_t)l * K + k) * A + a] / S;
+                    gp[((size_t)l * K + k) * A + a] += Q[(size_t)i * K + k] / S;
+                }
+            }
+        if (ll_ind) ll_ind[i] = lli;
+        total += lli;
+    }
+    for (int i = 0; i < N; i++) {
+        double s = 0.0;
+        for (int k = 0; k < K; k++) s += Q[(size_t)i * K + k] * gq[(size_t)i * K + k];
+        for (int k = 0; k < K; k++)
+            dq[(size_t)i * K + k] = Q[(size_t)i * K + k] * (gq[(size_t)i * K + k] - s);
+    }
+    for (size_t r = 0; r < (size_t)L * K; r++) {
+        double s = 0.0;
+        for (int a = 0; a < A; a++) s += P[r * A + a] * gp[r * A + a];
+        for (int a = 0; a < A; a++) dp[r * A + a] = P[r * A + a] * (gp[r * A + a] - s);
+    }
+    free(Q); free(P); free(gq); free(gp);
+    return total;
+}

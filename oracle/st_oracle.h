@@ -110,6 +110,13 @@ void orc_init_eps(int N, int L, int A, const int32_t *geno,
                   double fpriormean, int K, double *eps, double *F);
 double orc_est_logprob(double sumlikes, double sumsqlikes, int reps);
 
+/* --- gradient of ln P(D|Q,P), Z marginalised, w.r.t. softmax logits --------
+ * CalcLike.c:75-133 without the clamps; qlog [N][K], plog [L][K][A]; returns
+ * ln P(D); dq, dp as the logits; ll_ind [N] (may be NULL). */
+double orc_loglik_grad(int N, int L, int K, int A, const int32_t *geno,
+                       const double *qlog, const double *plog,
+                       double *dq, double *dp, double *ll_ind);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,11 @@ def lib():
         "st_set_state": ([vp, C.c_int, vp, sz], C.c_int),
         "st_field_bytes": ([vp, C.c_int], sz),
         "st_get_timing": ([vp, C.POINTER(C.c_double)], C.c_int),
+        "st_grad_create": ([vp, vp, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+        "st_grad_destroy": ([vp], C.c_int),
+        "st_loglik_grad": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "st_update_z_noalloc": ([C.c_int, vp, i32, i32, i32, i32, vp, vp, u64, i32, vp, vp, vp,
+                                 vp, vp, C.POINTER(sz)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -17,7 +17,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libstgpu.so")
 SOURCES = ["st_zpass.cu", "st_zpass_k1.cu", "st_zpass_k2.cu", "st_zpass_k3.cu",
            "st_zpass_k4.cu", "st_zpass_k5.cu", "st_zpass_k6.cu", "st_update.cu", "st_api.cu",
-           "st_noalloc.cu"]
+           "st_noalloc.cu", "st_grad.cu"]
 HEADERS = ["st_device.cuh", "st_types.h", "st_kernels.h", "st_zpass_fast.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -25,7 +25,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "-I" + os.path.join(ROOT, "include")]
 # The data pass must round every product and sum exactly like its host
 # restatement (bit-exact Z); the FP64 Metropolis/Dirichlet code may contract.
-PER_FILE = {"st_update.cu": ["-fmad=true"]}
+PER_FILE = {"st_update.cu": ["-fmad=true"], "st_grad.cu": ["-fmad=true"]}
 DEFAULT_FMAD = ["-fmad=false"]
 
 

@@ -1261,3 +1261,82 @@ extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
   cudaEventRecord(b->ev1, s);
   return ST_OK;
 }
+
+// ===========================================================================
+// gradient of ln P(D|Q,P) w.r.t. softmax logits
+// ===========================================================================
+struct st_grad {
+  st_ctx* ctx = nullptr;
+  st_data* data = nullptr;
+  int K = 0;
+  bool fp64 = false;
+  GradArgs a{};
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+};
+
+extern "C" int st_grad_create(st_ctx* ctx, st_data* data, int maxpops, int precision,
+                              st_grad** out) {
+  if (!ctx || !data || !out) return ST_ERR_ARG;
+  *out = nullptr;
+  if (precision != 32 && precision != 64)
+    return seterr(ctx, ST_ERR_ARG, "precision must be 32 or 64");
+  if (data->layout != kLayoutB2G)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the gradient needs biallelic 2-bit data");
+  if (grad_kclass(maxpops) == 0)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the gradient supports K = 1..%d", kGradMaxK);
+  cudaSetDevice(ctx->device);
+  st_grad* g = new st_grad();
+  g->ctx = ctx;
+  g->data = data;
+  g->K = maxpops;
+  g->fp64 = precision == 64;
+  GradArgs& a = g->a;
+  a.N = data->N; a.L = data->L; a.K = maxpops; a.wpr = data->wpr; a.g2 = data->g2;
+  grad_plan(a.N, a.L, &a);
+  const size_t es = g->fp64 ? 8 : 4;
+  const size_t NK = (size_t)a.N * a.K, LK2 = (size_t)a.L * a.K * 2;
+  struct { void** p; size_t b; } req[] = {
+      {&a.Q, NK * es}, {&a.P, LK2 * es}, {&a.gqpart, (size_t)a.lchunks * NK * es},
+      {(void**)&a.llpart, (size_t)a.lchunks * a.N * 8}, {&a.gppart, (size_t)a.ichunks * LK2 * es},
+      {(void**)&a.blockpart, (size_t)a.nblocks_q * 8}};
+  for (auto& r : req) {
+    int rc = ctx_alloc(ctx, r.b, r.p, &g->allocs, &g->bytes);
+    if (rc) {
+      for (void* p : g->allocs) cudaFree(p);
+      ctx->in_use -= g->bytes;
+      delete g;
+      return rc;
+    }
+  }
+  *out = g;
+  return ST_OK;
+}
+
+extern "C" int st_grad_destroy(st_grad* g) {
+  if (!g) return ST_ERR_ARG;
+  cudaSetDevice(g->ctx->device);
+  cudaStreamSynchronize(g->ctx->stream);
+  for (void* p : g->allocs) cudaFree(p);
+  g->ctx->in_use -= g->bytes;
+  delete g;
+  return ST_OK;
+}
+
+extern "C" int st_loglik_grad(st_grad* g, const void* q_logits, const void* p_logits, void* dq,
+                              void* dp, double* loglik, double* ll_ind) {
+  if (!g || !q_logits || !p_logits || !dq || !dp) return ST_ERR_ARG;
+  st_ctx* ctx = g->ctx;
+  cudaSetDevice(ctx->device);
+  GradArgs a = g->a;
+  a.qlog = q_logits;
+  a.plog = p_logits;
+  a.dq = dq;
+  a.dp = dp;
+  a.loglik = loglik;
+  a.ll_ind = ll_ind;
+  a.stream = ctx->stream;
+  Bracket br(ctx, ST_K_OTHER);
+  ctx->launches += 4 + (loglik ? 1 : 0);   // softmax, 2 passes, 2 finishes (+ total)
+  return cuda_check(ctx, launch_loglik_grad(a, g->fp64), "loglik_grad");
+}

@@ -51,4 +51,29 @@ int ctas_locus(const ChainDev& c, int block);
 int ctas_ind(const ChainDev& c, int block);
 int ctas_collect(const ChainDev& c, int block);
 
+// Gradient of ln P(D|Q,P) (Z marginalised) w.r.t. softmax logits, biallelic
+// 2-bit data.  T = float or double in every T buffer.
+constexpr int kGradMaxK = 16;
+struct GradArgs {
+  int N, L, K, wpr;
+  const uint32_t* g2;
+  const void* qlog;       // T [N][K]
+  const void* plog;       // T [L][K][2]
+  void* Q;                // T [N][K]    softmax workspace
+  void* P;                // T [L][K][2] softmax workspace
+  void* gqpart;           // T [lchunks][N][K]
+  double* llpart;         // [lchunks][N]
+  void* gppart;           // T [ichunks][L][K][2]
+  void* dq;               // T [N][K]
+  void* dp;               // T [L][K][2]
+  double* ll_ind;         // [N] or null
+  double* loglik;         // scalar or null
+  double* blockpart;      // [nblocks_q]
+  int lchunks, lchunk_len, ichunks, ichunk_len, nblocks_q;
+  cudaStream_t stream;
+};
+int grad_kclass(int K);                        // 0 if K is out of range
+void grad_plan(int N, int L, GradArgs* a);     // chunk sizes and counts
+cudaError_t launch_loglik_grad(const GradArgs& a, bool fp64);
+
 }  // namespace st

@@ -300,3 +300,33 @@ def test_dirichlet_p_matches_reference_in_distribution(orc, ref):
     for x in (do, dr):
         np.testing.assert_allclose(x.mean(0), mean, atol=4 * np.sqrt(var / len(x)).max())
         np.testing.assert_allclose(x.var(0), var, rtol=0.15)
+
+
+def test_loglik_grad_oracle_matches_finite_differences_and_calclike(orc, ref):
+    """The FP64 gradient restatement: ln P(D) equals the reference's CalcLike
+    (no clamp is reached here) and central differences match the gradient."""
+    from structure_b200 import synth
+    d = synth.snp_fmodel(30, 60, 3, np.array([.1, .2, .3]), .5, .05, 3)
+    g = d["geno"]
+    rng = np.random.default_rng(1)
+    ql, pl = rng.normal(size=(30, 3)), rng.normal(size=(60, 3, 2))
+    ll, dq, dp, lli = orc.loglik_grad(g, ql, pl)
+    Q = np.exp(ql) / np.exp(ql).sum(1, keepdims=True)
+    P = np.exp(pl) / np.exp(pl).sum(2, keepdims=True)
+    ref.set_globals(N=30, L=60, K=3, maxalleles=2)
+    lr = ref.lib.CalcLike(g.copy(), None, Q.copy(), P.copy(), None, None, None)
+    assert abs(ll - lr) <= 1e-12 * abs(lr)
+    assert abs(lli.sum() - ll) <= 1e-12 * abs(ll)
+    h = 1e-6
+    for i, k in [(0, 0), (5, 2), (29, 1)]:
+        a, b = ql.copy(), ql.copy()
+        a[i, k] += h
+        b[i, k] -= h
+        fd = (orc.loglik_grad(g, a, pl)[0] - orc.loglik_grad(g, b, pl)[0]) / (2 * h)
+        assert abs(fd - dq[i, k]) <= 1e-6 * max(1.0, abs(fd))
+    for l, k, a_ in [(0, 0, 0), (7, 2, 1), (59, 1, 0)]:
+        a, b = pl.copy(), pl.copy()
+        a[l, k, a_] += h
+        b[l, k, a_] -= h
+        fd = (orc.loglik_grad(g, ql, a)[0] - orc.loglik_grad(g, ql, b)[0]) / (2 * h)
+        assert abs(fd - dp[l, k, a_]) <= 1e-6 * max(1.0, abs(fd))
