@@ -143,7 +143,12 @@ typedef struct st_model {
     int32_t store_z;           /* keep Z in HBM (needed for st_get_state ST_F_Z) */
     int32_t precision;         /* 0: FP32 Z/P/Q arithmetic; 1: FP64 Z (U8 data) */
     int32_t tile_t, tile_w, tile_r; /* Z-pass tile (0 = choose): individuals per chunk, warps, locus blocks per CTA */
-    int32_t reserved[8];
+    int32_t mala;              /* 1: a Metropolis-adjusted Langevin move on every Q_i
+                                * after the Q update (Z summed out; biallelic
+                                * 2-bit data, K <= 16).  No reference counterpart. */
+    int32_t mala_target;       /* step-size adaptation target, acceptance x 1000
+                                * (0 = 574); steps adapt during burn-in only */
+    int32_t reserved[6];
 } st_model;
 
 int st_model_defaults(st_model *m);
@@ -168,6 +173,10 @@ int st_update_alpha(st_chain *c);  /* UpdateAlphaCL  src/Updates/UpdateAlpha.c:3
 int st_update_eps(st_chain *c);    /* UpdateEpsilonCL src/Updates/UpdateEpsilon.c:270-292 */
 int st_update_fst(st_chain *c);    /* UpdateFstCL    src/Updates/UpdateFst.c:100-140 */
 int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183         */
+/* One Metropolis-adjusted Langevin move on every Q_i with Z summed out and P
+ * fixed (chains created with st_model.mala; st_sweep runs it after the Q
+ * update).  No reference counterpart.                                        */
+int st_update_q_mala(st_chain *c);
 /* UpdateZ (src/Updates/UpdateZ.c:13-56) fed an explicit uniform array laid out
  * like the reference's randomArr: slot ind*L*2 + loc*2 + (draws so far at
  * that locus).  precision 64 reproduces the reference's FP64 arithmetic.
@@ -266,7 +275,8 @@ enum st_field {
     ST_F_STATS,        /* double [256]: like, sumlikes, sumsqlikes, ... */
     ST_F_REP,          /* int32: sweep counter */
     ST_F_ERR,          /* int32: device error word */
-    ST_F_DIMS          /* int32 [8]: N, L, K, A, layout, G, nchunks, ngroups */
+    ST_F_DIMS,         /* int32 [8]: N, L, K, A, layout, G, nchunks, ngroups */
+    ST_F_MALA_EPS      /* float [N]: Langevin step sizes (chains with st_model.mala) */
 };
 int st_get_state(st_chain *c, int field, void *host, size_t bytes);
 int st_set_state(st_chain *c, int field, const void *host, size_t bytes);

@@ -24,7 +24,7 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _ci, _cd, _cu32, _cu64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
 
-S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST = range(1, 10)
+S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA = range(1, 11)
 
 
 def rnd_words(w):
@@ -92,6 +92,8 @@ class Oracle:
         lib.orc_loglik_grad.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f64p, _f64p, _f64p, _f64p,
                                         _f64p]
         lib.orc_loglik_grad.restype = _cd
+        lib.orc_mala_step.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f32p, _f32p, _f64p, _ci, _f32p,
+                                      _cu64, _cu32, _ci, _cd, _f64p, _u8p]
 
     # -- RNG ---------------------------------------------------------------
     def philox(self, ctr, key):
@@ -248,6 +250,19 @@ class Oracle:
 
     def est_logprob(self, s, ss, reps):
         return self.lib.orc_est_logprob(s, ss, reps)
+
+    def mala_step(self, geno, Q, logQ, P, alpha, popalphas, eps, key, rep, burnin, target):
+        """One Langevin move on every Q_i; returns (Q, logQ, eps, logr, acc)."""
+        N, _, L = geno.shape
+        K = Q.shape[1]
+        Qo = np.ascontiguousarray(Q, np.float32).copy()
+        lQo = np.ascontiguousarray(logQ, np.float32).copy()
+        eo = np.ascontiguousarray(eps, np.float32).copy()
+        logr, acc = np.zeros(N), np.zeros(N, np.uint8)
+        self.lib.orc_mala_step(N, L, K, np.ascontiguousarray(geno, np.int32), Qo, lQo,
+                               np.ascontiguousarray(P, np.float32), np.ascontiguousarray(alpha, np.float64),
+                               int(popalphas), eo, key, rep, burnin, target, logr, acc)
+        return Qo, lQo, eo, logr, acc
 
     def loglik_grad(self, geno, qlog, plog):
         """ln P(D|softmax(qlog), softmax(plog)) and its gradient w.r.t. the

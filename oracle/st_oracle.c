@@ -722,3 +722,86 @@ double orc_loglik_grad(int N, int L, int K, int A, const int32_t *geno,
     free(Q); free(P); free(gq); free(gp);
     return total;
 }
+
+/* ll_i and dll/dQ_ik for one individual, Q and P given (P [L][K][2]). */
+static double ind_loglik_dq(int L, int K, const int32_t *geno, int i, int N_unused,
+                            const double *q, const float *P, double *g)
+{
+    (void)N_unused;
+    double ll = 0.0;
+    for (int k = 0; k < K; k++) g[k] = 0.0;
+    for (int line = 0; line < 2; line++)
+        for (int l = 0; l < L; l++) {
+            int a = geno[((size_t)i * 2 + line) * L + l];
+            if (a < 0) continue;
+            double S = 0.0;
+            for (int k = 0; k < K; k++) S += q[k] * (double)P[((size_t)l * K + k) * 2 + a];
+            ll += log(S);
+            for (int k = 0; k < K; k++) g[k] += (double)P[((size_t)l * K + k) * 2 + a] / S;
+        }
+    return ll;
+}
+
+void orc_mala_step(int N, int L, int K, const int32_t *geno, float *Q, float *logQ,
+                   const float *P, const double *alpha, int popalphas, float *eps,
+                   uint64_t key, uint32_t rep, int burnin, double target,
+                   double *logr, uint8_t *acc)
+{
+    double q[64], qp[64], g[64], gp[64], th[64], thp[64], al[64];
+    double A = 0.0;
+    for (int k = 0; k < K; k++) { al[k] = popalphas ? alpha[k] : alpha[0]; A += al[k]; }
+    for (int i = 0; i < N; i++) {
+        if (K < 2) { logr[i] = 0.0; acc[i] = 0; continue; }
+        float *Qi = Q + (size_t)i * K, *lQi = logQ + (size_t)i * K;
+        for (int k = 0; k < K; k++) q[k] = Qi[k];
+        double ll0 = ind_loglik_dq(L, K, geno, i, N, q, P, g);
+        double s = 0.0;
+        for (int k = 0; k < K; k++) s += q[k] * g[k];
+        for (int k = 0; k < K; k++) g[k] = q[k] * (g[k] - s);     /* dll/dlogit */
+        double e = eps[i], h = 0.5 * e * e, base = lQi[K - 1], m = 0.0;
+        for (int j = 0; j < K - 1; j++) {
+            uint32_t w[4];
+            philox4((uint32_t)i, 1u + (uint32_t)j, rep, ORC_S_MALA, key, w);
+            double xi = sqrt(-2.0 * log(orc_u01(w[0], w[1]))) * cos(TWO_PI * orc_u01(w[2], w[3]));
+            th[j] = (double)lQi[j] - base;
+            double grad = g[j] + al[j] - q[j] * A;
+            thp[j] = th[j] + h * grad + e * xi;
+            if (thp[j] > m) m = thp[j];
+        }
+        th[K - 1] = thp[K - 1] = 0.0;
+        double ss = 0.0;
+        for (int k = 0; k < K; k++) ss += exp(thp[k] - m);
+        for (int k = 0; k < K; k++) qp[k] = (double)(float)(exp(thp[k] - m) / ss);
+        double ll1 = ind_loglik_dq(L, K, geno, i, N, qp, P, gp);
+        s = 0.0;
+        for (int k = 0; k < K; k++) s += qp[k] * gp[k];
+        for (int k = 0; k < K; k++) gp[k] = qp[k] * (gp[k] - s);
+        double m0 = 0.0, m1 = 0.0, s0 = 0.0, s1 = 0.0;
+        for (int k = 0; k < K; k++) { if (th[k] > m0) m0 = th[k]; if (thp[k] > m1) m1 = thp[k]; }
+        for (int k = 0; k < K; k++) { s0 += exp(th[k] - m0); s1 += exp(thp[k] - m1); }
+        double lse0 = m0 + log(s0), lse1 = m1 + log(s1);
+        double lp0 = ll0, lp1 = ll1;
+        for (int k = 0; k < K; k++) { lp0 += al[k] * (th[k] - lse0); lp1 += al[k] * (thp[k] - lse1); }
+        double fwd = 0.0, bwd = 0.0;
+        for (int j = 0; j < K - 1; j++) {
+            double g0 = g[j] + al[j] - q[j] * A, g1 = gp[j] + al[j] - qp[j] * A;
+            double df = thp[j] - th[j] - h * g0, db = th[j] - thp[j] - h * g1;
+            fwd += df * df;
+            bwd += db * db;
+        }
+        double lr = lp1 - lp0 - (bwd - fwd) / (2.0 * e * e);
+        uint32_t w[4];
+        philox4((uint32_t)i, 0u, rep, ORC_S_MALA, key, w);
+        int a = log(orc_u01(w[0], w[1])) < lr;
+        logr[i] = lr;
+        acc[i] = (uint8_t)a;
+        if (a)
+            for (int k = 0; k < K; k++) { Qi[k] = (float)qp[k]; lQi[k] = (float)(thp[k] - lse1); }
+        if ((int)rep < burnin) {
+            double pa = lr >= 0.0 ? 1.0 : (lr == lr ? exp(lr) : 0.0);
+            double en = e * exp(pow((double)rep + 1.0, -0.6) * (pa - target));
+            en = en < 1e-6 ? 1e-6 : (en > 10.0 ? 10.0 : en);
+            eps[i] = (float)en;
+        }
+    }
+}

@@ -28,7 +28,7 @@ extern "C" {
 /* Philox stream identifiers: counter word 3 = stream << 24. */
 enum {
     ORC_S_INITZ = 1, ORC_S_Z = 2, ORC_S_P = 3, ORC_S_QG = 4, ORC_S_QM = 5,
-    ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9
+    ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10
 };
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
@@ -116,6 +116,18 @@ double orc_est_logprob(double sumlikes, double sumsqlikes, int reps);
 double orc_loglik_grad(int N, int L, int K, int A, const int32_t *geno,
                        const double *qlog, const double *plog,
                        double *dq, double *dp, double *ll_ind);
+
+/* --- Langevin move on Q (no reference counterpart) -------------------------
+ * One Metropolis-adjusted Langevin step per individual on the logits
+ * theta_j = log Q_j - log Q_{K-1} (j < K-1), target ll_i + sum_k alpha_k log Q_k,
+ * Z summed out, P fixed (P [L][K][2], biallelic).  Draws from the Philox
+ * stream ORC_S_MALA: normals at (i, 1+j), the acceptance uniform at (i, 0).
+ * Q, logQ are updated in place on acceptance; eps adapts when rep < burnin.
+ * logr [N] and acc [N] receive the log acceptance ratios and decisions. */
+void orc_mala_step(int N, int L, int K, const int32_t *geno, float *Q, float *logQ,
+                   const float *P, const double *alpha, int popalphas, float *eps,
+                   uint64_t key, uint32_t rep, int burnin, double target,
+                   double *logr, uint8_t *acc);
 
 #ifdef __cplusplus
 }

@@ -20,12 +20,13 @@ LAYOUT_AUTO, LAYOUT_U8, LAYOUT_B2G = 0, 1, 2
 
 (F_Q, F_LOGQ, F_TESTQ, F_LOGTESTQ, F_P, F_LOGP, F_EPS, F_F, F_ALPHA, F_LAMBDA, F_Z, F_N,
  F_M, F_LOGDIFF, F_QSUM, F_PSUM, F_SUMEPS, F_FSTSUM, F_SUMALPHA, F_SUMLAMBDA, F_ANCESTDIST,
- F_STATS, F_REP, F_ERR, F_DIMS) = range(1, 26)
+ F_STATS, F_REP, F_ERR, F_DIMS, F_MALA_EPS) = range(1, 27)
 
 # stats block offsets (csrc/st_types.h)
 ST_LIKE, ST_SUMLIKES, ST_SUMSQ, ST_NLIKE, ST_METROHITS = 0, 1, 2, 3, 4
 ST_ALPHA_T, ST_ALPHA_S = 6, 8
 ST_FST_DIFF, ST_FST_NEW, ST_ALPHA_LPD, ST_FST_LPD, ST_ALPHA_NEW = 40, 72, 104, 136, 168
+ST_MALA_ACC, ST_MALA_TRIES = 200, 201
 
 
 class StError(RuntimeError):
@@ -48,8 +49,9 @@ class Model(C.Structure):
         "metrofreq", "recessivealleles")] + \
         [(n, C.c_double) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
                                    "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
-        [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r")] + \
-        [("reserved", C.c_int32 * 8)]
+        [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r", "mala",
+                                  "mala_target")] + \
+        [("reserved", C.c_int32 * 6)]
 
 
 _lib = None
@@ -85,6 +87,7 @@ def lib():
         "st_update_z": ([vp], C.c_int), "st_update_alpha": ([vp], C.c_int),
         "st_update_eps": ([vp], C.c_int), "st_update_fst": ([vp], C.c_int),
         "st_collect": ([vp], C.c_int),
+        "st_update_q_mala": ([vp], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
         "st_sweep": ([vp, C.c_int], C.c_int), "st_run": ([vp], C.c_int),
         "st_sync": ([vp], C.c_int),
@@ -221,7 +224,7 @@ _DT = {F_Q: np.float32, F_LOGQ: np.float32, F_TESTQ: np.float32, F_LOGTESTQ: np.
        F_LOGDIFF: np.float64, F_QSUM: np.float64, F_PSUM: np.float64, F_SUMEPS: np.float64,
        F_FSTSUM: np.float64, F_SUMALPHA: np.float64, F_SUMLAMBDA: np.float64,
        F_ANCESTDIST: np.int32, F_STATS: np.float64, F_REP: np.int32, F_ERR: np.int32,
-       F_DIMS: np.int32}
+       F_DIMS: np.int32, F_MALA_EPS: np.float32}
 
 
 class Chain:
@@ -239,7 +242,8 @@ class Chain:
         return {F_Q: (N, K), F_LOGQ: (N, K), F_TESTQ: (N, K), F_LOGTESTQ: (N, K),
                 F_P: (L, K, A), F_LOGP: (L, K, A), F_EPS: (L, A), F_SUMEPS: (L, A),
                 F_Z: (N, 2, L), F_N: (L, K, A), F_M: (N, K), F_LOGDIFF: (N,),
-                F_QSUM: (N, K), F_PSUM: (L, K, A), F_STATS: (256,), F_DIMS: (8,)}.get(f, None)
+                F_QSUM: (N, K), F_PSUM: (L, K, A), F_STATS: (256,), F_DIMS: (8,),
+                F_MALA_EPS: (N,)}.get(f, None)
 
     def get(self, f):
         n = lib().st_field_bytes(self.h, f)
@@ -264,6 +268,7 @@ class Chain:
     def UpdateEpsilon(self): self.ctx.check(lib().st_update_eps(self.h))
     def UpdateFst(self): self.ctx.check(lib().st_update_fst(self.h))
     def DataCollection(self): self.ctx.check(lib().st_collect(self.h))
+    def UpdateQMala(self): self.ctx.check(lib().st_update_q_mala(self.h))
 
     def UpdateZInjected(self, uniforms, precision=64):
         u = np.ascontiguousarray(uniforms, np.float64)

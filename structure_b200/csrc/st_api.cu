@@ -60,6 +60,7 @@ struct st_chain {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   bool timed = false;
+  GradArgs mcur{}, mprop{};   // Langevin move: current and proposed Q passes
 };
 
 // Chains of one K capacity class: a contiguous slice of the batch table,
@@ -270,6 +271,10 @@ int check_model(st_ctx* ctx, const st_model* m) {
   if (m->burnin < 0 || m->numreps < 0) return seterr(ctx, ST_ERR_ARG, "negative BURNIN/NUMREPS");
   if (m->ancestdist && m->numboxes < 1) return seterr(ctx, ST_ERR_ARG, "NUMBOXES < 1");
   if (m->precision != 0 && m->precision != 1) return seterr(ctx, ST_ERR_ARG, "precision must be 0 or 1");
+  if (m->mala && (m->maxpops > kGradMaxK || m->precision != 0))
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move needs K <= %d and FP32", kGradMaxK);
+  if (m->mala_target < 0 || m->mala_target >= 1000)
+    return seterr(ctx, ST_ERR_ARG, "mala_target must be in 0..999 (acceptance x 1000)");
   return ST_OK;
 }
 
@@ -632,6 +637,23 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       {&ctr, (size_t)kCtrCount * 4}, {&rep, 4}, {&err, 4}, {&chain, sizeof(ChainDev)},
       {&prefix, 16}};
   if (model->store_z) bufs.push_back({&Z, (size_t)N * 2 * L});
+  void *mQp = nullptr, *mG = nullptr, *mGp = nullptr, *mLL = nullptr, *mLLp = nullptr,
+       *mTh = nullptr, *mThp = nullptr, *mEps = nullptr, *mgq = nullptr, *mll = nullptr,
+       *mbp = nullptr;
+  if (model->mala) {
+    if (!c->fast || A != 2) {
+      delete c;
+      return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move needs biallelic 2-bit data");
+    }
+    GradArgs& g = c->mcur;
+    g.N = N; g.L = L; g.K = K; g.wpr = data->wpr; g.g2 = data->g2;
+    grad_plan(N, L, &g);
+    for (Buf b : std::vector<Buf>{{&mQp, NK * 4}, {&mG, NK * 4}, {&mGp, NK * 4}, {&mLL, (size_t)N * 8},
+                                  {&mLLp, (size_t)N * 8}, {&mTh, NK * 8}, {&mThp, NK * 8},
+                                  {&mEps, (size_t)N * 4}, {&mgq, (size_t)g.lchunks * NK * 4},
+                                  {&mll, (size_t)g.lchunks * N * 8}, {&mbp, (size_t)g.nblocks_q * 8}})
+      bufs.push_back(b);
+  }
   if (model->ancestdist) bufs.push_back({&AD, NK * (size_t)h.numboxes * 4});
   for (auto& b : bufs) {
     rc = ctx_alloc(ctx, b.bytes, b.p, &c->allocs, &c->bytes);
@@ -648,6 +670,17 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   c->d_chain = (ChainDev*)chain;
   c->d_prefix = (int*)prefix;
   data->chains++;
+  h.mala = model->mala ? 1 : 0;
+  h.mala_target = (model->mala_target > 0 ? model->mala_target : 574) / 1000.0f;
+  if (model->mala) {
+    h.mQp = (float*)mQp; h.mG = (float*)mG; h.mGp = (float*)mGp; h.mLL = (double*)mLL;
+    h.mLLp = (double*)mLLp; h.mTh = (double*)mTh; h.mThp = (double*)mThp; h.mEps = (float*)mEps;
+    GradArgs& g = c->mcur;
+    g.P = h.P; g.Q = h.Q; g.gqpart = mgq; g.llpart = (double*)mll; g.blockpart = (double*)mbp;
+    g.dq = h.mG; g.ll_ind = h.mLL;
+    c->mprop = g;
+    c->mprop.Q = h.mQp; c->mprop.dq = h.mGp; c->mprop.ll_ind = h.mLLp;
+  }
 
   // ---- Initialization (src/Init.c:329-444, src/structure.c:51-58) ---------
   cudaStream_t s = ctx->stream;
@@ -687,6 +720,13 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   cudaMemsetAsync(h.err, 0, 4, s);
   cudaMemsetAsync(h.ldpart, 0, (size_t)h.ngroups * N * 8, s);
   if (h.AncestDist) cudaMemsetAsync(h.AncestDist, 0, NK * (size_t)h.numboxes * 4, s);
+  std::vector<float> e0;
+  if (h.mala) {
+    // first Langevin step ~ the posterior scale of a logit with 2L copies;
+    // adapted per individual during burn-in
+    e0.assign(N, (float)(1.0 / sqrt(2.0 * L + 1.0)));
+    cudaMemcpyAsync(h.mEps, e0.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+  }
   int zero = 0;
   cudaMemcpyAsync(c->d_prefix, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
   rc = upload_chain(c);
@@ -810,11 +850,30 @@ extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int 
 // ===========================================================================
 // sweeps
 // ===========================================================================
+// One Langevin move on every Q_i (Z summed out, P fixed): four kernels of the
+// gradient pass and two per-individual kernels.
+static int mala_step(st_chain* c) {
+  Bracket br(c->ctx, ST_K_OTHER);
+  c->ctx->launches += 5;   // 6 kernels, the bracket counted one
+  GradArgs a = c->mcur, b = c->mprop;
+  a.stream = b.stream = c->ctx->stream;
+  return cuda_check(c->ctx, launch_mala_step(a, b, c->d_chain), "mala");
+}
+
+extern "C" int st_update_q_mala(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.mala) return seterr(c->ctx, ST_ERR_STATE, "chain created without the Langevin move");
+  cudaSetDevice(c->ctx->device);
+  if (c->h.K < 2) return ST_OK;
+  return mala_step(c);
+}
+
 static int sweep_once(st_chain* c) {
   const int zflags = (c->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
                      (c->model.store_z ? kZfStoreZ : 0);
   int rc = locus(c, kLocP | kLocEps | kLocFst | kLocCollect);
   if (!rc) rc = update_q_impl(c, kIndAlpha | kIndCollect);
+  if (!rc && c->h.mala && c->h.K > 1) rc = mala_step(c);
   if (!rc) rc = zpass(c, kZNormal, zflags);
   if (!rc) c->host_rep++;
   return rc;
@@ -887,6 +946,7 @@ extern "C" size_t st_field_bytes(st_chain* c, int f) {
     case ST_F_STATS: return (size_t)kStSize * 8;
     case ST_F_REP: case ST_F_ERR: return 4;
     case ST_F_DIMS: return 32;
+    case ST_F_MALA_EPS: return h.mala ? (size_t)h.N * 4 : 0;
   }
   return 0;
 }
@@ -914,6 +974,7 @@ static void* field_ptr(st_chain* c, int f) {
     case ST_F_ANCESTDIST: return h.AncestDist;
     case ST_F_STATS: return h.stats;
     case ST_F_ERR: return h.err;
+    case ST_F_MALA_EPS: return h.mEps;
   }
   return nullptr;
 }
@@ -1172,6 +1233,9 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
     Bracket br(ctx, ST_K_IND);
     ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
   }
+  for (st_chain* c : b->chains)
+    if (c->h.mala && c->h.K > 1)
+      if (int rc = mala_step(c)) return rc;
   if (!b->fast)
     for (st_chain* c : b->chains) {
       ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
@@ -1281,7 +1345,7 @@ extern "C" int st_grad_create(st_ctx* ctx, st_data* data, int maxpops, int preci
   *out = nullptr;
   if (precision != 32 && precision != 64)
     return seterr(ctx, ST_ERR_ARG, "precision must be 32 or 64");
-  if (data->layout != kLayoutB2G)
+  if (data->layout != kLayoutB2G || data->A != 2)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "the gradient needs biallelic 2-bit data");
   if (grad_kclass(maxpops) == 0)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "the gradient supports K = 1..%d", kGradMaxK);

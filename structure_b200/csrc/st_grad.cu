@@ -24,6 +24,7 @@
 
 #include <cstdint>
 
+#include "st_device.cuh"
 #include "st_kernels.h"
 
 namespace st {
@@ -297,7 +298,163 @@ cudaError_t launch_t(const GradArgs& a) {
   return cudaGetLastError();
 }
 
+template <int KT>
+cudaError_t launch_q_kt(const GradArgs& a) {
+  const dim3 gi((a.N + kGradBlock - 1) / kGradBlock, a.lchunks);
+  grad_ind_kernel<float, KT><<<gi, kGradBlock, 0, a.stream>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Metropolis-adjusted Langevin move on Q_i, Z summed out, P fixed.
+// Coordinates: theta_j = log Q_j - log Q_{K-1}, j < K-1 (the last logit is
+// held at 0).  Target: ll_i(Q) + sum_k alpha_k log Q_k (the Dirichlet(alpha)
+// prior times the Jacobian prod_k Q_k of the map theta -> Q).  Its gradient
+// in theta_j is dll/dlogit_j + alpha_j - Q_j sum_k alpha_k.
+// Proposal theta' = theta + eps^2/2 grad + eps xi, xi ~ N(0, I); accepted
+// with the Metropolis-Hastings ratio of the Langevin proposal densities.
+// Random draws: Philox stream kSMala, counter (i, 1 + j) for xi_j and
+// (i, 0) for the acceptance uniform.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double normal_ab(uint32_t a, uint32_t b, uint32_t rep, uint32_t key) {
+  const U4 w = philox_s(a, b, rep, kSMala, key);
+  const double u1 = u01(w.x, w.y), u2 = u01(w.z, w.w);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+__device__ __forceinline__ double alpha_of(const ChainDev& ch, int k) {
+  return ch.popalphas ? ch.alpha[k] : ch.alpha[0];
+}
+
+__global__ void __launch_bounds__(kGradBlock) mala_propose_kernel(const ChainDev* __restrict__ chp) {
+  const ChainDev& ch = *chp;
+  const int i = blockIdx.x * kGradBlock + threadIdx.x;
+  if (i >= ch.N) return;
+  const int K = ch.K;
+  const uint32_t rep = (uint32_t)*ch.rep;
+  double A = 0.0;
+  for (int k = 0; k < K; k++) A += alpha_of(ch, k);
+  const float* lq = ch.logQ + (size_t)i * K;
+  const float* q = ch.Q + (size_t)i * K;
+  const float* g = ch.mG + (size_t)i * K;
+  double* th = ch.mTh + (size_t)i * K;
+  double* thp = ch.mThp + (size_t)i * K;
+  const double eps = ch.mEps[i];
+  const double base = lq[K - 1];
+  double m = 0.0;
+  for (int j = 0; j < K - 1; j++) {
+    const double t = (double)lq[j] - base;
+    const double grad = (double)g[j] + alpha_of(ch, j) - (double)q[j] * A;
+    const double tp = t + 0.5 * eps * eps * grad + eps * normal_ab((uint32_t)i, 1u + j, rep, ch.key);
+    th[j] = t;
+    thp[j] = tp;
+    m = tp > m ? tp : m;
+  }
+  th[K - 1] = thp[K - 1] = 0.0;
+  double s = 0.0;
+  for (int k = 0; k < K; k++) s += exp(thp[k] - m);
+  float* qp = ch.mQp + (size_t)i * K;
+  for (int k = 0; k < K; k++) qp[k] = (float)(exp(thp[k] - m) / s);
+}
+
+__global__ void __launch_bounds__(kGradBlock) mala_accept_kernel(const ChainDev* __restrict__ chp) {
+  const ChainDev& ch = *chp;
+  const int i = blockIdx.x * kGradBlock + threadIdx.x;
+  const int K = ch.K;
+  int acc = 0;
+  const bool valid = i < ch.N;
+  if (valid) {
+    const int rep = *ch.rep;
+    double A = 0.0;
+    for (int k = 0; k < K; k++) A += alpha_of(ch, k);
+    const double* th = ch.mTh + (size_t)i * K;
+    const double* thp = ch.mThp + (size_t)i * K;
+    const float* q = ch.Q + (size_t)i * K;
+    const float* qp = ch.mQp + (size_t)i * K;
+    const float* g = ch.mG + (size_t)i * K;
+    const float* gp = ch.mGp + (size_t)i * K;
+    double m0 = 0.0, m1 = 0.0;
+    for (int k = 0; k < K; k++) {
+      m0 = th[k] > m0 ? th[k] : m0;
+      m1 = thp[k] > m1 ? thp[k] : m1;
+    }
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = 0; k < K; k++) {
+      s0 += exp(th[k] - m0);
+      s1 += exp(thp[k] - m1);
+    }
+    const double lse0 = m0 + log(s0), lse1 = m1 + log(s1);
+    double lp0 = ch.mLL[i], lp1 = ch.mLLp[i];
+    for (int k = 0; k < K; k++) {
+      lp0 += alpha_of(ch, k) * (th[k] - lse0);
+      lp1 += alpha_of(ch, k) * (thp[k] - lse1);
+    }
+    const double eps = ch.mEps[i], h = 0.5 * eps * eps;
+    double fwd = 0.0, bwd = 0.0;
+    for (int j = 0; j < K - 1; j++) {
+      const double g0 = (double)g[j] + alpha_of(ch, j) - (double)q[j] * A;
+      const double g1 = (double)gp[j] + alpha_of(ch, j) - (double)qp[j] * A;
+      const double df = thp[j] - th[j] - h * g0;
+      const double db = th[j] - thp[j] - h * g1;
+      fwd += df * df;
+      bwd += db * db;
+    }
+    const double logr = lp1 - lp0 - (bwd - fwd) / (2.0 * eps * eps);
+    const U4 w = philox_s((uint32_t)i, 0u, (uint32_t)rep, kSMala, ch.key);
+    acc = log(u01(w.x, w.y)) < logr ? 1 : 0;
+    if (acc) {
+      float* qd = ch.Q + (size_t)i * K;
+      float* lqd = ch.logQ + (size_t)i * K;
+      for (int k = 0; k < K; k++) {
+        qd[k] = qp[k];
+        lqd[k] = (float)(thp[k] - lse1);
+      }
+    }
+    if (rep < ch.burnin) {
+      // Robbins-Monro adaptation toward the target acceptance (burn-in only)
+      const double pa = logr >= 0.0 ? 1.0 : (logr == logr ? exp(logr) : 0.0);
+      double e = eps * exp(pow((double)rep + 1.0, -0.6) * (pa - (double)ch.mala_target));
+      e = e < 1e-6 ? 1e-6 : (e > 10.0 ? 10.0 : e);
+      ch.mEps[i] = (float)e;
+    }
+  }
+  // acceptance count: one atomic per warp
+  const unsigned bal = __ballot_sync(0xffffffffu, acc);
+  const unsigned tries = __ballot_sync(0xffffffffu, valid);
+  if ((threadIdx.x & 31) == 0 && tries) {
+    atomicAdd(&ch.stats[kStMalaAcc], (double)__popc(bal));
+    atomicAdd(&ch.stats[kStMalaTries], (double)__popc(tries));
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_mala_step(const GradArgs& cur, const GradArgs& prop, const ChainDev* d_chain) {
+  const unsigned nb = (unsigned)((cur.N + kGradBlock - 1) / kGradBlock);
+  cudaError_t e = launch_grad_q(cur);
+  if (e != cudaSuccess) return e;
+  mala_propose_kernel<<<nb, kGradBlock, 0, cur.stream>>>(d_chain);
+  e = launch_grad_q(prop);
+  if (e != cudaSuccess) return e;
+  mala_accept_kernel<<<nb, kGradBlock, 0, cur.stream>>>(d_chain);
+  return cudaGetLastError();
+}
+
+// ll_i and dll/dlogit of Q only (FP32; P given directly, no softmax of P).
+cudaError_t launch_grad_q(const GradArgs& a) {
+  cudaError_t e = cudaSuccess;
+  switch (grad_kclass(a.K)) {
+    case 2: e = launch_q_kt<2>(a); break;
+    case 4: e = launch_q_kt<4>(a); break;
+    case 8: e = launch_q_kt<8>(a); break;
+    case 16: e = launch_q_kt<16>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return e;
+  grad_finish_q_kernel<float><<<(unsigned)((a.N + kGradBlock - 1) / kGradBlock), kGradBlock, 0,
+                                a.stream>>>(a);
+  return cudaGetLastError();
+}
 
 int grad_kclass(int K) {
   if (K < 1 || K > kGradMaxK) return 0;

@@ -75,5 +75,8 @@ struct GradArgs {
 int grad_kclass(int K);                        // 0 if K is out of range
 void grad_plan(int N, int L, GradArgs* a);     // chunk sizes and counts
 cudaError_t launch_loglik_grad(const GradArgs& a, bool fp64);
+cudaError_t launch_grad_q(const GradArgs& a);   // ll_i and dll/dlogit(Q) only, FP32
+// One Langevin move on every Q_i of a chain: cur.Q = chain Q, prop.Q = mQp.
+cudaError_t launch_mala_step(const GradArgs& cur, const GradArgs& prop, const ChainDev* d_chain);
 
 }  // namespace st

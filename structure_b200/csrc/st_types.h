@@ -15,7 +15,7 @@ constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
 // Philox stream ids (counter word 3 = id << 24).
 enum Stream : uint32_t {
   kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
-  kSAlpha = 7, kSEps = 8, kSFst = 9
+  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10
 };
 
 // Device error word bits.
@@ -43,6 +43,8 @@ enum : int {
   kStAlphaLpd = kStFstNew + kMaxPops,  // alpha log acceptance ratios
   kStFstLpd = kStAlphaLpd + kMaxPops,  // F log acceptance ratios
   kStAlphaNew = kStFstLpd + kMaxPops,  // alpha proposals
+  kStMalaAcc = kStAlphaNew + kMaxPops, // Langevin moves accepted
+  kStMalaTries,                        // Langevin moves proposed
   kStSize = 256
 };
 
@@ -87,6 +89,14 @@ struct ChainDev {
   int* rep;                             // device sweep counter
   int* err;                             // device error word
   const double* injected;               // parity uniforms (reference slots)
+  // optional Langevin move on Q (Z summed out)
+  int mala;
+  float mala_target;
+  float* mQp;                           // [N][K] proposed Q
+  float *mG, *mGp;                      // [N][K] dll/dlogit at current / proposed Q
+  double *mLL, *mLLp;                   // [N] ll_i at current / proposed Q
+  double *mTh, *mThp;                   // [N][K] logits (last fixed at 0)
+  float* mEps;                          // [N] step sizes
 };
 
 }  // namespace st

@@ -57,7 +57,7 @@ def _z(a, b, floor=0.0):
     return np.abs(a.mean(0) - b.mean(0)) / np.maximum(se, 1e-300)
 
 
-def _run_device(ctx, z, model):
+def _run_device(ctx, z, model, mala=0):
     geno = z["geno"].astype(np.int32)
     K = int(z["K"])
     R = len(z["sumlikes"])
@@ -65,7 +65,7 @@ def _run_device(ctx, z, model):
     mk = dict(maxpops=K, burnin=model["burnin"], numreps=model["numreps"],
               freqscorr=model["freqscorr"], inferalpha=model["inferalpha"], alpha=model["alpha"],
               alphapropsd=model["alphapropsd"], metrofreq=model["metrofreq"],
-              lambda_=model["lambda_"])
+              lambda_=model["lambda_"], mala=mala)
     for k in ("fpriormean", "fpriorsd"):
         if k in model:
             mk[k] = model[k]
@@ -75,6 +75,9 @@ def _run_device(ctx, z, model):
     res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[])
     for c in chains:
         assert c.sync() == 0
+        if mala:
+            st = c.get(api.F_STATS)
+            assert 0.2 < st[api.ST_MALA_ACC] / st[api.ST_MALA_TRIES] < 0.95
         st = c.get(api.F_STATS)
         assert st[api.ST_NLIKE] == model["numreps"]
         res["sumlikes"].append(st[api.ST_SUMLIKES])
@@ -89,12 +92,14 @@ def _run_device(ctx, z, model):
     return {k: np.array(v) for k, v in res.items()}
 
 
-@pytest.mark.parametrize("name", ["c1", "c2s"])
-def test_whole_runs_agree_with_reference_within_mcse(ctx, name):
+@pytest.mark.parametrize("name,mala", [("c1", 0), ("c2s", 0), ("c2s", 1)])
+def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
+    """mala=1: the same chains with the Langevin move on Q added to every
+    sweep still sample the reference's posterior."""
     z, model = _load(name)
     n = model["numreps"]
     Qtrue = z["Qtrue"]
-    dev = _run_device(ctx, z, model)
+    dev = _run_device(ctx, z, model, mala)
     sd = _summaries(dev["sumlikes"], dev["sumsqlikes"], dev["QSum"], dev["sumAlpha"],
                     dev["FstSum"], n, Qtrue)
     sr = _summaries(z["sumlikes"], z["sumsqlikes"], z["QSum"], z["sumAlpha"], z["FstSum"], n,
