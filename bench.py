@@ -384,6 +384,185 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Opt-in workloads (--workload): the other configurations' measurements.
+# ---------------------------------------------------------------------------
+def _ess(x):
+    """Effective sample size, Geyer's initial monotone sequence estimator."""
+    x = np.asarray(x, np.float64)
+    n = len(x)
+    x = x - x.mean()
+    if n < 4 or not np.any(x):
+        return float(n)
+    f = np.fft.rfft(x, 2 * n)
+    ac = np.fft.irfft(f * np.conj(f))[:n]
+    ac = ac / ac[0]
+    s, prev = 0.0, np.inf
+    for t in range(0, n - 1, 2):
+        g = ac[t] + ac[t + 1]
+        if g <= 0:
+            break
+        g = min(g, prev)
+        prev = g
+        s += g
+    return n / max(-1.0 + 2.0 * s, 1e-12)
+
+
+def run_grad(args):
+    """Config 4: forward + backward of ln P(D|Q,P) w.r.t. softmax logits,
+    N=5000, L=100,000, K=8, FP32, one evaluation per step."""
+    import torch
+    from structure_b200 import api, synth
+    from structure_b200.grad import LogLikGrad
+    d = synth.config4()
+    N, L, K = d["N"], d["L"], 8
+    ctx = api.Context(0)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
+                    layout=api.LAYOUT_B2G)
+    ev = LogLikGrad(ctx, data, K, precision=32)
+    g = torch.Generator(device="cuda").manual_seed(4)
+    ql = torch.randn(N, K, device="cuda", generator=g)
+    pl = torch.randn(L, K, 2, device="cuda", generator=g)
+    for _ in range(args.warmup):
+        ev(ql, pl)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        ev(ql, pl)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    codes = (d["packed"][:, :, None] >> (2 * np.arange(16, dtype=np.uint32))[None, None, :]) & 3
+    geno_obs = int((codes.reshape(L, -1)[:, :N] != 3).sum())
+    flops = geno_obs * 2 * (4 * K) * 2         # two passes x (2K + 2K FMA) x 2 FLOP
+    sm_mhz = clk["sm_mhz"] or 1965.0
+    peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    ach = flops / (ms / 1e3) / 1e12
+    # end to end: logits from pinned host memory, loglik and gradients back
+    qh, ph = ql.cpu().pin_memory(), pl.cpu().pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ll, dq, dp = ev(qh.to("cuda", non_blocking=True), ph.to("cuda", non_blocking=True))
+        ll.cpu(); dq.cpu(); dp.cpu()
+    e2e = args.steps / (time.perf_counter() - t0)
+    out = {"metric": "loglik+gradient evaluations/s", "value": round(1e3 / ms, 3),
+           "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic, seeded (config 4 generator)",
+           "config": {"workload": "differentiation N=5000 L=100000 K=8 (fwd + bwd, softmax logits)",
+                      "N": N, "L": L, "K": K, "l2": "inputs 125 MB packed > L2 after logits"},
+           "genotypes_per_s": round(geno_obs * 1e3 / ms, 1),
+           "roofline": {"bound": "fp32-fma", "achieved": round(ach, 3), "peak": round(peak, 2),
+                        "unit": "TFLOP/s", "frac": round(ach / peak, 4),
+                        "note": "4K FMA per genotype per pass, two passes; peak = 148 SM x 128 "
+                                "lanes x 2 x median SM clock (no tensor cores: K=8 contraction)"},
+           "e2e": {"value": round(e2e, 3), "unit": "evals/s",
+                   "h2d_bytes_per_step": int(qh.nbytes + ph.nbytes),
+                   "d2h_bytes_per_step": int(8 + qh.nbytes + ph.nbytes)},
+           "gpu_launches": 6 * args.steps, "clocks": clk}
+    print(json.dumps(out), flush=True)
+
+
+def run_mala(args):
+    """Config 4 mixing: Gibbs chain vs Gibbs + Langevin-on-Q chain, ESS per
+    second of device time for ln P(D) and for Q (median over entries)."""
+    from structure_b200 import api, synth
+    d = synth.config4()
+    N, L, K = d["N"], d["L"], 8
+    ctx = api.Context(0)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
+                    layout=api.LAYOUT_B2G)
+    burn, reps = max(args.warmup, 100), max(args.steps, 200)
+    sel = np.random.default_rng(0).choice(N, 64, replace=False)
+    res = {}
+    for name, mala in (("gibbs", 0), ("gibbs+mala", 1)):
+        m = api.model_defaults(maxpops=K, burnin=burn, numreps=reps, freqscorr=0, inferalpha=1,
+                               alpha=1.0, metrofreq=10, mala=mala)
+        c = api.Chain(ctx, data, m, 4000)
+        c.sweep(burn)
+        c.sync()
+        lnl, qs, t = [], [], 0.0
+        for _ in range(reps):
+            c.sweep(1)
+            c.sync()
+            t += c.timing_ms()
+            lnl.append(c.get(api.F_STATS)[api.ST_LIKE])
+            qs.append(c.get(api.F_Q)[sel])
+        qs = np.array(qs).reshape(reps, -1)
+        ess_l = _ess(lnl)
+        ess_q = float(np.median([_ess(qs[:, j]) for j in range(qs.shape[1])]))
+        st = c.get(api.F_STATS)
+        res[name] = {"sweeps": reps, "device_s": round(t / 1e3, 4),
+                     "ms_per_sweep": round(t / reps, 4),
+                     "ess_lnpd": round(ess_l, 1), "ess_lnpd_per_s": round(ess_l / (t / 1e3), 2),
+                     "ess_q_median": round(ess_q, 1),
+                     "ess_q_per_s": round(ess_q / (t / 1e3), 2),
+                     "mean_lnpd": round(float(np.mean(lnl)), 2)}
+        if mala:
+            res[name]["mala_acceptance"] = round(st[api.ST_MALA_ACC] / st[api.ST_MALA_TRIES], 4)
+        c.close()
+    out = {"metric": "ESS/s of ln P(D) and Q (Gibbs vs Gibbs + Langevin on Q)",
+           "value": res["gibbs+mala"]["ess_q_per_s"], "unit": "ESS/s (Q, median)",
+           "n_gpus": 1, "steps": reps, "warmup": burn, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (Z/P/Q) + f64 (MH)",
+           "data": "synthetic, seeded (config 4 generator)",
+           "config": {"workload": "mixing N=5000 L=100000 K=8, independent frequencies",
+                      "selected_q": "64 individuals x 8"},
+           "chains": res}
+    print(json.dumps(out), flush=True)
+
+
+def run_scale(args):
+    """Config 5: N=10,000, L=500,000, K=10 F model, POPALPHAS=1, 8 replicate
+    chains batched on one GPU under the context's HBM admission budget."""
+    import torch
+    from structure_b200 import api, synth
+    d = synth.config5()
+    N, L, K, B = d["N"], d["L"], 10, 8
+    ctx = api.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
+                    layout=api.LAYOUT_B2G)
+    mk = dict(maxpops=K, burnin=args.warmup, numreps=args.steps + 10, freqscorr=1,
+              inferalpha=1, popalphas=1, alpha=1.0, metrofreq=10, fpriormean=0.01,
+              fpriorsd=0.05, computeprob=1)
+    chains = [api.Chain(ctx, data, api.model_defaults(**mk), 5000 + r) for r in range(B)]
+    used, budget = ctx.memory()
+    b = api.Batch(ctx, chains)
+    b.sweep(args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.sweep(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    for c in chains:
+        assert c.sync() == 0
+    ms = e0.elapsed_time(e1)
+    codes_missing = 0.02
+    out = {"metric": METRIC, "value": round(B * args.steps / (ms / 1e3), 3), "unit": METRIC,
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
+           "data": "synthetic, seeded (config 5 generator)",
+           "config": {"workload": "scale N=10000 L=500000 K=10 F model, POPALPHAS=1, 8 chains",
+                      "N": N, "L": L, "K": K, "chains": B, "hbm_in_use_gb": round(used / 1e9, 2),
+                      "hbm_budget_gb": round(budget / 1e9, 2)},
+           "z_updates_per_s": round(B * args.steps / (ms / 1e3) * 2 * N * L * (1 - codes_missing), 1),
+           "clocks": clk}
+    b.close()
+    for c in chains:
+        c.close()
+    data.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -391,9 +570,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="snp", choices=["snp", "grad", "mala", "scale"],
+                    help="snp: the headline (default); grad: config 4 forward+backward; "
+                         "mala: config 4 ESS/s, Gibbs vs Gibbs+Langevin; scale: config 5")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload != "snp" and args.impl == "ours":
+        {"grad": run_grad, "mala": run_mala, "scale": run_scale}[args.workload](args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

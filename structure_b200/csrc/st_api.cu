@@ -194,7 +194,7 @@ int set_rep(st_chain* c, int rep) {
 
 // Z-pass tiling heuristic: W warps of 32 loci, T individuals per chunk (a
 // multiple of 16), R locus blocks per CTA.  Shared memory is kept under
-// 72 KB so three 256-thread CTAs fit on an SM (the kernel is built for 3).
+// 72 KB so three 256-thread CTAs fit on an SM where the K class allows.
 size_t zpass_smem_all(int KT, int K, int T, int W) {
   size_t s = 0;
   for (int mode : {kZNormal, kZMetro, kZInit, kZRecount, kZLike})
@@ -209,8 +209,19 @@ void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R)
   t = (t + 15) & ~15;
   const int np = (N + 15) & ~15;
   if (t > np) t = np;
-  const size_t budget = 72 * 1024;
-  while (m->tile_t <= 0 && t > 32 && zpass_smem_all(KT, K, t, w) > budget) t -= 16;
+  if (m->tile_t <= 0) {
+    // three CTAs per SM (72 KB each) if a tile of >= 128 individuals fits,
+    // else two (110 KB): the per-lane allele table of K classes 9-12 alone
+    // takes 61 KB, and small tiles rebuild it for every 32 individuals
+    auto fits = [&](int tt, size_t b) { return zpass_smem_all(KT, K, tt, w) <= b; };
+    int t3 = t;
+    while (t3 > 128 && !fits(t3, 72 * 1024)) t3 -= 16;
+    if (fits(t3, 72 * 1024)) {
+      t = t3;
+    } else {
+      while (t > 32 && !fits(t, 110 * 1024)) t -= 16;
+    }
+  }
   while (t > 16 && zpass_smem_all(KT, K, t, w) > 200 * 1024) t -= 16;
   int r = m->tile_r;
   if (r <= 0) {
@@ -227,15 +238,15 @@ void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R)
 
 int zpass(st_chain* c, int mode, int flags) {
   Bracket br(c->ctx, mode == kZMetro ? ST_K_METRO : (mode == kZNormal ? ST_K_ZPASS : ST_K_OTHER));
-  if (c->fast) {
-    LaunchSet ls = single(c, ctas_zpass_b2g(c->h));
-    return cuda_check(c->ctx, launch_zpass_b2g(ls, c->KT, c->h.tileW, mode, flags, c->zsmem),
-                      "zpass_b2g");
-  }
   st_ctx* ctx = c->ctx;
   if (mode == kZNormal || mode == kZInit || mode == kZRecount) {
     ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, ctx->stream));
     ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, ctx->stream));
+  }
+  if (c->fast) {
+    LaunchSet ls = single(c, ctas_zpass_b2g(c->h));
+    return cuda_check(c->ctx, launch_zpass_b2g(ls, c->KT, c->h.tileW, mode, flags, c->zsmem),
+                      "zpass_b2g");
   }
   if (mode == kZMetro)
     ST_CUDA(ctx, cudaMemsetAsync(c->h.ldpart, 0, sizeof(double) * (size_t)c->h.N, ctx->stream));
@@ -614,8 +625,8 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     h.nchunks = 1;
     h.ngroups = 1;
   }
-  h.cnt_chunks = h.nchunks;
-  h.cnt_groups = h.ngroups;
+  h.cnt_chunks = 1;
+  h.cnt_groups = 1;
 
   const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A, LA = (size_t)L * A;
   const int zctas = c->fast ? ctas_zpass_b2g(h) : ctas_zpass_u8(h, 256);
@@ -629,8 +640,8 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   std::vector<Buf> bufs = {
       {&Q, NK * 4}, {&logQ, NK * 4}, {&TQ, NK * 4}, {&lTQ, NK * 4}, {&P, LKA * 4},
       {&logP, LKA * 4}, {&eps, LA * 8}, {&F, (size_t)K * 8}, {&alpha, (size_t)K * 8},
-      {&lambda, (size_t)K * 8}, {&npart, (size_t)h.nchunks * LKA * 4},
-      {&mpart, (size_t)h.ngroups * NK * 4}, {&ldpart, (size_t)h.ngroups * N * 8},
+      {&lambda, (size_t)K * 8}, {&npart, LKA * 4},
+      {&mpart, NK * 4}, {&ldpart, (size_t)h.ngroups * N * 8},
       {&QSum, NK * 8}, {&PSum, LKA * 8}, {&SumEps, LA * 8}, {&FstSum, (size_t)K * 8},
       {&sumAlpha, (size_t)K * 8}, {&sumlambda, (size_t)K * 8}, {&stats, (size_t)kStSize * 8},
       {&likepart, (size_t)zctas * 8}, {&redpart, (size_t)nred * 8},
@@ -1019,12 +1030,12 @@ extern "C" int st_get_state(st_chain* c, int f, void* host, size_t bytes) {
     return ST_OK;
   }
   if (f == ST_F_LOGDIFF) {
-    std::vector<double> part((size_t)h.cnt_groups * h.N);
+    std::vector<double> part((size_t)h.ngroups * h.N);
     ST_CUDA(c->ctx, cudaMemcpy(part.data(), h.ldpart, part.size() * 8, cudaMemcpyDeviceToHost));
     double* o = (double*)host;
     for (int i = 0; i < h.N; i++) {
       double s2 = 0.0;
-      for (int g = 0; g < h.cnt_groups; g++) s2 += part[(size_t)g * h.N + i];
+      for (int g = 0; g < h.ngroups; g++) s2 += part[(size_t)g * h.N + i];
       o[i] = s2;
     }
     return ST_OK;
@@ -1236,11 +1247,10 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
   for (st_chain* c : b->chains)
     if (c->h.mala && c->h.K > 1)
       if (int rc = mala_step(c)) return rc;
-  if (!b->fast)
-    for (st_chain* c : b->chains) {
-      ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
-      ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
-    }
+  for (st_chain* c : b->chains) {   // the Z pass adds into cleared histograms
+    ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
+    ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
+  }
   {
     Bracket br(ctx, ST_K_ZPASS);
     if (b->fast) {

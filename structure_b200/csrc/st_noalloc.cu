@@ -16,8 +16,9 @@
 //    whose partials need more is rejected with ST_ERR_ADMISSION.
 //  * Every call on a device uses the same array, and it keeps what the last
 //    call left.  The call itself rewrites the header (chain descriptor, the
-//    done counter of the last-CTA protocol, the error word), which must start
-//    at zero; every partial it reads back is written by the same call first.
+//    done counter of the last-CTA protocol, the error word) and clears the two
+//    count histograms the Z pass adds into, all of which must start at zero;
+//    the ln P(D) partials are written before they are read.
 //    Two calls whose kernels overlap on the GPU (different streams, or
 //    different host threads without ordering) race on the array.
 //  * The first call on a device looks up the array's device address with
@@ -66,8 +67,9 @@ int k_class(int K) {
 }
 
 // Same tile as a chain created with tile_t = tile_r = 0: T individuals per
-// chunk (shared memory of every Z-pass mode under 72 KB), the K class's
-// width, and R locus blocks per CTA for ~6 CTAs per SM.
+// chunk (shared memory of every Z-pass mode under 72 KB, or 110 KB where a
+// tile of 128 does not fit), the K class's width, and R locus blocks per CTA
+// for ~6 CTAs per SM.
 void pick_tile(int KT, int K, int N, int L, int* T, int* W, int* R) {
   const int w = zpass_b2g_width(KT);
   auto smem_all = [&](int t) {
@@ -79,7 +81,13 @@ void pick_tile(int KT, int K, int N, int L, int* T, int* W, int* R) {
   int t = 256;
   const int np = (N + 15) & ~15;
   if (t > np) t = np;
-  while (t > 32 && smem_all(t) > 72 * 1024) t -= 16;
+  int t3 = t;
+  while (t3 > 128 && smem_all(t3) > 72 * 1024) t3 -= 16;
+  if (smem_all(t3) <= 72 * 1024) {
+    t = t3;
+  } else {
+    while (t > 32 && smem_all(t) > 110 * 1024) t -= 16;
+  }
   const long lblocks = (L + 32 * w - 1) / (32 * w);
   const long nch = (N + t - 1) / t;
   long r = (lblocks * nch) / (148L * 3 * 2);
@@ -90,8 +98,8 @@ void pick_tile(int KT, int K, int N, int L, int* T, int* W, int* R) {
   *R = (int)r;
 }
 
-// Sums the per-CTA partials into the caller's outputs:
-// n_out[l][k][a] = sum_c npart[c][k][a][l], m_out[i][k] = sum_g mpart[g][i][k].
+// Copies the Z pass's histograms into the caller's layouts:
+// n_out[l][k][a] = npart[k][a][l], m_out[i][k] = mpart[i][k].
 __global__ void noalloc_sum_kernel(const Head* head, const int32_t* npart, const int32_t* mpart,
                                    const double* stats, int32_t* n_out, int32_t* m_out,
                                    double* like_out, int32_t* err_out) {
@@ -101,15 +109,10 @@ __global__ void noalloc_sum_kernel(const Head* head, const int32_t* npart, const
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < nn + nm; j += stride) {
     if (j < nn) {
-      int32_t s = 0;
-      for (int c = 0; c < h.nchunks; c++) s += npart[(size_t)c * nn + j];
       const size_t l = j % L, ka = j / L;
-      n_out[l * (size_t)K * 2 + ka] = s;
+      n_out[l * (size_t)K * 2 + ka] = npart[j];
     } else {
-      const size_t q = j - nn;
-      int32_t s = 0;
-      for (int g = 0; g < h.ngroups; g++) s += mpart[(size_t)g * nm + q];
-      m_out[q] = s;
+      m_out[j - nn] = mpart[j - nn];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -141,12 +144,14 @@ int run(int device, const uint32_t* g2, int wpr, int N, int L, int K, const floa
   const int ngroups = (lblocks + R - 1) / R;
   const size_t ntiles = (size_t)nchunks * ngroups;
 
-  // scratch layout: head | stats | likepart | npart | mpart
+  // scratch layout: head | stats | likepart | n histogram | m histogram
   const size_t o_stats = align256(sizeof(Head));
   const size_t o_like = o_stats + align256(sizeof(double) * kStSize);
   const size_t o_n = o_like + align256(sizeof(double) * ntiles);
-  const size_t o_m = o_n + align256(sizeof(int32_t) * (size_t)nchunks * K * 2 * L);
-  const size_t need = o_m + align256(sizeof(int32_t) * (size_t)ngroups * N * K);
+  const size_t nbytes = sizeof(int32_t) * (size_t)K * 2 * L;
+  const size_t mbytes = sizeof(int32_t) * (size_t)N * K;
+  const size_t o_m = o_n + align256(nbytes);
+  const size_t need = o_m + align256(mbytes);
   if (scratch_bytes) *scratch_bytes = need;
   if (need > kScratchBytes) return ST_ERR_ADMISSION;
 
@@ -174,7 +179,7 @@ int run(int device, const uint32_t* g2, int wpr, int N, int L, int K, const floa
   }
   h.tileT = T; h.tileW = W; h.tileR = R;
   h.nchunks = nchunks; h.ngroups = ngroups;
-  h.cnt_chunks = nchunks; h.cnt_groups = ngroups;
+  h.cnt_chunks = 1; h.cnt_groups = 1;
   h.g2 = g2;
   h.Q = const_cast<float*>(Q);
   h.P = const_cast<float*>(P);
@@ -190,6 +195,10 @@ int run(int device, const uint32_t* g2, int wpr, int N, int L, int K, const floa
 
   // pageable source: the call returns once the bytes are staged
   if (cudaMemcpyAsync(dhead, &hd, sizeof hd, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    return ST_ERR_CUDA;
+  // the Z pass adds into the histograms: they must start at zero
+  if (cudaMemsetAsync(s + o_n, 0, nbytes, stream) != cudaSuccess ||
+      cudaMemsetAsync(s + o_m, 0, mbytes, stream) != cudaSuccess)
     return ST_ERR_CUDA;
 
   LaunchSet ls;

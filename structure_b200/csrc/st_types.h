@@ -64,7 +64,8 @@ struct ChainDev {
   uint32_t key;             // seed32: low word of splitmix64(chain seed)
   // Z-pass tiling: T individuals per chunk, W warps, R locus blocks per CTA
   int tileT, tileW, tileR, nchunks, ngroups;
-  // count partials currently held (producer's decomposition)
+  // count histogram slices summed by the consumers (1: every producer adds
+  // into slice 0); Metropolis log-ratio partials have ngroups slices
   int cnt_chunks, cnt_groups;
   // data
   const uint32_t* g2;
@@ -77,8 +78,8 @@ struct ChainDev {
   double *eps;                          // L*A
   double *F, *alpha, *lambda;           // K
   uint8_t* Z;                           // N*2*L (optional)
-  int32_t* npart;                       // [chunks][K][A][L]
-  int32_t* mpart;                       // [groups][N][K]
+  int32_t* npart;                       // [K][A][L] allele counts
+  int32_t* mpart;                       // [N][K] ancestry counts
   double* ldpart;                       // [groups][N]
   // accumulators
   double *QSum, *PSum, *SumEps, *FstSum, *sumAlpha, *sumlambda;

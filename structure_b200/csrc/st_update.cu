@@ -291,7 +291,7 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
   } else if (mode == kIndAccept) {
     double ld = 0.0;
     if (ivalid)
-      for (int g = 0; g < ch.cnt_groups; g++) ld += ch.ldpart[(size_t)g * N + i];
+      for (int g = 0; g < ch.ngroups; g++) ld += ch.ldpart[(size_t)g * N + i];
     bool acc = false;
     if (ivalid) {
       const U4 w = philox_s((uint32_t)i, 0, (uint32_t)rep, kSQMA, key);

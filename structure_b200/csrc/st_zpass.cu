@@ -13,9 +13,10 @@
 //   Q rows of the chunk in shared memory (broadcast reads).  n[l][k][a] is a
 //   lane-private shared-memory histogram (lane-minor, conflict-free); m[i][k]
 //   is reduced across the warp's 32 loci with one redux.sync per step on
-//   7-bit packed fields.  Counts leave as per-CTA partials (plain stores, no
-//   global atomics): npart[chunk][k][a][l] and mpart[group][i][k], summed by
-//   the consumers.
+//   7-bit packed fields.  Counts are added into one histogram per chain,
+//   n[k][a][l] and m[i][k], with integer reductions (cleared by the host
+//   before the pass); the Metropolis log ratios leave as per-CTA partials
+//   ldpart[group][i].
 #include <cstdio>
 #include "st_device.cuh"
 #include "st_kernels.h"

@@ -8,9 +8,10 @@
 //   shared-memory table, Q rows of the chunk in shared memory (broadcast
 //   reads).  n[l][k][a] is a lane-private shared-memory histogram (lane-minor,
 //   conflict-free); m[i][k] is reduced across the warp's 32 loci with
-//   redux.sync on 7-bit packed fields.  Counts leave as per-CTA partials
-//   (plain stores, no global atomics): npart[chunk][k][a][l] and
-//   mpart[group][i][k], summed by the consumers.
+//   redux.sync on 7-bit packed fields.  Each CTA adds its nonzero counts
+//   into the chain's single histograms n[k][a][l] and m[i][k] with integer
+//   reductions in L2 (exact, so order-free); the host clears them before the
+//   pass.
 #pragma once
 #include "st_device.cuh"
 #include "st_kernels.h"
@@ -429,10 +430,11 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     if (kCounts) {
       __syncwarp();
       if (valid) {
-        const size_t cbase = (size_t)ichunk * K * A;
         for (int k = 0; k < K; k++) {
-          ch.npart[((cbase + (size_t)k * A) + 0) * L + l] = mycol[(k * 2) * NW32];
-          if (A > 1) ch.npart[((cbase + (size_t)k * A) + 1) * L + l] = mycol[(k * 2 + 1) * NW32];
+          const int v0 = mycol[(k * 2) * NW32];
+          if (v0) atomicAdd(&ch.npart[((size_t)k * A + 0) * L + l], v0);
+          const int v1 = mycol[(k * 2 + 1) * NW32];
+          if (A > 1 && v1) atomicAdd(&ch.npart[((size_t)k * A + 1) * L + l], v1);
         }
       }
     }
@@ -440,10 +442,11 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   }
   __syncthreads();
   if (kCounts) {
-    int* dst = ch.mpart + ((size_t)grp * N + i0) * K;
+    int* dst = ch.mpart + (size_t)i0 * K;
     for (int idx = threadIdx.x; idx < nT * K; idx += NW32) {
       const int ii = idx / K;
-      dst[idx] = sM[ii * KT + (idx - ii * K)];
+      const int v = sM[ii * KT + (idx - ii * K)];
+      if (v) atomicAdd(&dst[idx], v);
     }
   }
   if (MODE == kZMetro) {

@@ -89,13 +89,14 @@ def microsat(N=200, L=100, K=3, amin=2, amax=10, qalpha=0.5, missing=0.05, seed=
 
 
 def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=1024,
-               want_int32=True):
+               want_int32=True, indep_beta=None):
     """Configs 2/3/5: biallelic SNPs under the F model; whole genotypes missing.
     Genotype code g = copies of allele 1 (0,1,2; 3 = missing).  At each locus the
     allele labels are chosen so that the first non-missing copy (scanning
     individuals, then lines) is allele 0, so the reference's recoding
     (datain.c:824-904) leaves the codes unchanged; heterozygotes are stored
-    0 on line 0, 1 on line 1."""
+    0 on line 0, 1 on line 1.  indep_beta=(a, b): independent frequencies
+    P_kl ~ Beta(a, b) instead of the F model (config 4)."""
     rng = np.random.default_rng(seed)
     F = np.asarray(F, np.float64)
     Q = rng.dirichlet(np.full(K, qalpha), size=N)
@@ -111,7 +112,10 @@ def snp_fmodel(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), chunk=1024,
         l1 = min(L, l0 + chunk)
         n = l1 - l0
         p = np.clip(rng.beta(p_beta[0], p_beta[1], size=n), 1e-4, 1 - 1e-4)
-        P1 = rng.beta(p[None, :] * fr[:, None], (1 - p[None, :]) * fr[:, None])  # [K, n]
+        if indep_beta is None:
+            P1 = rng.beta(p[None, :] * fr[:, None], (1 - p[None, :]) * fr[:, None])  # [K, n]
+        else:
+            P1 = rng.beta(indep_beta[0], indep_beta[1], size=(K, n))
         u = rng.random((N, 2, n), dtype=np.float32)
         z = np.zeros((N, 2, n), np.int8)
         for k in range(K - 1):
@@ -192,3 +196,19 @@ def config3_datasets(seed=None, want_int32=True):
         F = rng.uniform(0.02, 0.2, size=4)
         out.append(snp_fmodel(N, L, 4, F, 0.3, 0.03, base * 10 + s + 100, want_int32=want_int32))
     return out
+
+
+def config4(N=5000, L=100000, seed=None, want_int32=False):
+    """Config 4: N=5000, L=100,000 biallelic SNPs, K=8, Q ~ Dir(0.2), independent
+    frequencies P ~ Beta(0.5, 0.5), no missing data."""
+    return snp_fmodel(N, L, 8, np.full(8, 0.5), 0.2, 0.0,
+                      DATA_SEED_BASE + 4 if seed is None else seed, want_int32=want_int32,
+                      indep_beta=(0.5, 0.5))
+
+
+def config5(N=10000, L=500000, seed=None, want_int32=False):
+    """Config 5: N=10,000, L=500,000 biallelic SNPs, 2% missing, K=10 F model with
+    F_k ~ U[0.01, 0.3], Q ~ Dir(0.1)."""
+    rng = np.random.default_rng(DATA_SEED_BASE + 5 if seed is None else seed)
+    F = rng.uniform(0.01, 0.3, 10)
+    return snp_fmodel(N, L, 10, F, 0.1, 0.02, int(rng.integers(1 << 31)), want_int32=want_int32)
