@@ -64,15 +64,23 @@ __global__ void grad_softmax_kernel(GradArgs a) {
   }
 }
 
+// FP32 uses the hardware reciprocal and logarithm (a few ulp; the gradient
+// is checked to 2e-4 of its largest entry); FP64 keeps IEEE division and log.
+__device__ __forceinline__ float div_t(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double div_t(double a, double b) { return a / b; }
+__device__ __forceinline__ float log_t(float a) { return __logf(a); }
+__device__ __forceinline__ double log_t(double a) { return log(a); }
+
 // Weights of one genotype: copies of allele 0 / S0 and of allele 1 / S1, and
-// its log-likelihood terms.  gt: 0 = 0/0, 1 = 0/1, 2 = 1/1.
+// its log-likelihood terms.  gt: 0 = 0/0, 1 = 0/1, 2 = 1/1, 3 = missing (all
+// zero, so callers need no branch).
 template <typename T>
 __device__ __forceinline__ void genotype_terms(uint32_t gt, T s0, T s1, T& w0, T& w1, T& ll) {
   const T c0 = gt == 0u ? T(2) : (gt == 1u ? T(1) : T(0));
-  const T c1 = T(2) - c0;
-  w0 = c0 > T(0) ? c0 / s0 : T(0);
-  w1 = c1 > T(0) ? c1 / s1 : T(0);
-  ll = (c0 > T(0) ? c0 * log(s0) : T(0)) + (c1 > T(0) ? c1 * log(s1) : T(0));
+  const T c1 = gt == 2u ? T(2) : (gt == 1u ? T(1) : T(0));
+  w0 = c0 > T(0) ? div_t(c0, s0) : T(0);
+  w1 = c1 > T(0) ? div_t(c1, s1) : T(0);
+  ll = (c0 > T(0) ? c0 * log_t(s0) : T(0)) + (c1 > T(0) ? c1 * log_t(s1) : T(0));
 }
 
 template <typename T, int KT>
@@ -111,9 +119,9 @@ __global__ void __launch_bounds__(kGradBlock) grad_ind_kernel(GradArgs a) {
     __syncthreads();
     if (valid) {
       T llb = T(0);
+#pragma unroll 4
       for (int j = 0; j < nj; j++) {
         const uint32_t gt = (sW[j][myc] >> sh) & 3u;
-        if (gt == 3u) continue;
         T s0 = T(0), s1 = T(0);
 #pragma unroll
         for (int k = 0; k < KT; k++) {
@@ -169,9 +177,9 @@ __global__ void __launch_bounds__(kGradBlock) grad_loc_kernel(GradArgs a) {
     for (int wj = 0; wj < ni; wj += 16) {
       const uint32_t w = __ldg(row + ((ib + wj) >> 4));
       const int nh = min(16, ni - wj);
+#pragma unroll 4
       for (int h = 0; h < nh; h++) {
         const uint32_t gt = (w >> (2 * h)) & 3u;
-        if (gt == 3u) continue;
         const T* q = sQ[wj + h];
         T s0 = T(0), s1 = T(0);
 #pragma unroll
