@@ -1,0 +1,121 @@
+"""The reference's own front end, for checking the structure_b200 front end.
+
+TEST INFRASTRUCTURE ONLY (the checker, never the product): runs, in this
+process, the reference's parameter reader (src/params.c GetParams), data
+reader and recoder (src/datain.c ReadInputFile, FindMaxAlleles and
+CountAlleles, as src/structure.c:266-320 and src/Init.c:392-396 call them) and
+result writer (src/output.c OutPutResults), all compiled from the reference
+sources into oracle/_ref/libstref.so.  The reference keeps its state in
+process globals and exits on errors, so each scenario runs in its own process:
+
+    python oracle/ref_front.py <workdir> <spec.json>
+
+spec: {"argv": [...], "read_data": bool, "sums": "<npz in workdir>" or null,
+       "rep": int}.  The working directory is <workdir> (the reference opens
+its files relative to it).  Results go to <workdir>/ref_out.json and
+<workdir>/ref_data.npz; OutPutResults writes OUTFILE_f (and OUTFILE_q).
+"""
+import ctypes as C
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+INT_KEYS = ["NUMINDS", "NUMLOCI", "MISSING", "LABEL", "POPDATA", "MARKERNAMES", "PHASEINFO",
+            "MAPDISTANCES", "MARKOVPHASE", "LINES", "ONEROWPERIND", "RECESSIVEALLELES",
+            "NOTAMBIGUOUS", "POPFLAG", "PHENOTYPE", "EXTRACOLS", "MAXPOPS", "BURNIN", "NUMREPS",
+            "USEPOPINFO", "PFROMPOPFLAGONLY", "INFERALPHA", "INFERLAMBDA", "POPSPECIFICLAMBDA",
+            "POPALPHAS", "COMPUTEPROB", "NOADMIX", "ADMBURNIN", "PHASED", "PRINTQHAT",
+            "PRINTQSUM", "UPDATEFREQ", "PRINTLIKES", "INTERMEDSAVE", "PRINTKLD", "PRINTNET",
+            "PRINTLAMBDA", "ECHODATA", "ANCESTDIST", "NUMBOXES", "GENSBACK", "FREQSCORR",
+            "ONEFST", "UNIFPRIORALPHA", "STARTATPOPINFO", "RANDOMIZE", "LINKAGE", "METROFREQ",
+            "REPORTHITRATE", "NOQS", "POSTERIOR", "PICTUREFILE", "INDIVIDUALR", "NUMSIMSTATS",
+            "POOLFREQ", "LOCUSxONLY", "PHENOTYPECOL", "MISSINGPHENO", "LOCPRIOR",
+            "UPDATELOCPRIOR", "LOCISPOP", "LOCDATA", "SEED"]
+REAL_KEYS = ["ANCESTPINT", "MIGRPRIOR", "ALPHA", "LOG10RPROPSD", "LOG10RMIN", "LOG10RMAX",
+             "LOG10RSTART", "FPRIORMEAN", "FPRIORSD", "LAMBDA", "ALPHAMAX", "ALPHAPRIORA",
+             "ALPHAPRIORB", "ALPHAPROPSD", "EMERROR", "LOCPRIORINIT", "MAXLOCPRIOR",
+             "LOCPRIORSTEP"]
+
+
+class IND(C.Structure):
+    _fields_ = [("Label", C.c_char * 12), ("Population", C.c_int), ("PopFlag", C.c_int),
+                ("Phenotype", C.c_int), ("Location", C.c_int), ("myloc", C.c_int)]
+
+
+def main(workdir, specpath):
+    with open(specpath) as f:
+        spec = json.load(f)
+    lib = C.CDLL(os.path.join(HERE, "_ref", "libstref.so"))
+    os.chdir(workdir)
+    argv = [a.encode() for a in spec["argv"]]
+    cargv = (C.c_char_p * len(argv))(*argv)
+    lib.GetParams.argtypes = [C.c_int, C.c_int, C.c_void_p]
+    lib.GetParams(0, len(argv), cargv)
+    g = lambda n, t=C.c_int: t.in_dll(lib, n)
+    out = {"int": {k: g(k).value for k in INT_KEYS},
+           "real": {k: g(k, C.c_double).value for k in REAL_KEYS},
+           "str": {k: (C.c_char * 201).in_dll(lib, k).value.decode() for k in ("DATAFILE", "OUTFILE")}}
+    if spec.get("read_data"):
+        N, L, LINES = g("NUMINDS").value, g("NUMLOCI").value, g("LINES").value
+        geno = (C.c_int * (N * LINES * L))()
+        mapd = (C.c_double * L)()
+        names = (C.c_char * (L * 15))()
+        inds = (IND * N)()
+        phase = (C.c_double * (N * L))()
+        rec = (C.c_int * L)()
+        lib.ReadInputFile(geno, mapd, names, inds, phase, rec)
+        lib.FindMaxAlleles.restype = C.c_int
+        A = lib.FindMaxAlleles(geno, rec)
+        g("MAXALLELES").value = A
+        na = (C.c_int * L)()
+        tr = (C.c_int * (L * max(A, 1)))()
+        lib.CountAlleles(geno, na, tr, rec)
+        out["A"] = A
+        out["int"]["MISSING_AFTER"] = g("MISSING").value
+        np.savez(os.path.join(workdir, "ref_data.npz"),
+                 geno=np.ctypeslib.as_array(geno).reshape(N, LINES, L).copy(),
+                 numalleles=np.ctypeslib.as_array(na).copy(),
+                 translation=np.ctypeslib.as_array(tr).reshape(L, max(A, 1)).copy(),
+                 labels=np.array([x.Label.decode() for x in inds]),
+                 pop=np.array([x.Population for x in inds]),
+                 popflag=np.array([x.PopFlag for x in inds]),
+                 location=np.array([x.Location for x in inds]),
+                 phenotype=np.array([x.Phenotype for x in inds]),
+                 names=np.array([bytes(names[l * 15:(l + 1) * 15]).split(b"\0")[0].decode()
+                                 for l in range(L)]))
+        if spec.get("sums"):
+            z = np.load(os.path.join(workdir, spec["sums"]))
+            K = g("MAXPOPS").value
+            d = lambda a: np.ascontiguousarray(a, np.float64).ctypes.data_as(C.c_void_p)
+            keep = {k: np.ascontiguousarray(z[k], np.float64) for k in
+                    ("QSum", "PSum", "SumEps", "FstSum", "sumAlpha", "sumlambda")}
+            ad = np.ascontiguousarray(z["AncestDist"], np.int32) if "AncestDist" in z.files else None
+            zeros = {k: np.zeros(n) for k, n in (("sumR", N + 1), ("varR", N + 1), ("R", N),
+                                                  ("lambda", K), ("sil", N), ("iln", N))}
+            P = lambda a: a.ctypes.data_as(C.c_void_p)
+            lib.OutPutResults.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_void_p]
+            lib.OutPutResults(geno, int(spec["rep"]), 1, inds, P(keep["PSum"]), P(keep["QSum"]),
+                              P(keep["FstSum"]), P(ad) if ad is not None else None, None,
+                              float(z["sumlikes"]), float(z["sumsqlikes"]), P(keep["sumAlpha"]),
+                              P(zeros["sumR"]), P(zeros["varR"]), na, tr, 1, names,
+                              P(zeros["R"]), P(keep["SumEps"]), P(zeros["lambda"]),
+                              P(keep["sumlambda"]), None, 0, P(zeros["sil"]), P(zeros["iln"]),
+                              len(argv), cargv)
+    with open(os.path.join(workdir, "ref_out.json"), "w") as f:
+        json.dump(out, f)
+
+
+if __name__ == "__main__":
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)   # the reference prints progress on stdout
+    main(sys.argv[1], sys.argv[2])

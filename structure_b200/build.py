@@ -59,7 +59,37 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_frontend(force, verbose)
     return LIB
+
+
+FRONT = os.path.join(HERE, "frontend")
+FRONT_LIB = os.path.join(HERE, "libstfront.so")
+CLI = os.path.join(HERE, "stgpu_structure")
+CXX = os.environ.get("CXX", "g++")
+
+
+def build_frontend(force=False, verbose=False):
+    """libstfront.so (parameters, data file, result files) and the
+    stgpu_structure command line linked against libstgpu.so."""
+    inc = "-I" + os.path.join(ROOT, "include")
+    front = os.path.join(FRONT, "front.cpp")
+    main = os.path.join(FRONT, "main.cpp")
+    hdr = os.path.join(ROOT, "include", "stfront.h")
+    cxx = [CXX, "-O2", "-std=c++17", "-Wall", inc]
+    steps = []
+    if force or _stale(FRONT_LIB, [front, hdr]):
+        steps.append(cxx + ["-fPIC", "-shared", "-fvisibility=hidden", front, "-o", FRONT_LIB])
+    if force or _stale(CLI, [front, main, hdr, LIB, os.path.join(ROOT, "include", "stgpu.h")]):
+        steps.append(cxx + [main, front, "-L" + HERE, "-lstgpu", "-Wl,-rpath,$ORIGIN",
+                            "-Wl,-rpath,/usr/local/cuda/lib64", "-o", CLI])
+    for cmd in steps:
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, cmd)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,185 @@
+// main.cpp -- stgpu_structure: the `structure` command line on the GPU sweep
+// engine.  Reads mainparams / extraparams and the data file like the
+// reference program (src/structure.c:155-700, with the same -m -e -i -o -K
+// -L -N -D flags), runs BURNIN + NUMREPS sweeps of one chain on the GPU
+// through libstgpu (include/stgpu.h), prints progress every UPDATEFREQ
+// sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
+//
+// Options the GPU path does not implement (LINKAGE, NOADMIX, USEPOPINFO,
+// LOCPRIOR, INFERLAMBDA, RECESSIVEALLELES, PLOIDY other than 2) stop the
+// program with a message instead of running a different model.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include "stfront.h"
+#include "stgpu.h"
+
+namespace {
+
+int pi(stf_run* r, const char* k) {
+  int v = 0;
+  stf_param_int(r, k, &v);
+  return v;
+}
+
+double pd(stf_run* r, const char* k) {
+  double v = 0.0;
+  stf_param_double(r, k, &v);
+  return v;
+}
+
+int die(const char* what, const char* msg) {
+  fprintf(stderr, "%s: %s\n\nExiting the program due to error(s) listed above.\n\n", what, msg);
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  stf_run* r = nullptr;
+  if (stf_open(argc, argv, &r) != STF_OK) return die("parameters", stf_last_error(r));
+  const char* unsupported[] = {"LINKAGE", "NOADMIX", "USEPOPINFO", "LOCPRIOR", "INFERLAMBDA",
+                               "RECESSIVEALLELES"};
+  for (const char* k : unsupported)
+    if (pi(r, k)) {
+      fprintf(stderr, "%s=1 is not available on the GPU path.\n", k);
+      return 1;
+    }
+  if (pi(r, "MAXPOPS") < 1 || pi(r, "MAXPOPS") > 32)
+    return die("parameters", "MAXPOPS must be in 1..32");
+  char datafile[256];
+  stf_param_str(r, "DATAFILE", datafile, sizeof datafile);
+  printf("Reading file \"%s\".\n", datafile);
+  if (stf_read_data(r) != STF_OK) return die("data", stf_last_error(r));
+  int dims[4];
+  stf_dims(r, dims);
+  const int N = dims[0], L = dims[1], A = dims[3], K = pi(r, "MAXPOPS");
+  std::vector<int32_t> geno((size_t)N * 2 * L), na(L), tr((size_t)L * (A > 0 ? A : 1));
+  stf_geno(r, geno.data(), na.data(), tr.data());
+  for (int32_t& g : geno)
+    if (g < 0) g = -9;   // the engine's missing code
+  std::vector<int32_t> popflag(N);
+  stf_individuals(r, nullptr, popflag.data(), nullptr, nullptr, nullptr);
+  int amin = 1 << 30, amax = 0;
+  double asum = 0.0;
+  for (int v : na) {
+    amin = v < amin ? v : amin;
+    amax = v > amax ? v : amax;
+    asum += v;
+  }
+  printf("Number of alleles per locus: min=%2d; ave=%2.1f; max=%2d\n", amin, asum / L, amax);
+
+  // seed: RANDOMIZE=1 (or the example seed 2245) takes one from the clock,
+  // and every seed used is appended to seed.txt (src/ran.c:114-126)
+  int seed = pi(r, "SEED");
+  if (pi(r, "RANDOMIZE") || seed == 2245) seed = (int)time(nullptr);
+  stf_set_param_int(r, "SEED", seed);
+  if (FILE* sf = fopen("seed.txt", "a")) {
+    fprintf(sf, "%i\n", seed);
+    fclose(sf);
+  }
+
+  st_ctx* ctx = nullptr;
+  st_data* data = nullptr;
+  st_chain* c = nullptr;
+  int rc = st_ctx_create(0, 0, &ctx);
+  if (rc != ST_OK) return die("GPU", "no CUDA device (st_ctx_create failed)");
+  st_data_desc d{};
+  d.num_inds = N;
+  d.num_loci = L;
+  d.lines = 2;
+  d.layout = ST_LAYOUT_AUTO;
+  d.geno = geno.data();
+  d.num_alleles = na.data();
+  d.popflags = popflag.data();
+  rc = st_data_upload(ctx, &d, &data);
+  if (rc != ST_OK) return die("GPU", st_last_error(ctx));
+  st_model m;
+  st_model_defaults(&m);
+  m.maxpops = K;
+  m.burnin = pi(r, "BURNIN");
+  m.numreps = pi(r, "NUMREPS");
+  m.freqscorr = pi(r, "FREQSCORR");
+  m.onefst = pi(r, "ONEFST");
+  m.inferalpha = pi(r, "INFERALPHA");
+  m.popalphas = pi(r, "POPALPHAS");
+  m.popspecificlambda = pi(r, "POPSPECIFICLAMBDA");
+  m.unifprioralpha = pi(r, "UNIFPRIORALPHA");
+  m.computeprob = pi(r, "COMPUTEPROB");
+  m.pfrompopflagonly = pi(r, "PFROMPOPFLAGONLY");
+  m.ancestdist = pi(r, "ANCESTDIST");
+  m.numboxes = pi(r, "NUMBOXES");
+  m.metrofreq = pi(r, "METROFREQ");
+  m.alpha = pd(r, "ALPHA");
+  m.alphamax = pd(r, "ALPHAMAX");
+  m.alphapropsd = pd(r, "ALPHAPROPSD");
+  m.alphapriora = pd(r, "ALPHAPRIORA");
+  m.alphapriorb = pd(r, "ALPHAPRIORB");
+  m.lambda = pd(r, "LAMBDA");
+  m.fpriormean = pd(r, "FPRIORMEAN");
+  m.fpriorsd = pd(r, "FPRIORSD");
+  rc = st_chain_create(ctx, data, &m, (uint64_t)seed, &c);
+  if (rc != ST_OK) return die("GPU", st_last_error(ctx));
+
+  printf("\n\n--------------------------------------\n\n");
+  printf("Finished initialization; starting MCMC \n");
+  printf("%d iterations + %d burnin\n\n", m.numreps, m.burnin);
+  const int total = m.burnin + m.numreps, every = pi(r, "UPDATEFREQ") > 0 ? pi(r, "UPDATEFREQ") : 100;
+  std::vector<double> alpha(K), F(K), stats(256);
+  printf(" Rep#:   Alpha   %s Ln Like    Est Ln P(D)\n", m.freqscorr ? " F(mean)" : "");
+  for (int done = 0; done < total;) {
+    const int n = total - done < every ? total - done : every;
+    rc = st_sweep(c, n);
+    if (rc == ST_OK) rc = st_sync(c);
+    if (rc != ST_OK) return die("GPU", st_last_error(ctx));
+    done += n;
+    st_get_state(c, ST_F_ALPHA, alpha.data(), alpha.size() * 8);
+    st_get_state(c, ST_F_F, F.data(), F.size() * 8);
+    st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
+    double fm = 0.0;
+    for (double v : F) fm += v / K;
+    printf("%5d:    %1.3f  ", done, alpha[0]);
+    if (m.freqscorr) printf("  %1.3f  ", fm);
+    if (done > m.burnin && m.computeprob) {
+      const double reps = done - m.burnin, mean = stats[1] / reps;
+      const double var = reps > 1 ? (stats[2] - stats[1] * stats[1] / reps) / (reps - 1) : 0.0;
+      printf("%9.0f  %9.0f", stats[0], mean - var / 2.0);
+    } else if (done == m.burnin) {
+      printf("\nBURNIN completed");
+    }
+    printf("\n");
+  }
+  const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A;
+  std::vector<double> QSum(NK), PSum(LKA), SumEps((size_t)L * A), FstSum(K), sumAlpha(K),
+      sumlambda(K);
+  std::vector<int32_t> AD;
+  st_get_state(c, ST_F_QSUM, QSum.data(), NK * 8);
+  st_get_state(c, ST_F_PSUM, PSum.data(), LKA * 8);
+  st_get_state(c, ST_F_SUMEPS, SumEps.data(), SumEps.size() * 8);
+  st_get_state(c, ST_F_FSTSUM, FstSum.data(), K * 8);
+  st_get_state(c, ST_F_SUMALPHA, sumAlpha.data(), K * 8);
+  st_get_state(c, ST_F_SUMLAMBDA, sumlambda.data(), K * 8);
+  st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
+  if (m.ancestdist) {
+    AD.resize(NK * (size_t)m.numboxes);
+    st_get_state(c, ST_F_ANCESTDIST, AD.data(), AD.size() * 4);
+  }
+  printf("\nMCMC completed\n");
+  rc = stf_write_results(r, total, QSum.data(), PSum.data(), SumEps.data(), FstSum.data(),
+                         sumAlpha.data(), sumlambda.data(), AD.empty() ? nullptr : AD.data(),
+                         stats[1], stats[2]);
+  if (rc != STF_OK) return die("output", stf_last_error(r));
+  char outfile[256];
+  stf_param_str(r, "OUTFILE", outfile, sizeof outfile);
+  printf("Final results printed to file %s_f\n\n", outfile);
+  printf("Structure seed: %d\n", seed);
+  st_chain_destroy(c);
+  st_data_destroy(data);
+  st_ctx_destroy(ctx);
+  stf_close(r);
+  return 0;
+}

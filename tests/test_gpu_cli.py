@@ -1,0 +1,60 @@
+"""stgpu_structure end to end: mainparams / extraparams and a data file in, a
+run of the GPU chain, OUTFILE_f out, for multi-allelic data (one byte per
+allele copy) and for biallelic data (2 bits per genotype).  The file format
+itself is checked byte for byte against the reference's writer in
+tests/test_frontend.py; here the run's numbers are checked for sense."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from test_frontend import _scenario
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "structure_b200", "stgpu_structure")
+
+
+def _snp_data(d, p):
+    s = __import__("structure_b200.synth", fromlist=["synth"])
+    g = s.snp_fmodel(p["N"], p["L"], 3, np.array([0.1, 0.2, 0.3]), 0.4, 0.02, 5)["geno"]
+    rows = []
+    for i in range(p["N"]):
+        for line in range(2):
+            rows.append(" ".join([f"s{i}", str(1 + i % 3)] + [str(v) for v in g[i, line]]))
+    with open(os.path.join(d, p["infile"]), "w") as f:
+        f.write("\n".join(rows) + "\n")
+
+
+@pytest.mark.parametrize("kind", ["microsat", "snp"])
+def test_cli_run_writes_results(tmp_path, kind):
+    d = str(tmp_path)
+    if kind == "microsat":
+        p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200)
+    else:
+        p = _scenario(d, N=80, L=300, burnin=200, numreps=600, updatefreq=200, markernames=0)
+        _snp_data(d, p)
+    r = subprocess.run([CLI, "-D", "99"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Final results printed to file results_f" in r.stdout
+    text = open(os.path.join(d, "results_f")).read()
+    for section in ("Run parameters:", "Proportion of membership", "Net nucleotide distance",
+                    "Estimated Ln Prob of Data", "Inferred ancestry of individuals:",
+                    "Estimated Allele Frequencies in each cluster",
+                    "Values of parameters used in structure:"):
+        assert section in text, section
+    lnp = float(re.search(r"Estimated Ln Prob of Data   = (\S+)", text).group(1))
+    mean = float(re.search(r"Mean value of ln likelihood = (\S+)", text).group(1))
+    assert np.isfinite(lnp) and lnp <= mean < 0
+    assert "   600 Reps" in text
+    rows = re.findall(r"^\s*\d+\s+\S+\s+\(\s*\d+\)\s+\d+ :\s+((?:[0-9.]+ ){3})", text, re.M)
+    assert len(rows) == p["N"]
+    q = np.array([[float(x) for x in row.split()] for row in rows])
+    np.testing.assert_allclose(q.sum(1), 1.0, atol=0.003)
+    fst = [float(x) for x in re.findall(r"Mean value of Fst_\d+\s+= (\S+)", text)]
+    assert len(fst) == 3 and all(0 < f < 1 for f in fst)
+    assert "SEED=99" in text
+    assert open(os.path.join(d, "seed.txt")).read().strip() == "99"
