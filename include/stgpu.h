@@ -282,6 +282,15 @@ int st_get_state(st_chain *c, int field, void *host, size_t bytes);
 int st_set_state(st_chain *c, int field, const void *host, size_t bytes);
 size_t st_field_bytes(st_chain *c, int field);
 
+/* Checkpoint / resume; no counterpart in the reference.
+ * st_chain_save writes every array of the chain, its sweep counter and its
+ * random-stream key to a file; st_chain_load restores them into a chain
+ * created on the same data with the same K, layout and options (seed
+ * irrelevant).  Draws are keyed by (seed, sweep, update, element), so the
+ * loaded chain continues exactly as the saved one would have.             */
+int st_chain_save(st_chain *c, const char *path);
+int st_chain_load(st_chain *c, const char *path);
+
 /* Per-chain timing of the last st_sweep / st_batch_sweep call (ms). */
 int st_get_timing(st_chain *c, double *ms_total);
 

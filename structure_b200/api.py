@@ -88,6 +88,8 @@ def lib():
         "st_update_eps": ([vp], C.c_int), "st_update_fst": ([vp], C.c_int),
         "st_collect": ([vp], C.c_int),
         "st_update_q_mala": ([vp], C.c_int),
+        "st_chain_save": ([vp, C.c_char_p], C.c_int),
+        "st_chain_load": ([vp, C.c_char_p], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
         "st_sweep": ([vp, C.c_int], C.c_int), "st_run": ([vp], C.c_int),
         "st_sync": ([vp], C.c_int),
@@ -269,6 +271,14 @@ class Chain:
     def UpdateFst(self): self.ctx.check(lib().st_update_fst(self.h))
     def DataCollection(self): self.ctx.check(lib().st_collect(self.h))
     def UpdateQMala(self): self.ctx.check(lib().st_update_q_mala(self.h))
+
+    def save(self, path):
+        """Checkpoint the whole chain state to `path` (st_chain_save)."""
+        self.ctx.check(lib().st_chain_save(self.h, os.fsencode(path)))
+
+    def load(self, path):
+        """Resume from a checkpoint of a chain of the same shape (st_chain_load)."""
+        self.ctx.check(lib().st_chain_load(self.h, os.fsencode(path)))
 
     def UpdateZInjected(self, uniforms, precision=64):
         u = np.ascontiguousarray(uniforms, np.float64)

@@ -1414,3 +1414,115 @@ extern "C" int st_loglik_grad(st_grad* g, const void* q_logits, const void* p_lo
   ctx->launches += 4 + (loglik ? 1 : 0);   // softmax, 2 passes, 2 finishes (+ total)
   return cuda_check(ctx, launch_loglik_grad(a, g->fp64), "loglik_grad");
 }
+
+// ===========================================================================
+// checkpoint / resume
+// ===========================================================================
+// File: "STGPUCK1", then int32 {version, N, L, K, A, layout, ngroups, host_rep,
+// store_z, ancestdist, numboxes, mala}, uint32 key, the st_model as created,
+// then every device array of the chain in the order of ckpt_fields() as
+// (uint64 byte count, bytes).  Philox draws are keyed by (seed, sweep, update,
+// element), so a chain loaded at sweep s continues exactly as the saved one.
+namespace {
+
+constexpr char kCkptMagic[8] = {'S', 'T', 'G', 'P', 'U', 'C', 'K', '1'};
+constexpr int32_t kCkptVersion = 1;
+
+struct CkField { void* p; size_t bytes; };
+
+std::vector<CkField> ckpt_fields(st_chain* c) {
+  ChainDev& h = c->h;
+  const size_t NK = (size_t)h.N * h.K, LKA = (size_t)h.L * h.K * h.A, LA = (size_t)h.L * h.A;
+  std::vector<CkField> f = {
+      {h.Q, NK * 4}, {h.logQ, NK * 4}, {h.TestQ, NK * 4}, {h.logTestQ, NK * 4},
+      {h.P, LKA * 4}, {h.logP, LKA * 4}, {h.eps, LA * 8}, {h.F, (size_t)h.K * 8},
+      {h.alpha, (size_t)h.K * 8}, {h.lambda, (size_t)h.K * 8}, {h.npart, LKA * 4},
+      {h.mpart, NK * 4}, {h.ldpart, (size_t)h.ngroups * h.N * 8}, {h.QSum, NK * 8},
+      {h.PSum, LKA * 8}, {h.SumEps, LA * 8}, {h.FstSum, (size_t)h.K * 8},
+      {h.sumAlpha, (size_t)h.K * 8}, {h.sumlambda, (size_t)h.K * 8},
+      {h.stats, (size_t)kStSize * 8}, {h.err, 4}};
+  if (h.Z) f.push_back({h.Z, (size_t)h.N * 2 * h.L});
+  if (h.AncestDist) f.push_back({h.AncestDist, NK * (size_t)h.numboxes * 4});
+  if (h.mala) f.push_back({h.mEps, (size_t)h.N * 4});
+  return f;
+}
+
+void ckpt_header(st_chain* c, int32_t hdr[12]) {
+  const ChainDev& h = c->h;
+  const int32_t v[12] = {kCkptVersion, h.N, h.L, h.K, h.A, h.layout, h.ngroups, c->host_rep,
+                         h.Z != nullptr, h.AncestDist != nullptr, h.numboxes, h.mala};
+  memcpy(hdr, v, sizeof v);
+}
+
+}  // namespace
+
+extern "C" int st_chain_save(st_chain* c, const char* path) {
+  if (!c || !path) return ST_ERR_ARG;
+  st_ctx* ctx = c->ctx;
+  cudaSetDevice(ctx->device);
+  ST_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  FILE* f = fopen(path, "wb");
+  if (!f) return seterr(ctx, ST_ERR_ARG, "cannot open %s for writing", path);
+  int32_t hdr[12];
+  ckpt_header(c, hdr);
+  bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, 4, 12, f) == 12 &&
+            fwrite(&c->h.key, 4, 1, f) == 1 && fwrite(&c->model, sizeof(st_model), 1, f) == 1;
+  std::vector<char> buf;
+  for (const CkField& fl : ckpt_fields(c)) {
+    if (!ok) break;
+    buf.resize(fl.bytes);
+    if (cudaMemcpy(buf.data(), fl.p, fl.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      fclose(f);
+      return seterr(ctx, ST_ERR_CUDA, "checkpoint read-back failed");
+    }
+    const uint64_t n = fl.bytes;
+    ok = fwrite(&n, 8, 1, f) == 1 && fwrite(buf.data(), 1, fl.bytes, f) == fl.bytes;
+  }
+  if (fclose(f) != 0) ok = false;
+  return ok ? ST_OK : seterr(ctx, ST_ERR_ARG, "writing %s failed", path);
+}
+
+extern "C" int st_chain_load(st_chain* c, const char* path) {
+  if (!c || !path) return ST_ERR_ARG;
+  st_ctx* ctx = c->ctx;
+  cudaSetDevice(ctx->device);
+  FILE* f = fopen(path, "rb");
+  if (!f) return seterr(ctx, ST_ERR_ARG, "cannot open %s", path);
+  char magic[8];
+  int32_t hdr[12], mine[12];
+  uint32_t key = 0;
+  st_model model;
+  bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, kCkptMagic, 8) == 0 &&
+            fread(hdr, 4, 12, f) == 12 && fread(&key, 4, 1, f) == 1 &&
+            fread(&model, sizeof(st_model), 1, f) == 1;
+  ckpt_header(c, mine);
+  // the chain must have been created on the same data with the same shape;
+  // the sweep counter (slot 7) is what the file restores
+  for (int j = 0; ok && j < 12; j++)
+    if (j != 7 && hdr[j] != mine[j]) ok = false;
+  if (!ok) {
+    fclose(f);
+    return seterr(ctx, ST_ERR_STATE, "%s is not a checkpoint of a chain of this shape", path);
+  }
+  std::vector<char> buf;
+  ST_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (const CkField& fl : ckpt_fields(c)) {
+    uint64_t n = 0;
+    if (fread(&n, 8, 1, f) != 1 || n != fl.bytes) { ok = false; break; }
+    buf.resize(fl.bytes);
+    if (fread(buf.data(), 1, fl.bytes, f) != fl.bytes) { ok = false; break; }
+    if (cudaMemcpy(fl.p, buf.data(), fl.bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+      fclose(f);
+      return seterr(ctx, ST_ERR_CUDA, "checkpoint upload failed");
+    }
+  }
+  fclose(f);
+  if (!ok) return seterr(ctx, ST_ERR_STATE, "%s is truncated or of another chain", path);
+  c->h.key = key;
+  c->h.cnt_chunks = 1;
+  c->h.cnt_groups = 1;
+  int rc = upload_chain(c);
+  if (!rc) rc = set_rep(c, hdr[7]);
+  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "checkpoint load");
+  return rc;
+}
