@@ -123,7 +123,7 @@ typedef struct st_model {
     int32_t onefst;            /* ONEFST */
     int32_t inferalpha;        /* INFERALPHA */
     int32_t popalphas;         /* POPALPHAS */
-    int32_t inferlambda;       /* INFERLAMBDA: must be 0 */
+    int32_t inferlambda;       /* INFERLAMBDA */
     int32_t popspecificlambda; /* POPSPECIFICLAMBDA */
     int32_t unifprioralpha;    /* UNIFPRIORALPHA */
     int32_t computeprob;       /* COMPUTEPROB */
@@ -173,6 +173,8 @@ int st_update_alpha(st_chain *c);  /* UpdateAlphaCL  src/Updates/UpdateAlpha.c:3
 int st_update_eps(st_chain *c);    /* UpdateEpsilonCL src/Updates/UpdateEpsilon.c:270-292 */
 int st_update_fst(st_chain *c);    /* UpdateFstCL    src/Updates/UpdateFst.c:100-140 */
 int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183         */
+int st_update_lambda(st_chain *c); /* UpdateLambda / UpdatePopLambda (CPU only in the
+                                      reference) src/Updates/UpdateLambda.c:8-102   */
 /* One Metropolis-adjusted Langevin move on every Q_i with Z summed out and P
  * fixed (chains created with st_model.mala; st_sweep runs it after the Q
  * update).  No reference counterpart.                                        */

@@ -24,7 +24,7 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _ci, _cd, _cu32, _cu64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
 
-S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA = range(1, 11)
+S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA, S_LAMBDA = range(1, 12)
 
 
 def rnd_words(w):
@@ -92,6 +92,8 @@ class Oracle:
         lib.orc_loglik_grad.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f64p, _f64p, _f64p, _f64p,
                                         _f64p]
         lib.orc_loglik_grad.restype = _cd
+        lib.orc_update_lambda.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f64p, _ci, _ci, _f64p,
+                                          _cu64, _cu32, _f64p]
         lib.orc_mala_step.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f32p, _f32p, _f64p, _ci, _f32p,
                                       _cu64, _cu32, _ci, _cd, _f64p, _u8p]
 
@@ -251,6 +253,16 @@ class Oracle:
     def est_logprob(self, s, ss, reps):
         return self.lib.orc_est_logprob(s, ss, reps)
 
+    def update_lambda(self, numalleles, logP, eps, freqscorr, popspecific, lam, key, rep):
+        L, K, A = logP.shape
+        out = np.ascontiguousarray(lam, np.float64).copy()
+        lpd = np.full(K, np.nan)
+        self.lib.orc_update_lambda(L, K, A, np.ascontiguousarray(numalleles, np.int32),
+                                   np.ascontiguousarray(logP, np.float32),
+                                   np.ascontiguousarray(eps, np.float64), int(freqscorr),
+                                   int(popspecific), out, key, rep, lpd)
+        return out, lpd
+
     def mala_step(self, geno, Q, logQ, P, alpha, popalphas, eps, key, rep, burnin, target):
         """One Langevin move on every Q_i; returns (Q, logQ, eps, logr, acc)."""
         N, _, L = geno.shape
@@ -283,7 +295,8 @@ class RefModel(C.Structure):
                                    "burnin", "numreps", "computeprob", "pfrompopflagonly",
                                    "ancestdist", "numboxes")] + \
               [(n, _cd) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
-                                  "alphapriorb", "lambda_", "fpriormean", "fpriorsd")]
+                                  "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
+              [("inferlambda", _ci), ("popspecificlambda", _ci)]
 
 
 class RefView(C.Structure):
@@ -291,7 +304,8 @@ class RefView(C.Structure):
               [(n, C.POINTER(_cd)) for n in ("Q", "P", "Eps", "SumEps", "Fst", "FstSum", "Alpha",
                                             "sumAlpha", "PSum", "QSum", "like", "sumlikes",
                                             "sumsqlikes")] + \
-              [("maxalleles", _ci), ("rep", _ci)]
+              [("maxalleles", _ci), ("rep", _ci)] + \
+              [(n, C.POINTER(_cd)) for n in ("lambda_", "sumlambda")]
 
 
 def ref_model(**kw):
@@ -299,7 +313,7 @@ def ref_model(**kw):
              unifprioralpha=1, metrofreq=10, burnin=0, numreps=1, computeprob=1,
              pfrompopflagonly=0, ancestdist=0, numboxes=1000, alpha=1.0, alphamax=10.0,
              alphapropsd=0.025, alphapriora=0.05, alphapriorb=0.001, lambda_=1.0,
-             fpriormean=0.01, fpriorsd=0.05)
+             fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0)
     d.update(kw)
     return RefModel(**d)
 
@@ -349,6 +363,8 @@ class RefLib:
         lib.FPriorDiff.argtypes = [_cd, _cd]
         lib.FPriorDiff.restype = _cd
         lib.UpdateAlpha.argtypes = [_f64p, _f64p, C.c_void_p, _ci]
+        lib.UpdateLambda.argtypes = [_f64p, _f64p, _f64p, _i32p]
+        lib.UpdatePopLambda.argtypes = [_f64p, _f64p, _i32p]
         lib.UpdateP.argtypes = [_f64p, _f64p, _f64p, _i32p, _i32p, _i32p, _f64p, C.c_void_p, _f64p]
         lib.stref_guard_hits.restype = C.c_long
         lib.UpdateEpsilon.argtypes = [_f64p, _f64p, _f64p, _i32p, _cd]
@@ -412,4 +428,5 @@ class RefLib:
             Fst=arr(v.Fst, K), Alpha=arr(v.Alpha, K), QSum=arr(v.QSum, N * K).reshape(N, K),
             PSum=arr(v.PSum, L * K * A).reshape(L, K, A), SumEps=arr(v.SumEps, L * A).reshape(L, A),
             FstSum=arr(v.FstSum, K), sumAlpha=arr(v.sumAlpha, K),
-            like=v.like[0], sumlikes=v.sumlikes[0], sumsqlikes=v.sumsqlikes[0])
+            like=v.like[0], sumlikes=v.sumlikes[0], sumsqlikes=v.sumsqlikes[0],
+            lambda_=arr(v.lambda_, K), sumlambda=arr(v.sumlambda, K))

@@ -32,6 +32,7 @@
 #include "Updates/UpdateAlpha.h"
 #include "Updates/UpdateEpsilon.h"
 #include "Updates/UpdateFst.h"
+#include "Updates/UpdateLambda.h"
 
 /* ---- OpenCL host helpers (Kernels.c) as no-ops ------------------------- */
 int InitCLDict(CLDict *d) { (void)d; return EXIT_SUCCESS; }
@@ -136,6 +137,7 @@ typedef struct stref_model {
     int ancestdist, numboxes;
     double alpha, alphamax, alphapropsd, alphapriora, alphapriorb;
     double lambda, fpriormean, fpriorsd;
+    int inferlambda, popspecificlambda;
 } stref_model;
 
 void stref_set_globals(const stref_model *m)
@@ -151,7 +153,8 @@ void stref_set_globals(const stref_model *m)
     COMPUTEPROB = m->computeprob; PFROMPOPFLAGONLY = m->pfrompopflagonly;
     ANCESTDIST = m->ancestdist; NUMBOXES = m->numboxes > 0 ? m->numboxes : 1000;
     USEPOPINFO = 0; NOADMIX = 0; LOCPRIOR = 0; LINKAGE = 0; RECESSIVEALLELES = 0;
-    INFERLAMBDA = 0; POPSPECIFICLAMBDA = 0; STARTATPOPINFO = 0; POPDATA = 0;
+    INFERLAMBDA = m->inferlambda; POPSPECIFICLAMBDA = m->popspecificlambda;
+    STARTATPOPINFO = 0; POPDATA = 0;
     INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = 0;
     NOALPHA = 0; PHASED = 0; PHASEINFO = 0; MARKOVPHASE = 0; NOQS = 0;
     LOCDATA = 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0; GENSBACK = 2;
@@ -261,6 +264,10 @@ int stref_chain_sweeps(stref_chain *c, int nsweeps)
         fill_uniform(c->randomArr, (size_t)N * L * 2);
         UpdateZ(c->Z, c->Q, c->P, c->Geno, c->randomArr);
         if (INFERALPHA) UpdateAlpha(c->Q, c->Alpha, c->Individual, rep);
+        if (INFERLAMBDA) {       /* structure.c:586-593 */
+            if (POPSPECIFICLAMBDA) UpdatePopLambda(c->P, c->lambda, c->NumAlleles);
+            else UpdateLambda(c->P, c->Eps, c->lambda, c->NumAlleles);
+        }
         if (FREQSCORR) {
             UpdateEpsilon(c->P, c->Eps, c->Fst, c->NumAlleles, c->lambda[0]);
             UpdateFst(c->Eps, c->Fst, c->P, c->NumAlleles);
@@ -281,6 +288,7 @@ typedef struct stref_view {
     double *Q, *P, *Eps, *SumEps, *Fst, *FstSum, *Alpha, *sumAlpha;
     double *PSum, *QSum, *like, *sumlikes, *sumsqlikes;
     int maxalleles, rep;
+    double *lambda, *sumlambda;
 } stref_view;
 
 void stref_chain_view(stref_chain *c, stref_view *v)
@@ -292,6 +300,7 @@ void stref_chain_view(stref_chain *c, stref_view *v)
     v->sumAlpha = c->sumAlpha; v->PSum = c->PSum; v->QSum = c->QSum;
     v->like = &c->like; v->sumlikes = &c->sumlikes; v->sumsqlikes = &c->sumsqlikes;
     v->maxalleles = c->m.maxalleles; v->rep = c->rep;
+    v->lambda = c->lambda; v->sumlambda = c->sumlambda;
 }
 
 void stref_chain_free(stref_chain *c)

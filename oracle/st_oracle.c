@@ -805,3 +805,48 @@ void orc_mala_step(int N, int L, int K, const int32_t *geno, float *Q, float *lo
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Updates/UpdateLambda.c:8-102 UpdatePopLambda / UpdateLambda: proposal      */
+/* N(lambda, 0.3) inside (0, 10), log ratio over loci with >1 allele.         */
+/* ------------------------------------------------------------------------ */
+void orc_update_lambda(int L, int K, int A, const int32_t *numalleles, const float *logP,
+                       const double *eps, int freqscorr, int popspecific, double *lambda,
+                       uint64_t key, uint32_t rep, double *lpd_out)
+{
+    const double maxl = 10.0, sd = 0.3;
+    int npop = popspecific ? K : 1;
+    for (int q = 0; q < npop; q++) {
+        double lam = lambda[q];
+        double nw = lam + sd * orc_normal((uint32_t)q, rep, ORC_S_LAMBDA, key);
+        if (lpd_out) lpd_out[q] = NAN;
+        if (!(nw > 0.0 && nw < maxl)) continue;
+        double reps = popspecific ? 1.0 : (freqscorr ? 1.0 : (double)K);
+        double sum = 0.0;
+        for (int l = 0; l < L; l++) {
+            int na = numalleles[l];
+            if (na <= 1) continue;
+            sum += reps * orc_lgamma(na * nw);
+            sum -= reps * orc_lgamma(na * lam);
+            sum += reps * na * orc_lgamma(lam);
+            sum -= reps * na * orc_lgamma(nw);
+            double slog = 0.0;
+            if (popspecific) {
+                for (int a = 0; a < na; a++) slog += (double)logP[((size_t)l * K + q) * A + a];
+            } else if (freqscorr) {
+                for (int a = 0; a < na; a++) slog += log(eps[(size_t)l * A + a]);
+            } else {
+                for (int k = 0; k < K; k++)
+                    for (int a = 0; a < na; a++) slog += (double)logP[((size_t)l * K + k) * A + a];
+            }
+            sum += (nw - lam) * slog;
+        }
+        if (lpd_out) lpd_out[q] = sum;
+        uint32_t w[4];
+        philox4((uint32_t)q, 1, rep, ORC_S_LAMBDA, key, w);
+        if (orc_rnd31_block(w) < exp(sum)) {
+            if (popspecific) lambda[q] = nw;
+            else for (int k = 0; k < K; k++) lambda[k] = nw;
+        }
+    }
+}

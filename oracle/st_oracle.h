@@ -28,7 +28,8 @@ extern "C" {
 /* Philox stream identifiers: counter word 3 = stream << 24. */
 enum {
     ORC_S_INITZ = 1, ORC_S_Z = 2, ORC_S_P = 3, ORC_S_QG = 4, ORC_S_QM = 5,
-    ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10
+    ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10,
+    ORC_S_LAMBDA = 11
 };
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
@@ -99,6 +100,14 @@ void orc_fst_diffs(int L, int K, int A, const int32_t *numalleles,
 void orc_update_fst(int K, int onefst, double fpriormean, double fpriorsd,
                     int Leff, const double *diff, const double *newf,
                     double *F, uint64_t key, uint32_t rep, double *lpd_out);
+
+/* --- lambda (Updates/UpdateLambda.c:8-102) ------------------------------- */
+/* logP [L][K][A] (log P as stored), eps [L][A]; popspecific: one value per
+ * population, else one shared value (from eps with freqscorr, else from P of
+ * every population).  lpd_out [npop] receives the log acceptance ratios. */
+void orc_update_lambda(int L, int K, int A, const int32_t *numalleles, const float *logP,
+                       const double *eps, int freqscorr, int popspecific, double *lambda,
+                       uint64_t key, uint32_t rep, double *lpd_out);
 
 /* --- likelihood and bookkeeping (CalcLike.c:75-133,387-426; output.c) ---- */
 double orc_calc_like(int N, int L, int K, int A, const int32_t *geno,

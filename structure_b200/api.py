@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libstgpu.so")
+# STGPU_LIB selects another build of the library (e.g. one installed elsewhere)
+LIB_PATH = os.environ.get("STGPU_LIB") or os.path.join(HERE, "libstgpu.so")
 
 ST_OK, ST_ERR_ARG, ST_ERR_CUDA, ST_ERR_NOMEM, ST_ERR_ADMISSION = 0, -1, -2, -3, -4
 ST_ERR_STATE, ST_ERR_DEVICE, ST_ERR_UNSUPPORTED, ST_ERR_NODEVICE = -5, -6, -7, -8
@@ -26,7 +27,7 @@ LAYOUT_AUTO, LAYOUT_U8, LAYOUT_B2G = 0, 1, 2
 ST_LIKE, ST_SUMLIKES, ST_SUMSQ, ST_NLIKE, ST_METROHITS = 0, 1, 2, 3, 4
 ST_ALPHA_T, ST_ALPHA_S = 6, 8
 ST_FST_DIFF, ST_FST_NEW, ST_ALPHA_LPD, ST_FST_LPD, ST_ALPHA_NEW = 40, 72, 104, 136, 168
-ST_MALA_ACC, ST_MALA_TRIES = 200, 201
+ST_MALA_ACC, ST_MALA_TRIES, ST_LAMBDA_LPD = 200, 201, 202
 
 
 class StError(RuntimeError):
@@ -63,6 +64,8 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
+        if os.environ.get("STGPU_LIB"):
+            raise OSError(f"STGPU_LIB={LIB_PATH} does not exist")
         from . import build
         build.build()
     L = C.CDLL(LIB_PATH)
@@ -88,6 +91,7 @@ def lib():
         "st_update_eps": ([vp], C.c_int), "st_update_fst": ([vp], C.c_int),
         "st_collect": ([vp], C.c_int),
         "st_update_q_mala": ([vp], C.c_int),
+        "st_update_lambda": ([vp], C.c_int),
         "st_chain_save": ([vp, C.c_char_p], C.c_int),
         "st_chain_load": ([vp, C.c_char_p], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
@@ -271,6 +275,7 @@ class Chain:
     def UpdateFst(self): self.ctx.check(lib().st_update_fst(self.h))
     def DataCollection(self): self.ctx.check(lib().st_collect(self.h))
     def UpdateQMala(self): self.ctx.check(lib().st_update_q_mala(self.h))
+    def UpdateLambda(self): self.ctx.check(lib().st_update_lambda(self.h))
 
     def save(self, path):
         """Checkpoint the whole chain state to `path` (st_chain_save)."""

@@ -9,7 +9,7 @@
 #include <vector>
 #include <algorithm>
 #include <cuda_runtime.h>
-#include "../../include/stgpu.h"
+#include "stgpu.h"
 #include "st_kernels.h"
 
 using namespace st;
@@ -274,7 +274,6 @@ int check_model(st_ctx* ctx, const st_model* m) {
   if (m->linkage) return seterr(ctx, ST_ERR_UNSUPPORTED, "LINKAGE=1 is not on the GPU path");
   if (m->usepopinfo) return seterr(ctx, ST_ERR_UNSUPPORTED, "USEPOPINFO=1 is not on the GPU path");
   if (m->locprior) return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR=1 is not on the GPU path");
-  if (m->inferlambda) return seterr(ctx, ST_ERR_UNSUPPORTED, "INFERLAMBDA=1 is not on the GPU path");
   if (m->recessivealleles)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "RECESSIVEALLELES=1 is not on the GPU path");
   if (m->freqscorr && (m->fpriormean <= 0 || m->fpriorsd <= 0))
@@ -589,6 +588,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   h.layout = data->layout; h.wpr = data->wpr; h.Leff = data->Leff;
   h.freqscorr = model->freqscorr; h.onefst = model->onefst; h.inferalpha = model->inferalpha;
   h.popalphas = model->popalphas; h.unifprioralpha = model->unifprioralpha;
+  h.inferlambda = model->inferlambda; h.popspecificlambda = model->popspecificlambda;
   h.computeprob = model->computeprob; h.pfrompopflagonly = model->pfrompopflagonly;
   h.ancestdist = model->ancestdist; h.numboxes = model->numboxes > 0 ? model->numboxes : 1;
   h.metrofreq = model->metrofreq; h.burnin = model->burnin;
@@ -861,6 +861,20 @@ extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int 
 // ===========================================================================
 // sweeps
 // ===========================================================================
+// UpdateLambda / UpdatePopLambda (src/Updates/UpdateLambda.c:8-102).
+static int lambda_step(st_chain* c) {
+  Bracket br(c->ctx, ST_K_OTHER);
+  LaunchSet ls = single(c, ctas_lambda(c->h, 256));
+  return cuda_check(c->ctx, launch_lambda(ls, 256), "lambda");
+}
+
+extern "C" int st_update_lambda(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.inferlambda) return seterr(c->ctx, ST_ERR_STATE, "UpdateLambda needs INFERLAMBDA=1");
+  cudaSetDevice(c->ctx->device);
+  return lambda_step(c);
+}
+
 // One Langevin move on every Q_i (Z summed out, P fixed): four kernels of the
 // gradient pass and two per-individual kernels.
 static int mala_step(st_chain* c) {
@@ -882,7 +896,10 @@ extern "C" int st_update_q_mala(st_chain* c) {
 static int sweep_once(st_chain* c) {
   const int zflags = (c->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
                      (c->model.store_z ? kZfStoreZ : 0);
-  int rc = locus(c, kLocP | kLocEps | kLocFst | kLocCollect);
+  // with INFERLAMBDA, lambda is updated between P and eps (src/structure.c:586-599)
+  int rc = c->h.inferlambda ? locus(c, kLocP) : locus(c, kLocP | kLocEps | kLocFst | kLocCollect);
+  if (!rc && c->h.inferlambda) rc = lambda_step(c);
+  if (!rc && c->h.inferlambda) rc = locus(c, kLocEps | kLocFst | kLocCollect);
   if (!rc) rc = update_q_impl(c, kIndAlpha | kIndCollect);
   if (!rc && c->h.mala && c->h.K > 1) rc = mala_step(c);
   if (!rc) rc = zpass(c, kZNormal, zflags);
@@ -1218,9 +1235,19 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
   LaunchSet li{b->d_table, b->d_pi, n, b->ti, s};
   const int zflags = (c0->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
                      (c0->model.store_z ? kZfStoreZ : 0);
+  bool lam = false;
+  for (st_chain* c : b->chains) lam = lam || c->h.inferlambda;
   {
     Bracket br(ctx, ST_K_LOCUS);
-    ST_CUDA(ctx, launch_locus(ll, b->G, kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
+    ST_CUDA(ctx, launch_locus(ll, b->G, lam ? kLocP : kLocP | kLocEps | kLocFst | kLocCollect,
+                              kBlockLoc));
+  }
+  if (lam) {
+    for (st_chain* c : b->chains)
+      if (c->h.inferlambda)
+        if (int rc = lambda_step(c)) return rc;
+    Bracket br(ctx, ST_K_LOCUS);
+    ST_CUDA(ctx, launch_locus(ll, b->G, kLocEps | kLocFst | kLocCollect, kBlockLoc));
   }
   if (metro) {
     {

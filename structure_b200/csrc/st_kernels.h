@@ -42,6 +42,7 @@ cudaError_t launch_zpass_u8(const LaunchSet& ls, int mode, int flags);
 cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block);
 cudaError_t launch_ind(const LaunchSet& ls, int G, int mode, int stages, int block);
 cudaError_t launch_collect(const LaunchSet& ls, int block);
+cudaError_t launch_lambda(const LaunchSet& ls, int block);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
 
 // CTA counts per chain for each launch kind (host-side mirror of the tiling).
@@ -50,6 +51,7 @@ int ctas_zpass_u8(const ChainDev& c, int block);
 int ctas_locus(const ChainDev& c, int block);
 int ctas_ind(const ChainDev& c, int block);
 int ctas_collect(const ChainDev& c, int block);
+int ctas_lambda(const ChainDev& c, int block);
 
 // Gradient of ln P(D|Q,P) (Z marginalised) w.r.t. softmax logits, biallelic
 // 2-bit data.  T = float or double in every T buffer.

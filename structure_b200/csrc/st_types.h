@@ -15,7 +15,7 @@ constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
 // Philox stream ids (counter word 3 = id << 24).
 enum Stream : uint32_t {
   kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
-  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10
+  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11
 };
 
 // Device error word bits.
@@ -45,11 +45,13 @@ enum : int {
   kStAlphaNew = kStFstLpd + kMaxPops,  // alpha proposals
   kStMalaAcc = kStAlphaNew + kMaxPops, // Langevin moves accepted
   kStMalaTries,                        // Langevin moves proposed
+  kStLambdaLpd = kStMalaAcc + 2,       // lambda log acceptance ratios (K)
   kStSize = 256
 };
 
 // Done-counter slots of the last-CTA protocol.
-enum : int { kCtrZ = 0, kCtrLocus = 1, kCtrInd = 2, kCtrMetro = 3, kCtrCount = 8 };
+enum : int { kCtrZ = 0, kCtrLocus = 1, kCtrInd = 2, kCtrMetro = 3, kCtrLambda = 4,
+             kCtrCount = 8 };
 
 struct ChainDev {
   // dimensions
@@ -57,7 +59,7 @@ struct ChainDev {
   int layout, wpr;          // genotype layout, B2G words per locus row
   int Leff;                 // loci with at least one observed allele
   // model (mainparams / extraparams)
-  int freqscorr, onefst, inferalpha, popalphas, unifprioralpha;
+  int freqscorr, onefst, inferalpha, popalphas, unifprioralpha, inferlambda, popspecificlambda;
   int computeprob, pfrompopflagonly, ancestdist, numboxes, metrofreq, burnin;
   double alphamax, alphapropsd, alphapriora, alphapriorb;
   double fpriormean, fpriorsd, invsqrtnuminds;

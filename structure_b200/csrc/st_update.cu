@@ -237,6 +237,95 @@ cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block) {
 }
 
 // ---------------------------------------------------------------------------
+// Lambda kernel: UpdateLambda / UpdatePopLambda (Updates/UpdateLambda.c:8-102).
+// Metropolis on lambda under a uniform prior on (0, LAMBDAMAX = 10), proposal
+// N(lambda, LAMBDAPROPSD = 0.3); one value (all populations share it), or one
+// per population with POPSPECIFICLAMBDA.  Log ratio, summed over loci with
+// more than one allele:
+//   reps * [lgamma(na new) - lgamma(na lambda) + na lgamma(lambda) - na lgamma(new)]
+//   + (new - lambda) * sum_reps sum_a log freq,
+// where the frequencies are P of population q (per population), or eps
+// (FREQSCORR, reps = 1) or P of every population (reps = K).  Thread = locus;
+// per-CTA sums go to redpart, the last CTA adds them in order and decides.
+// Draws: the normal at (q, 0), the rand()-style uniform at (q, 1) of stream
+// kSLambda.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr double kLambdaMax = 10.0;      // structure.h:19 LAMBDAMAX
+constexpr double kLambdaPropSd = 0.3;    // structure.h:20 LAMBDAPROPSD
+}  // namespace
+
+__global__ void __launch_bounds__(256)
+lambda_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains) {
+  __shared__ double sred[8];
+  __shared__ double snew[kMaxPops];
+  const int c = find_chain(prefix, nchains, blockIdx.x);
+  ChainDev& ch = chains[c];
+  const int tile = blockIdx.x - prefix[c];
+  const int L = ch.L, K = ch.K, A = ch.A;
+  const int rep = *ch.rep;
+  const uint32_t key = ch.key;
+  const int npop = ch.popspecificlambda ? K : 1;
+  const int nblocks = (L + blockDim.x - 1) / blockDim.x;
+  if (threadIdx.x < npop)
+    snew[threadIdx.x] = ch.lambda[threadIdx.x] +
+                        kLambdaPropSd * normal_draw((uint32_t)threadIdx.x, (uint32_t)rep, kSLambda, key);
+  __syncthreads();
+  const int l = tile * blockDim.x + threadIdx.x;
+  const int na = l < L ? ch.numalleles[l] : 0;
+  for (int q = 0; q < npop; q++) {
+    const double lam = ch.lambda[q], nw = snew[q];
+    double term = 0.0;
+    if (na > 1 && nw > 0.0 && nw < kLambdaMax) {
+      const double reps = ch.popspecificlambda ? 1.0 : (ch.freqscorr ? 1.0 : (double)K);
+      term = reps * (lanczos_lgamma(na * nw) - lanczos_lgamma(na * lam) +
+                     na * lanczos_lgamma(lam) - na * lanczos_lgamma(nw));
+      double slog = 0.0;
+      if (ch.popspecificlambda) {
+        for (int a = 0; a < na; a++) slog += (double)ch.logP[((size_t)l * K + q) * A + a];
+      } else if (ch.freqscorr) {
+        for (int a = 0; a < na; a++) slog += log(ch.eps[(size_t)l * A + a]);
+      } else {
+        for (int k = 0; k < K; k++)
+          for (int a = 0; a < na; a++) slog += (double)ch.logP[((size_t)l * K + k) * A + a];
+      }
+      term += (nw - lam) * slog;
+    }
+    for (int off = 16; off > 0; off >>= 1) term += __shfl_down_sync(0xffffffffu, term, off);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = term;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += sred[w];
+      ch.redpart[(size_t)tile * npop + q] = sum;
+    }
+    __syncthreads();
+  }
+  if (last_cta_arrive(&ch.ctr[kCtrLambda], (unsigned)nblocks) && threadIdx.x < npop) {
+    const int q = threadIdx.x;
+    double sum = 0.0;
+    for (int b = 0; b < nblocks; b++) sum += ch.redpart[(size_t)b * npop + q];
+    const double nw = snew[q];
+    ch.stats[kStLambdaLpd + q] = sum;
+    if (nw > 0.0 && nw < kLambdaMax &&
+        rnd31(philox_s((uint32_t)q, 1, (uint32_t)rep, kSLambda, key)) < exp(sum)) {
+      if (ch.popspecificlambda) {
+        ch.lambda[q] = nw;
+      } else {
+        for (int k = 0; k < K; k++) ch.lambda[k] = nw;
+      }
+    }
+  }
+}
+
+int ctas_lambda(const ChainDev& c, int block) { return (c.L + block - 1) / block; }
+
+cudaError_t launch_lambda(const LaunchSet& ls, int block) {
+  lambda_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Individual kernel
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)

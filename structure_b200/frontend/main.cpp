@@ -6,7 +6,7 @@
 // sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
 //
 // Options the GPU path does not implement (LINKAGE, NOADMIX, USEPOPINFO,
-// LOCPRIOR, INFERLAMBDA, RECESSIVEALLELES, PLOIDY other than 2) stop the
+// LOCPRIOR, RECESSIVEALLELES, PLOIDY other than 2) stop the
 // program with a message instead of running a different model.
 #include <cstdio>
 #include <cstdlib>
@@ -42,7 +42,7 @@ int die(const char* what, const char* msg) {
 int main(int argc, char** argv) {
   stf_run* r = nullptr;
   if (stf_open(argc, argv, &r) != STF_OK) return die("parameters", stf_last_error(r));
-  const char* unsupported[] = {"LINKAGE", "NOADMIX", "USEPOPINFO", "LOCPRIOR", "INFERLAMBDA",
+  const char* unsupported[] = {"LINKAGE", "NOADMIX", "USEPOPINFO", "LOCPRIOR",
                                "RECESSIVEALLELES"};
   for (const char* k : unsupported)
     if (pi(r, k)) {
@@ -107,6 +107,7 @@ int main(int argc, char** argv) {
   m.onefst = pi(r, "ONEFST");
   m.inferalpha = pi(r, "INFERALPHA");
   m.popalphas = pi(r, "POPALPHAS");
+  m.inferlambda = pi(r, "INFERLAMBDA");
   m.popspecificlambda = pi(r, "POPSPECIFICLAMBDA");
   m.unifprioralpha = pi(r, "UNIFPRIORALPHA");
   m.computeprob = pi(r, "COMPUTEPROB");

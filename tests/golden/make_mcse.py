@@ -16,6 +16,7 @@ Runs:
   c1  -- N=200, L=100 multi-allelic loci (2..10 alleles), K=3, 5% copies
          missing; admixture, alpha inferred, independent frequencies, lambda=1;
          1,000 burn-in + 10,000 sweeps; 8 chains.
+  c1l -- the same data and run with lambda inferred (INFERLAMBDA=1).
   c2s -- N=200, L=1,000 biallelic SNPs, K=3 F model (F = .10, .20, .30), 3%
          genotypes missing; alpha and F inferred; 2,000 burn-in + 4,000 sweeps;
          8 chains.
@@ -43,6 +44,10 @@ def runs():
         "c1": dict(geno=c1["geno"], raw=c1["geno_raw"], numalleles=c1["numalleles"], Q=c1["Q"],
                    K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
                                    alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0)),
+        "c1l": dict(geno=c1["geno"], raw=c1["geno_raw"], numalleles=c1["numalleles"], Q=c1["Q"],
+                    K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
+                                    alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
+                                    inferlambda=1)),
         "c2s": dict(geno=c2["geno"], raw=c2["geno"], numalleles=c2["numalleles"], Q=c2["Q"],
                     K=3, model=dict(burnin=2000, numreps=4000, freqscorr=1, inferalpha=1,
                                     alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
@@ -58,11 +63,12 @@ def _chain(job):
     ref = RefLib()
     N, _, L = raw.shape
     m = ref_model(N=N, L=L, K=K, maxalleles=2, **model)
-    ch = ref.chain_new(m, raw, seed=1000 * (1 if name == "c1" else 2) + r)
+    ch = ref.chain_new(m, raw, seed=1000 * (2 if name == "c2s" else 1) + r)
     ref.lib.stref_chain_sweeps(ch, model["burnin"] + model["numreps"])
     v = ref.chain_view(ch, N, L, K)
     return dict(sumlikes=v["sumlikes"], sumsqlikes=v["sumsqlikes"], QSum=v["QSum"],
-                sumAlpha=v["sumAlpha"], FstSum=v["FstSum"], Alpha=v["Alpha"], Fst=v["Fst"])
+                sumAlpha=v["sumAlpha"], FstSum=v["FstSum"], Alpha=v["Alpha"], Fst=v["Fst"],
+                sumlambda=v["sumlambda"])
 
 
 def main():

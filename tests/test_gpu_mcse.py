@@ -5,8 +5,8 @@ The device chains and the reference's own CPU chains (tests/golden/mcse_*.npz,
 made by tests/golden/make_mcse.py with the reference functions compiled from
 its sources) use different random streams and different Dirichlet samplers,
 so single draws cannot be compared; whole runs are compared through their
-summaries instead: mean and variance of ln P(D), mean alpha, mean F (F model)
-and the posterior-mean Q.  Eight chains per side; each summary's standard
+summaries instead: mean and variance of ln P(D), mean alpha, mean F (F model),
+mean lambda (INFERLAMBDA) and the posterior-mean Q.  Eight chains per side; each summary's standard
 error comes from the spread over chains.  Population labels are arbitrary in
 every chain, so each chain's labels are first matched to the generating Q.
 
@@ -66,13 +66,13 @@ def _run_device(ctx, z, model, mala=0):
               freqscorr=model["freqscorr"], inferalpha=model["inferalpha"], alpha=model["alpha"],
               alphapropsd=model["alphapropsd"], metrofreq=model["metrofreq"],
               lambda_=model["lambda_"], mala=mala)
-    for k in ("fpriormean", "fpriorsd"):
+    for k in ("fpriormean", "fpriorsd", "inferlambda"):
         if k in model:
             mk[k] = model[k]
     chains = [api.Chain(ctx, data, api.model_defaults(**mk), 77000 + r) for r in range(R)]
     b = api.Batch(ctx, chains)
     b.sweep(model["burnin"] + model["numreps"])
-    res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[])
+    res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[], sumlambda=[])
     for c in chains:
         assert c.sync() == 0
         if mala:
@@ -85,6 +85,7 @@ def _run_device(ctx, z, model, mala=0):
         res["QSum"].append(c.get(api.F_QSUM))
         res["sumAlpha"].append(c.get(api.F_SUMALPHA))
         res["FstSum"].append(c.get(api.F_FSTSUM))
+        res["sumlambda"].append(c.get(api.F_SUMLAMBDA))
     b.close()
     for c in chains:
         c.close()
@@ -92,7 +93,7 @@ def _run_device(ctx, z, model, mala=0):
     return {k: np.array(v) for k, v in res.items()}
 
 
-@pytest.mark.parametrize("name,mala", [("c1", 0), ("c2s", 0), ("c2s", 1)])
+@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c2s", 0), ("c2s", 1)])
 def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
     """mala=1: the same chains with the Langevin move on Q added to every
     sweep still sample the reference's posterior."""
@@ -114,6 +115,10 @@ def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
         assert _z(sd[k], sr[k]) <= 5.0, (k, report)
     if model["freqscorr"]:
         assert (_z(sd["F"], sr["F"]) <= 5.0).all(), (sd["F"].mean(0), sr["F"].mean(0))
+    if model.get("inferlambda"):
+        ld, lr = dev["sumlambda"][:, 0] / n, z["sumlambda"][:, 0] / n
+        print("  lambda   ", ld.mean(), lr.mean(), "z", float(_z(ld, lr)))
+        assert _z(ld, lr) <= 5.0, (ld.mean(), lr.mean())
     zq = _z(sd["Q"], sr["Q"], floor=0.002)
     assert zq.max() <= 6.0, zq.max()
     assert np.abs(sd["Q"].mean(0) - sr["Q"].mean(0)).mean() <= 0.01

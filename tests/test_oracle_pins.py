@@ -330,3 +330,45 @@ def test_loglik_grad_oracle_matches_finite_differences_and_calclike(orc, ref):
         b[l, k, a_] -= h
         fd = (orc.loglik_grad(g, ql, a)[0] - orc.loglik_grad(g, ql, b)[0]) / (2 * h)
         assert abs(fd - dp[l, k, a_]) <= 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("freqscorr,popspecific", [(0, 0), (1, 0), (0, 1)])
+def test_update_lambda_matches_reference(orc, ref, freqscorr, popspecific):
+    """UpdateLambda / UpdatePopLambda fed the oracle's normals and rand()
+    words make the same moves; the oracle's log ratios are the reference's."""
+    from structure_b200 import synth
+    from oracle.oracle import S_LAMBDA
+    d = synth.microsat(N=30, L=50, K=3, seed=12)
+    na = d["numalleles"].astype(np.int32)
+    L, K, A = len(na), 3, int(na.max())
+    rng = np.random.default_rng(4 + freqscorr + 2 * popspecific)
+    key, rep = 0x1A3B, 7
+    for trial in range(6):
+        P = np.zeros((L, K, A))
+        for l in range(L):
+            P[l, :, :na[l]] = rng.dirichlet(np.full(na[l], 0.8), K)
+        logP = np.log(np.maximum(P, 1e-300)).astype(np.float32)
+        Pd = np.where(P > 0, np.exp(logP.astype(np.float64)), 0.0)
+        eps = np.zeros((L, A))
+        for l in range(L):
+            eps[l, :na[l]] = rng.dirichlet(np.ones(na[l]) * 3)
+        lam = rng.uniform(0.3, 3.0, K) if popspecific else np.full(K, rng.uniform(0.3, 3.0))
+        mine, lpd = orc.update_lambda(na, logP, eps, freqscorr, popspecific, lam, key, rep + trial)
+        npop = K if popspecific else 1
+        normals = [orc.normal(q, rep + trial, S_LAMBDA, key) for q in range(npop)]
+        rands = []
+        for q in range(npop):
+            nw = lam[q] + 0.3 * normals[q]
+            if 0 < nw < 10:
+                rands += rnd_words(orc.stream(q, 1, rep + trial, S_LAMBDA, key))
+        ref.set_globals(N=30, L=L, K=K, maxalleles=A, freqscorr=freqscorr)
+        theirs = lam.copy()
+        ref.normal_queue(normals)
+        ref.rand_queue(rands)
+        if popspecific:
+            ref.lib.UpdatePopLambda(Pd.copy(), theirs, na)
+        else:
+            ref.lib.UpdateLambda(Pd.copy(), eps.copy(), theirs, na)
+        ref.rand_queue(None)
+        ref.normal_queue(None)
+        np.testing.assert_array_equal(mine, theirs)
