@@ -115,7 +115,7 @@ int st_data_layout(const st_data *data);
 typedef struct st_model {
     int32_t maxpops;           /* MAXPOPS (K), 1..32 */
     int32_t burnin, numreps;   /* BURNIN, NUMREPS */
-    int32_t noadmix;           /* NOADMIX: must be 0 */
+    int32_t noadmix;           /* NOADMIX: each individual from one population */
     int32_t linkage;           /* LINKAGE: must be 0 */
     int32_t usepopinfo;        /* USEPOPINFO: must be 0 */
     int32_t locprior;          /* LOCPRIOR: must be 0 */
@@ -148,7 +148,9 @@ typedef struct st_model {
                                 * 2-bit data, K <= 16).  No reference counterpart. */
     int32_t mala_target;       /* step-size adaptation target, acceptance x 1000
                                 * (0 = 574); steps adapt during burn-in only */
-    int32_t reserved[6];
+    int32_t admburnin;         /* ADMBURNIN: NOADMIX chains use the admixture Q update
+                                * (and update alpha) until this sweep */
+    int32_t reserved[5];
 } st_model;
 
 int st_model_defaults(st_model *m);

@@ -24,7 +24,8 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _ci, _cd, _cu32, _cu64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
 
-S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA, S_LAMBDA = range(1, 12)
+(S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA, S_LAMBDA,
+ S_NOADMIX) = range(1, 13)
 
 
 def rnd_words(w):
@@ -92,6 +93,8 @@ class Oracle:
         lib.orc_loglik_grad.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f64p, _f64p, _f64p, _f64p,
                                         _f64p]
         lib.orc_loglik_grad.restype = _cd
+        lib.orc_update_q_noadmix.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _cu64, _cu32,
+                                             _f32p, _f32p, _i32p]
         lib.orc_update_lambda.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f64p, _ci, _ci, _f64p,
                                           _cu64, _cu32, _f64p]
         lib.orc_mala_step.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f32p, _f32p, _f64p, _ci, _f32p,
@@ -253,6 +256,15 @@ class Oracle:
     def est_logprob(self, s, ss, reps):
         return self.lib.orc_est_logprob(s, ss, reps)
 
+    def update_q_noadmix(self, geno, logP, key, rep):
+        N, _, L = geno.shape
+        _, K, A = logP.shape
+        Q, lQ = np.zeros((N, K), np.float32), np.zeros((N, K), np.float32)
+        pick = np.zeros(N, np.int32)
+        self.lib.orc_update_q_noadmix(N, L, K, A, np.ascontiguousarray(geno, np.int32),
+                                      np.ascontiguousarray(logP, np.float32), key, rep, Q, lQ, pick)
+        return Q, lQ, pick
+
     def update_lambda(self, numalleles, logP, eps, freqscorr, popspecific, lam, key, rep):
         L, K, A = logP.shape
         out = np.ascontiguousarray(lam, np.float64).copy()
@@ -296,7 +308,8 @@ class RefModel(C.Structure):
                                    "ancestdist", "numboxes")] + \
               [(n, _cd) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
                                   "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
-              [("inferlambda", _ci), ("popspecificlambda", _ci)]
+              [("inferlambda", _ci), ("popspecificlambda", _ci), ("noadmix", _ci),
+               ("admburnin", _ci)]
 
 
 class RefView(C.Structure):
@@ -313,7 +326,8 @@ def ref_model(**kw):
              unifprioralpha=1, metrofreq=10, burnin=0, numreps=1, computeprob=1,
              pfrompopflagonly=0, ancestdist=0, numboxes=1000, alpha=1.0, alphamax=10.0,
              alphapropsd=0.025, alphapriora=0.05, alphapriorb=0.001, lambda_=1.0,
-             fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0)
+             fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0, noadmix=0,
+             admburnin=0)
     d.update(kw)
     return RefModel(**d)
 
@@ -365,6 +379,7 @@ class RefLib:
         lib.UpdateAlpha.argtypes = [_f64p, _f64p, C.c_void_p, _ci]
         lib.UpdateLambda.argtypes = [_f64p, _f64p, _f64p, _i32p]
         lib.UpdatePopLambda.argtypes = [_f64p, _f64p, _i32p]
+        lib.UpdateQNoAdmix.argtypes = [_i32p, _f64p, _f64p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.UpdateP.argtypes = [_f64p, _f64p, _f64p, _i32p, _i32p, _i32p, _f64p, C.c_void_p, _f64p]
         lib.stref_guard_hits.restype = C.c_long
         lib.UpdateEpsilon.argtypes = [_f64p, _f64p, _f64p, _i32p, _cd]

@@ -138,6 +138,7 @@ typedef struct stref_model {
     double alpha, alphamax, alphapropsd, alphapriora, alphapriorb;
     double lambda, fpriormean, fpriorsd;
     int inferlambda, popspecificlambda;
+    int noadmix, admburnin;
 } stref_model;
 
 void stref_set_globals(const stref_model *m)
@@ -152,10 +153,10 @@ void stref_set_globals(const stref_model *m)
     METROFREQ = m->metrofreq; BURNIN = m->burnin; NUMREPS = m->numreps;
     COMPUTEPROB = m->computeprob; PFROMPOPFLAGONLY = m->pfrompopflagonly;
     ANCESTDIST = m->ancestdist; NUMBOXES = m->numboxes > 0 ? m->numboxes : 1000;
-    USEPOPINFO = 0; NOADMIX = 0; LOCPRIOR = 0; LINKAGE = 0; RECESSIVEALLELES = 0;
+    USEPOPINFO = 0; NOADMIX = m->noadmix; LOCPRIOR = 0; LINKAGE = 0; RECESSIVEALLELES = 0;
     INFERLAMBDA = m->inferlambda; POPSPECIFICLAMBDA = m->popspecificlambda;
     STARTATPOPINFO = 0; POPDATA = 0;
-    INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = 0;
+    INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = m->admburnin;
     NOALPHA = 0; PHASED = 0; PHASEINFO = 0; MARKOVPHASE = 0; NOQS = 0;
     LOCDATA = 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0; GENSBACK = 2;
 }

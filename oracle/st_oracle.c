@@ -850,3 +850,40 @@ void orc_update_lambda(int L, int K, int A, const int32_t *numalleles, const flo
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Updates/UpdateQ.c:310-383 UpdateQNoAdmix with mymath.c:80-100 PickAnOption */
+/* ------------------------------------------------------------------------ */
+void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const float *logP,
+                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick)
+{
+    double p[64];
+    for (int i = 0; i < N; i++) {
+        double mx = 0.0;
+        for (int k = 0; k < K; k++) {
+            double s = 0.0;
+            for (int l = 0; l < L; l++)
+                for (int line = 0; line < 2; line++) {
+                    int a = geno[((size_t)i * 2 + line) * L + l];
+                    if (a >= 0) s += (double)logP[((size_t)l * K + k) * A + a];
+                }
+            p[k] = s;
+            if (k == 0 || s > mx) mx = s;
+        }
+        double sum = 0.0;
+        for (int k = 0; k < K; k++) sum += (p[k] = exp(p[k] - mx));
+        uint32_t w[4];
+        philox4((uint32_t)i, 0, rep, ORC_S_NOADMIX, key, w);
+        double r = (double)(w[0] >> 1) / 2147483648.0 * sum, cum = 0.0;
+        int pk = K - 1;
+        for (int k = 0; k < K; k++) {
+            cum += p[k];
+            if (r <= cum) { pk = k; break; }
+        }
+        if (pick) pick[i] = pk;
+        for (int k = 0; k < K; k++) {
+            Q[(size_t)i * K + k] = k == pk ? 1.0f : 0.0f;
+            logQ[(size_t)i * K + k] = k == pk ? 0.0f : -INFINITY;
+        }
+    }
+}

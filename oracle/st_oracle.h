@@ -29,7 +29,7 @@ extern "C" {
 enum {
     ORC_S_INITZ = 1, ORC_S_Z = 2, ORC_S_P = 3, ORC_S_QG = 4, ORC_S_QM = 5,
     ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10,
-    ORC_S_LAMBDA = 11
+    ORC_S_LAMBDA = 11, ORC_S_NOADMIX = 12
 };
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
@@ -100,6 +100,13 @@ void orc_fst_diffs(int L, int K, int A, const int32_t *numalleles,
 void orc_update_fst(int K, int onefst, double fpriormean, double fpriorsd,
                     int Leff, const double *diff, const double *newf,
                     double *F, uint64_t key, uint32_t rep, double *lpd_out);
+
+/* --- NOADMIX Q (Updates/UpdateQ.c:310-383, mymath.c:80-100) -------------- */
+/* ll_ik = sum over loci and copies of logP[l][k][allele] (FP64); pick k with
+ * u*sum <= cumulative exp(ll - max), u = (w>>1)/2^31 of the Philox word at
+ * (i, 0) of ORC_S_NOADMIX.  Q, logQ become one-hot (0 / -inf). */
+void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const float *logP,
+                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick);
 
 /* --- lambda (Updates/UpdateLambda.c:8-102) ------------------------------- */
 /* logP [L][K][A] (log P as stored), eps [L][A]; popspecific: one value per

@@ -51,8 +51,8 @@ class Model(C.Structure):
         [(n, C.c_double) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
                                    "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
         [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r", "mala",
-                                  "mala_target")] + \
-        [("reserved", C.c_int32 * 6)]
+                                  "mala_target", "admburnin")] + \
+        [("reserved", C.c_int32 * 5)]
 
 
 _lib = None

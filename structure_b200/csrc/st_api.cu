@@ -270,7 +270,10 @@ int ind(st_chain* c, int mode, int stages) {
 int check_model(st_ctx* ctx, const st_model* m) {
   if (m->maxpops < 1 || m->maxpops > kMaxPops)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "MAXPOPS=%d outside 1..%d", m->maxpops, kMaxPops);
-  if (m->noadmix) return seterr(ctx, ST_ERR_UNSUPPORTED, "NOADMIX=1 is not on the GPU path");
+  if (m->noadmix && m->mala)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move needs the admixture model");
+  if (m->noadmix && m->admburnin >= m->burnin)
+    return seterr(ctx, ST_ERR_ARG, "ADMBURNIN must finish before BURNIN (src/Util.c:70)");
   if (m->linkage) return seterr(ctx, ST_ERR_UNSUPPORTED, "LINKAGE=1 is not on the GPU path");
   if (m->usepopinfo) return seterr(ctx, ST_ERR_UNSUPPORTED, "USEPOPINFO=1 is not on the GPU path");
   if (m->locprior) return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR=1 is not on the GPU path");
@@ -548,6 +551,7 @@ extern "C" int st_model_defaults(st_model* m) {
   // src/params.c:571-670 PresetValues
   m->maxpops = 2;
   m->burnin = 10000;
+  m->admburnin = 2500;   // src/params.c:610 (BURNIN/4 of the preset BURNIN)
   m->numreps = 20000;
   m->freqscorr = 1;
   m->onefst = 0;
@@ -589,6 +593,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   h.freqscorr = model->freqscorr; h.onefst = model->onefst; h.inferalpha = model->inferalpha;
   h.popalphas = model->popalphas; h.unifprioralpha = model->unifprioralpha;
   h.inferlambda = model->inferlambda; h.popspecificlambda = model->popspecificlambda;
+  h.noadmix = model->noadmix; h.admburnin = model->admburnin;
   h.computeprob = model->computeprob; h.pfrompopflagonly = model->pfrompopflagonly;
   h.ancestdist = model->ancestdist; h.numboxes = model->numboxes > 0 ? model->numboxes : 1;
   h.metrofreq = model->metrofreq; h.burnin = model->burnin;
@@ -648,6 +653,11 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       {&ctr, (size_t)kCtrCount * 4}, {&rep, 4}, {&err, 4}, {&chain, sizeof(ChainDev)},
       {&prefix, 16}};
   if (model->store_z) bufs.push_back({&Z, (size_t)N * 2 * L});
+  void* napart = nullptr;
+  if (model->noadmix) {
+    noadmix_plan(N, L, &h.na_lchunks, &h.na_lchunk_len);
+    bufs.push_back({&napart, (size_t)h.na_lchunks * NK * 8});
+  }
   void *mQp = nullptr, *mG = nullptr, *mGp = nullptr, *mLL = nullptr, *mLLp = nullptr,
        *mTh = nullptr, *mThp = nullptr, *mEps = nullptr, *mgq = nullptr, *mll = nullptr,
        *mbp = nullptr;
@@ -681,6 +691,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   c->d_chain = (ChainDev*)chain;
   c->d_prefix = (int*)prefix;
   data->chains++;
+  h.napart = (double*)napart;
   h.mala = model->mala ? 1 : 0;
   h.mala_target = (model->mala_target > 0 ? model->mala_target : 574) / 1000.0f;
   if (model->mala) {
@@ -787,9 +798,29 @@ extern "C" int st_update_fst(st_chain* c) {
   return locus(c, kLocFst);
 }
 
+// NOADMIX schedule (src/Updates/UpdateQ.c:738-745, UpdateAlpha.c:204): the
+// one-population update from sweep ADMBURNIN+1 (or BURNIN+1), admixture Gibbs
+// before it; alpha moves only before sweep ADMBURNIN (or BURNIN+1).
+static bool noadmix_q(const ChainDev& h, int rep) {
+  return h.noadmix && (rep > h.admburnin || rep > h.burnin);
+}
+static bool alpha_moves(const ChainDev& h, int rep) {
+  return !(h.noadmix && (rep >= h.admburnin || rep > h.burnin));
+}
+
 static int update_q_impl(st_chain* c, int stages) {
   const int rep = c->host_rep;
-  if (c->h.metrofreq > 0 && rep % c->h.metrofreq == 0) {
+  if (!alpha_moves(c->h, rep)) stages &= ~kIndAlpha;
+  if (noadmix_q(c->h, rep)) {
+    {
+      Bracket br(c->ctx, ST_K_IND);
+      c->ctx->launches++;   // two kernels
+      int rc = cuda_check(c->ctx, launch_noadmix(c->h, c->d_chain, c->ctx->stream), "noadmix");
+      if (rc) return rc;
+    }
+    return ind(c, kIndNone, stages);
+  }
+  if (!c->h.noadmix && c->h.metrofreq > 0 && rep % c->h.metrofreq == 0) {
     int rc = ind(c, kIndPropose, 0);
     if (!rc) rc = zpass(c, kZMetro, 0);
     if (!rc) rc = ind(c, kIndAccept, stages);
@@ -1137,11 +1168,12 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
     if (c->ctx != ctx || c->fast != b->fast || c->h.metrofreq != c0->h.metrofreq ||
         c->host_rep != c0->host_rep || c->model.store_z != c0->model.store_z ||
         c->model.precision != c0->model.precision ||
-        c->h.computeprob != c0->h.computeprob) {
+        c->h.computeprob != c0->h.computeprob || c->h.noadmix != c0->h.noadmix ||
+        (c0->h.noadmix && (c->h.admburnin != c0->h.admburnin || c->h.burnin != c0->h.burnin))) {
       delete b;
       return seterr(ctx, ST_ERR_ARG,
                     "batched chains must share the context, data path, METROFREQ, COMPUTEPROB, "
-                    "sweep counter and Z storage");
+                    "NOADMIX schedule, sweep counter and Z storage");
     }
     G = std::max(G, c->h.G);
   }
@@ -1268,8 +1300,21 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
     Bracket br(ctx, ST_K_IND);
     ST_CUDA(ctx, launch_ind(li, b->G, kIndAccept, kIndAlpha | kIndCollect, kBlockInd));
   } else {
-    Bracket br(ctx, ST_K_IND);
-    ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, kIndAlpha | kIndCollect, kBlockInd));
+    // NOADMIX batches share the schedule (checked at st_batch_create)
+    const int rep = c0->host_rep;
+    const int astage = alpha_moves(c0->h, rep) ? kIndAlpha : 0;
+    if (noadmix_q(c0->h, rep)) {
+      for (st_chain* c : b->chains) {
+        Bracket br(ctx, ST_K_IND);
+        ctx->launches++;   // two kernels
+        ST_CUDA(ctx, launch_noadmix(c->h, c->d_chain, s));
+      }
+      Bracket br(ctx, ST_K_IND);
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndNone, astage | kIndCollect, kBlockInd));
+    } else {
+      Bracket br(ctx, ST_K_IND);
+      ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, astage | kIndCollect, kBlockInd));
+    }
   }
   for (st_chain* c : b->chains)
     if (c->h.mala && c->h.K > 1)
@@ -1345,11 +1390,11 @@ extern "C" int st_batch_sweep(st_batch* b, int nsweeps) {
   cudaStream_t s = ctx->stream;
   // graphs replay the same launches; per-launch profiling events need the
   // direct path, and the legacy default stream cannot be captured
-  const bool graphs = b->graphs && !ctx->profile && s != nullptr;
+  const bool graphs = b->graphs && !ctx->profile && s != nullptr && !c0->h.noadmix;
   cudaEventRecord(b->ev0, s);
   for (int sw = 0; sw < nsweeps; sw++) {
     const int rep = c0->host_rep;
-    const bool metro = c0->h.metrofreq > 0 && rep % c0->h.metrofreq == 0;
+    const bool metro = !c0->h.noadmix && c0->h.metrofreq > 0 && rep % c0->h.metrofreq == 0;
     if (graphs && batch_graph(b, metro)) {
       ST_CUDA(ctx, cudaGraphLaunch(b->gx[metro ? 1 : 0], s));
       ctx->launches += b->glaunches[metro ? 1 : 0];

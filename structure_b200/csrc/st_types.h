@@ -15,7 +15,7 @@ constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
 // Philox stream ids (counter word 3 = id << 24).
 enum Stream : uint32_t {
   kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
-  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11
+  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11, kSNoAdmix = 12
 };
 
 // Device error word bits.
@@ -92,6 +92,11 @@ struct ChainDev {
   int* rep;                             // device sweep counter
   int* err;                             // device error word
   const double* injected;               // parity uniforms (reference slots)
+  // no-admixture model (NOADMIX): per-individual log likelihood of each
+  // population, partial over locus chunks, then a categorical pick
+  int noadmix, admburnin;
+  double* napart;                       // [na_lchunks][N][K]
+  int na_lchunks, na_lchunk_len;
   // optional Langevin move on Q (Z summed out)
   int mala;
   float mala_target;

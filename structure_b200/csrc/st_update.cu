@@ -487,7 +487,8 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
     if (sHits && threadIdx.x == 0) atomicAdd(&ch.stats[kStMetroHits], (double)sHits);
     if (collect && tile == 0 && threadIdx.x == 0)
       for (int q = 0; q < K; q++) {
-        if (!ch.inferalpha) ch.sumAlpha[q] += ch.alpha[q];
+        // src/output.c:79-83: no alpha sums under NOADMIX
+        if (!ch.inferalpha && !ch.noadmix) ch.sumAlpha[q] += ch.alpha[q];
         ch.sumlambda[q] += ch.lambda[q];
       }
   }

@@ -5,8 +5,8 @@
 // through libstgpu (include/stgpu.h), prints progress every UPDATEFREQ
 // sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
 //
-// Options the GPU path does not implement (LINKAGE, NOADMIX, USEPOPINFO,
-// LOCPRIOR, RECESSIVEALLELES, PLOIDY other than 2) stop the
+// Options the GPU path does not implement (LINKAGE, USEPOPINFO, LOCPRIOR,
+// RECESSIVEALLELES, PLOIDY other than 2) stop the
 // program with a message instead of running a different model.
 #include <cstdio>
 #include <cstdlib>
@@ -42,8 +42,7 @@ int die(const char* what, const char* msg) {
 int main(int argc, char** argv) {
   stf_run* r = nullptr;
   if (stf_open(argc, argv, &r) != STF_OK) return die("parameters", stf_last_error(r));
-  const char* unsupported[] = {"LINKAGE", "NOADMIX", "USEPOPINFO", "LOCPRIOR",
-                               "RECESSIVEALLELES"};
+  const char* unsupported[] = {"LINKAGE", "USEPOPINFO", "LOCPRIOR", "RECESSIVEALLELES"};
   for (const char* k : unsupported)
     if (pi(r, k)) {
       fprintf(stderr, "%s=1 is not available on the GPU path.\n", k);
@@ -107,6 +106,8 @@ int main(int argc, char** argv) {
   m.onefst = pi(r, "ONEFST");
   m.inferalpha = pi(r, "INFERALPHA");
   m.popalphas = pi(r, "POPALPHAS");
+  m.noadmix = pi(r, "NOADMIX");
+  m.admburnin = pi(r, "ADMBURNIN");
   m.inferlambda = pi(r, "INFERLAMBDA");
   m.popspecificlambda = pi(r, "POPSPECIFICLAMBDA");
   m.unifprioralpha = pi(r, "UNIFPRIORALPHA");

@@ -17,6 +17,8 @@ Runs:
          missing; admixture, alpha inferred, independent frequencies, lambda=1;
          1,000 burn-in + 10,000 sweeps; 8 chains.
   c1l -- the same data and run with lambda inferred (INFERLAMBDA=1).
+  c1n -- the same data under the no-admixture model (NOADMIX=1, ADMBURNIN=500);
+         24 chains (the variance of ln P(D) varies more between chains here).
   c2s -- N=200, L=1,000 biallelic SNPs, K=3 F model (F = .10, .20, .30), 3%
          genotypes missing; alpha and F inferred; 2,000 burn-in + 4,000 sweeps;
          8 chains.
@@ -48,6 +50,10 @@ def runs():
                     K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
                                     alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
                                     inferlambda=1)),
+        "c1n": dict(geno=c1["geno"], raw=c1["geno_raw"], numalleles=c1["numalleles"], Q=c1["Q"],
+                    K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
+                                    alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
+                                    noadmix=1, admburnin=500), chains=24),
         "c2s": dict(geno=c2["geno"], raw=c2["geno"], numalleles=c2["numalleles"], Q=c2["Q"],
                     K=3, model=dict(burnin=2000, numreps=4000, freqscorr=1, inferalpha=1,
                                     alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
@@ -77,8 +83,9 @@ def main():
     for name, run in runs().items():
         if only and name not in only:
             continue
-        jobs = [(name, r, run["raw"], run["K"], run["model"]) for r in range(CHAINS)]
-        with ctx.Pool(min(CHAINS, os.cpu_count() or 1)) as pool:
+        nch = run.get("chains", CHAINS)
+        jobs = [(name, r, run["raw"], run["K"], run["model"]) for r in range(nch)]
+        with ctx.Pool(min(nch, os.cpu_count() or 1)) as pool:
             res = pool.map(_chain, jobs)
         out = {k: np.array([x[k] for x in res]) for k in res[0]}
         np.savez_compressed(os.path.join(HERE, f"mcse_{name}.npz"),

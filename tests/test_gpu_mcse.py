@@ -66,7 +66,7 @@ def _run_device(ctx, z, model, mala=0):
               freqscorr=model["freqscorr"], inferalpha=model["inferalpha"], alpha=model["alpha"],
               alphapropsd=model["alphapropsd"], metrofreq=model["metrofreq"],
               lambda_=model["lambda_"], mala=mala)
-    for k in ("fpriormean", "fpriorsd", "inferlambda"):
+    for k in ("fpriormean", "fpriorsd", "inferlambda", "noadmix", "admburnin"):
         if k in model:
             mk[k] = model[k]
     chains = [api.Chain(ctx, data, api.model_defaults(**mk), 77000 + r) for r in range(R)]
@@ -93,7 +93,7 @@ def _run_device(ctx, z, model, mala=0):
     return {k: np.array(v) for k, v in res.items()}
 
 
-@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c2s", 0), ("c2s", 1)])
+@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c1n", 0), ("c2s", 0), ("c2s", 1)])
 def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
     """mala=1: the same chains with the Langevin move on Q added to every
     sweep still sample the reference's posterior."""

@@ -372,3 +372,32 @@ def test_update_lambda_matches_reference(orc, ref, freqscorr, popspecific):
         ref.rand_queue(None)
         ref.normal_queue(None)
         np.testing.assert_array_equal(mine, theirs)
+
+
+def test_update_q_noadmix_matches_reference(orc, ref):
+    """UpdateQNoAdmix (running product of P rescaled below 1e-100, then
+    PickAnOption on rand()) fed the oracle's rand() words picks the same
+    population for every individual."""
+    from structure_b200 import synth
+    from oracle.oracle import S_NOADMIX
+    d = synth.microsat(N=50, L=80, K=4, seed=21)
+    geno, na = d["geno"], d["numalleles"].astype(np.int32)
+    N, _, L = geno.shape
+    K, A = 4, int(na.max())
+    rng = np.random.default_rng(3)
+    P = np.zeros((L, K, A))
+    for l in range(L):
+        P[l, :, :na[l]] = rng.dirichlet(np.full(na[l], 0.9), K)
+    logP = np.log(np.maximum(P, 1e-300)).astype(np.float32)
+    Pd = np.where(P > 0, np.exp(logP.astype(np.float64)), 0.0)
+    key, rep = 0x9A9A, 11
+    Qo, _, pick = orc.update_q_noadmix(geno, logP, key, rep)
+    words = [int(orc.stream(i, 0, rep, S_NOADMIX, key)[0]) >> 1 for i in range(N)]
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, noadmix=1)
+    Qr = np.zeros((N, K))
+    ref.rand_queue(words)
+    ref.lib.UpdateQNoAdmix(geno.copy(), Qr, Pd.copy(), ref.individuals(N), None, None)
+    ref.rand_queue(None)
+    np.testing.assert_array_equal(Qr.argmax(1), pick)
+    np.testing.assert_array_equal(Qo, Qr.astype(np.float32))
+    assert len(set(pick)) > 1
