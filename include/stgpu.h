@@ -103,6 +103,7 @@ typedef struct st_data_desc {
     const uint32_t *packed;    /* B2G words or NULL */
     const int32_t *num_alleles;/* [num_loci] NumAlleles */
     const int32_t *popflags;   /* [num_inds] Individual[].PopFlag or NULL */
+    const int32_t *population; /* [num_inds] Individual[].Population (POPDATA) or NULL */
 } st_data_desc;
 
 int st_data_upload(st_ctx *ctx, const st_data_desc *desc, st_data **out);
@@ -117,7 +118,7 @@ typedef struct st_model {
     int32_t burnin, numreps;   /* BURNIN, NUMREPS */
     int32_t noadmix;           /* NOADMIX: each individual from one population */
     int32_t linkage;           /* LINKAGE: must be 0 */
-    int32_t usepopinfo;        /* USEPOPINFO: must be 0 */
+    int32_t usepopinfo;        /* USEPOPINFO (needs population data) */
     int32_t locprior;          /* LOCPRIOR: must be 0 */
     int32_t freqscorr;         /* FREQSCORR */
     int32_t onefst;            /* ONEFST */
@@ -150,7 +151,11 @@ typedef struct st_model {
                                 * (0 = 574); steps adapt during burn-in only */
     int32_t admburnin;         /* ADMBURNIN: NOADMIX chains use the admixture Q update
                                 * (and update alpha) until this sweep */
-    int32_t reserved[5];
+    int32_t gensback;          /* GENSBACK (USEPOPINFO) */
+    int32_t popflag_given;     /* 1: popflags in the data are POPFLAG values; 0: every
+                                * individual with a population is flagged (POPFLAG=0) */
+    int32_t reserved[2];
+    double migrprior;          /* MIGRPRIOR (USEPOPINFO) */
 } st_model;
 
 int st_model_defaults(st_model *m);
@@ -280,7 +285,9 @@ enum st_field {
     ST_F_REP,          /* int32: sweep counter */
     ST_F_ERR,          /* int32: device error word */
     ST_F_DIMS,         /* int32 [8]: N, L, K, A, layout, G, nchunks, ngroups */
-    ST_F_MALA_EPS      /* float [N]: Langevin step sizes (chains with st_model.mala) */
+    ST_F_MALA_EPS,     /* float [N]: Langevin step sizes (chains with st_model.mala) */
+    ST_F_USEPOPPROBS   /* double [N][K][GENSBACK+1]: USEPOPINFO posterior sums
+                        * (the reference's UsePopProbs, from sweep BURNIN on) */
 };
 int st_get_state(st_chain *c, int field, void *host, size_t bytes);
 int st_set_state(st_chain *c, int field, const void *host, size_t bytes);

@@ -25,7 +25,7 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _ci, _cd, _cu32, _cu64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
 
 (S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA, S_LAMBDA,
- S_NOADMIX) = range(1, 13)
+ S_NOADMIX, S_POPINFO) = range(1, 14)
 
 
 def rnd_words(w):
@@ -95,6 +95,8 @@ class Oracle:
         lib.orc_loglik_grad.restype = _cd
         lib.orc_update_q_noadmix.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _cu64, _cu32,
                                              _f32p, _f32p, _i32p]
+        lib.orc_update_q_withpops.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _i32p, _i32p,
+                                              _ci, _cd, _cu64, _cu32, _ci, _f32p, _f32p, _f64p]
         lib.orc_update_lambda.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f64p, _ci, _ci, _f64p,
                                           _cu64, _cu32, _f64p]
         lib.orc_mala_step.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f32p, _f32p, _f64p, _ci, _f32p,
@@ -265,6 +267,21 @@ class Oracle:
                                       np.ascontiguousarray(logP, np.float32), key, rep, Q, lQ, pick)
         return Q, lQ, pick
 
+    def update_q_withpops(self, geno, P, population, popflags, gensback, migrprior, key, rep,
+                          burnin, Q, logQ, usepop=None):
+        """USEPOPINFO migrant-model Q of the flagged individuals (others untouched)."""
+        N, _, L = geno.shape
+        _, K, A = P.shape
+        Qo = np.ascontiguousarray(Q, np.float32).copy()
+        lQo = np.ascontiguousarray(logQ, np.float32).copy()
+        up = np.zeros((N, K, gensback + 1)) if usepop is None else np.array(usepop, np.float64)
+        self.lib.orc_update_q_withpops(N, L, K, A, np.ascontiguousarray(geno, np.int32),
+                                       np.ascontiguousarray(P, np.float32),
+                                       np.ascontiguousarray(population, np.int32),
+                                       np.ascontiguousarray(popflags, np.int32), gensback,
+                                       migrprior, key, rep, burnin, Qo, lQo, up)
+        return Qo, lQo, up
+
     def update_lambda(self, numalleles, logP, eps, freqscorr, popspecific, lam, key, rep):
         L, K, A = logP.shape
         out = np.ascontiguousarray(lam, np.float64).copy()
@@ -309,7 +326,8 @@ class RefModel(C.Structure):
               [(n, _cd) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
                                   "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
               [("inferlambda", _ci), ("popspecificlambda", _ci), ("noadmix", _ci),
-               ("admburnin", _ci)]
+               ("admburnin", _ci), ("usepopinfo", _ci), ("gensback", _ci), ("popflag", _ci),
+               ("migrprior", _cd)]
 
 
 class RefView(C.Structure):
@@ -318,7 +336,7 @@ class RefView(C.Structure):
                                             "sumAlpha", "PSum", "QSum", "like", "sumlikes",
                                             "sumsqlikes")] + \
               [("maxalleles", _ci), ("rep", _ci)] + \
-              [(n, C.POINTER(_cd)) for n in ("lambda_", "sumlambda")]
+              [(n, C.POINTER(_cd)) for n in ("lambda_", "sumlambda", "UsePopProbs")]
 
 
 def ref_model(**kw):
@@ -327,7 +345,7 @@ def ref_model(**kw):
              pfrompopflagonly=0, ancestdist=0, numboxes=1000, alpha=1.0, alphamax=10.0,
              alphapropsd=0.025, alphapriora=0.05, alphapriorb=0.001, lambda_=1.0,
              fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0, noadmix=0,
-             admburnin=0)
+             admburnin=0, usepopinfo=0, gensback=2, popflag=0, migrprior=0.05)
     d.update(kw)
     return RefModel(**d)
 
@@ -351,7 +369,11 @@ class RefLib:
         lib.stref_individuals.argtypes = [_ci, C.c_void_p]
         lib.stref_individuals.restype = C.c_void_p
         lib.stref_free.argtypes = [C.c_void_p]
-        lib.stref_chain_new.argtypes = [C.POINTER(RefModel), _i32p, C.c_void_p, _cu64]
+        lib.stref_chain_new.argtypes = [C.POINTER(RefModel), _i32p, C.c_void_p, C.c_void_p, _cu64]
+        lib.stref_individuals_pop.argtypes = [_ci, C.c_void_p, C.c_void_p]
+        lib.stref_individuals_pop.restype = C.c_void_p
+        lib.UpdateQWithPops.argtypes = [_i32p, _f64p, _f64p, C.c_void_p, _f64p, _ci, C.c_void_p,
+                                        _f64p, C.c_void_p]
         lib.stref_chain_new.restype = C.c_void_p
         lib.stref_chain_sweeps.argtypes = [C.c_void_p, _ci]
         lib.stref_chain_sweeps.restype = _ci
@@ -421,13 +443,21 @@ class RefLib:
         self.lib.stref_normal_queue(v.ctypes.data, v.size)
 
     # -- chain -----------------------------------------------------------------
-    def chain_new(self, model, geno, popflags=None, seed=1):
+    def chain_new(self, model, geno, popflags=None, seed=1, population=None):
         pf = None if popflags is None else np.ascontiguousarray(popflags, np.int32)
-        self._keep.append(pf)
+        pp = None if population is None else np.ascontiguousarray(population, np.int32)
+        self._keep += [pf, pp]
         return self.lib.stref_chain_new(C.byref(model), np.ascontiguousarray(geno, np.int32),
-                                        None if pf is None else pf.ctypes.data, seed)
+                                        None if pf is None else pf.ctypes.data,
+                                        None if pp is None else pp.ctypes.data, seed)
 
-    def chain_view(self, ch, N, L, K):
+    def individuals_pop(self, N, popflags, population):
+        pf = np.ascontiguousarray(popflags, np.int32)
+        pp = np.ascontiguousarray(population, np.int32)
+        self._keep += [pf, pp]
+        return self.lib.stref_individuals_pop(N, pf.ctypes.data, pp.ctypes.data)
+
+    def chain_view(self, ch, N, L, K, gensback=2):
         v = RefView()
         self.lib.stref_chain_view(ch, C.byref(v))
         A = v.maxalleles
@@ -444,4 +474,6 @@ class RefLib:
             PSum=arr(v.PSum, L * K * A).reshape(L, K, A), SumEps=arr(v.SumEps, L * A).reshape(L, A),
             FstSum=arr(v.FstSum, K), sumAlpha=arr(v.sumAlpha, K),
             like=v.like[0], sumlikes=v.sumlikes[0], sumsqlikes=v.sumsqlikes[0],
-            lambda_=arr(v.lambda_, K), sumlambda=arr(v.sumlambda, K))
+            lambda_=arr(v.lambda_, K), sumlambda=arr(v.sumlambda, K),
+            usepop=(arr(v.UsePopProbs, N * K * (gensback + 1)).reshape(N, K, gensback + 1)
+                    if v.UsePopProbs else None))

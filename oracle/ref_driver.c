@@ -139,6 +139,8 @@ typedef struct stref_model {
     double lambda, fpriormean, fpriorsd;
     int inferlambda, popspecificlambda;
     int noadmix, admburnin;
+    int usepopinfo, gensback, popflag;
+    double migrprior;
 } stref_model;
 
 void stref_set_globals(const stref_model *m)
@@ -153,18 +155,29 @@ void stref_set_globals(const stref_model *m)
     METROFREQ = m->metrofreq; BURNIN = m->burnin; NUMREPS = m->numreps;
     COMPUTEPROB = m->computeprob; PFROMPOPFLAGONLY = m->pfrompopflagonly;
     ANCESTDIST = m->ancestdist; NUMBOXES = m->numboxes > 0 ? m->numboxes : 1000;
-    USEPOPINFO = 0; NOADMIX = m->noadmix; LOCPRIOR = 0; LINKAGE = 0; RECESSIVEALLELES = 0;
+    USEPOPINFO = m->usepopinfo; NOADMIX = m->noadmix; LOCPRIOR = 0; LINKAGE = 0;
+    RECESSIVEALLELES = 0;
     INFERLAMBDA = m->inferlambda; POPSPECIFICLAMBDA = m->popspecificlambda;
-    STARTATPOPINFO = 0; POPDATA = 0;
+    STARTATPOPINFO = 0; POPDATA = m->usepopinfo ? 1 : 0; POPFLAG = m->popflag;
+    MIGRPRIOR = m->migrprior;
     INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = m->admburnin;
     NOALPHA = 0; PHASED = 0; PHASEINFO = 0; MARKOVPHASE = 0; NOQS = 0;
-    LOCDATA = 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0; GENSBACK = 2;
+    LOCDATA = 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0;
+    GENSBACK = m->usepopinfo ? m->gensback : 2;
 }
 
 struct IND *stref_individuals(int N, const int32_t *popflags)
 {
     struct IND *ind = calloc((size_t)N, sizeof(struct IND));
     for (int i = 0; i < N; i++) ind[i].PopFlag = popflags ? popflags[i] : 0;
+    return ind;
+}
+
+/* individuals with a given population (1-based) as well */
+struct IND *stref_individuals_pop(int N, const int32_t *popflags, const int32_t *population)
+{
+    struct IND *ind = stref_individuals(N, popflags);
+    for (int i = 0; i < N; i++) ind[i].Population = population ? population[i] : 0;
     return ind;
 }
 void stref_free(void *p) { free(p); }
@@ -175,7 +188,7 @@ typedef struct stref_chain {
     int *Geno, *Z, *Z1, *NumAlleles, *Translation, *AncestDist;
     double *Q, *P, *Eps, *SumEps, *Fst, *FstSum, *Alpha, *sumAlpha;
     double *lambda, *sumlambda, *PSum, *QSum, *R, *sumR, *varR;
-    double *sumIndLikes, *indLikesNorm, *randomArr, *Phase;
+    double *sumIndLikes, *indLikesNorm, *randomArr, *Phase, *UsePopProbs;
     double like, sumlikes, sumsqlikes;
     size_t nrand;
     struct IND *Individual;
@@ -190,7 +203,7 @@ static void fill_uniform(double *a, size_t n)
 /* geno: raw int32 [N][2][L] with -9 missing; recoded in a private copy by the
  * reference's own Initialization -> CountAlleles. */
 stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
-                             const int32_t *popflags, uint64_t seed)
+                             const int32_t *popflags, const int32_t *population, uint64_t seed)
 {
     stref_chain *c = calloc(1, sizeof(stref_chain));
     int N = m->N, L = m->L, K = m->K;
@@ -228,7 +241,9 @@ stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
     c->sumIndLikes = calloc((size_t)N, sizeof(double));
     c->indLikesNorm = calloc((size_t)N, sizeof(double));
     if (m->ancestdist) c->AncestDist = calloc((size_t)N * K * NUMBOXES, sizeof(int));
-    c->Individual = stref_individuals(N, popflags);
+    c->Individual = stref_individuals_pop(N, popflags, population);
+    if (m->usepopinfo)
+        c->UsePopProbs = calloc((size_t)N * K * (GENSBACK + 1), sizeof(double));
     size_t nr = (size_t)N * L * 2;
     size_t np = (size_t)L * K * A * MAXRANDOM;
     size_t nq = (size_t)N * MAXRANDOM;
@@ -239,7 +254,7 @@ stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
     CLDict dict;
     Initialization(c->Geno, NULL, c->Individual, c->Translation, c->NumAlleles,
                    c->Z, c->Z1, c->Eps, c->SumEps, c->Fst, c->PSum, c->Q, c->QSum,
-                   c->FstSum, c->AncestDist, NULL, c->Alpha, c->sumAlpha, c->sumR,
+                   c->FstSum, c->AncestDist, c->UsePopProbs, c->Alpha, c->sumAlpha, c->sumR,
                    c->varR, &c->sumlikes, &c->sumsqlikes, &savefreq, c->R,
                    c->lambda, c->sumlambda, c->Phase, NULL, NULL, NULL, 0,
                    c->sumIndLikes, c->indLikesNorm, &dict);
@@ -261,7 +276,7 @@ int stref_chain_sweeps(stref_chain *c, int nsweeps)
         if (METROFREQ > 0 && rep % METROFREQ == 0)
             fill_uniform(c->randomArr, (size_t)N * MAXRANDOM);
         UpdateQ(c->Geno, NULL, c->Q, c->P, c->Z, c->Alpha, rep, c->Individual,
-                NULL, NULL, NULL, c->randomArr);
+                c->UsePopProbs, NULL, NULL, c->randomArr);
         fill_uniform(c->randomArr, (size_t)N * L * 2);
         UpdateZ(c->Z, c->Q, c->P, c->Geno, c->randomArr);
         if (INFERALPHA) UpdateAlpha(c->Q, c->Alpha, c->Individual, rep);
@@ -289,7 +304,7 @@ typedef struct stref_view {
     double *Q, *P, *Eps, *SumEps, *Fst, *FstSum, *Alpha, *sumAlpha;
     double *PSum, *QSum, *like, *sumlikes, *sumsqlikes;
     int maxalleles, rep;
-    double *lambda, *sumlambda;
+    double *lambda, *sumlambda, *UsePopProbs;
 } stref_view;
 
 void stref_chain_view(stref_chain *c, stref_view *v)
@@ -301,7 +316,7 @@ void stref_chain_view(stref_chain *c, stref_view *v)
     v->sumAlpha = c->sumAlpha; v->PSum = c->PSum; v->QSum = c->QSum;
     v->like = &c->like; v->sumlikes = &c->sumlikes; v->sumsqlikes = &c->sumsqlikes;
     v->maxalleles = c->m.maxalleles; v->rep = c->rep;
-    v->lambda = c->lambda; v->sumlambda = c->sumlambda;
+    v->lambda = c->lambda; v->sumlambda = c->sumlambda; v->UsePopProbs = c->UsePopProbs;
 }
 
 void stref_chain_free(stref_chain *c)
@@ -310,7 +325,7 @@ void stref_chain_free(stref_chain *c)
                   c->Q, c->P, c->Eps, c->SumEps, c->Fst, c->FstSum, c->Alpha,
                   c->sumAlpha, c->lambda, c->sumlambda, c->PSum, c->QSum, c->R,
                   c->sumR, c->varR, c->sumIndLikes, c->indLikesNorm, c->randomArr,
-                  c->Phase, c->Individual};
+                  c->Phase, c->Individual, c->UsePopProbs};
     for (size_t j = 0; j < sizeof(ps) / sizeof(ps[0]); j++) free(ps[j]);
     free(c);
 }

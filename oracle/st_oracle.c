@@ -887,3 +887,81 @@ void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Updates/UpdateQ.c:499-706 UpdateQWithPops: migrant model for individuals  */
+/* with prior population information.                                        */
+/* ------------------------------------------------------------------------ */
+void orc_update_q_withpops(int N, int L, int K, int A, const int32_t *geno, const float *P,
+                           const int32_t *population, const int32_t *popflags, int gensback,
+                           double migrprior, uint64_t key, uint32_t rep, int burnin, float *Q,
+                           float *logQ, double *usepop)
+{
+    const int G = gensback + 1;
+    double post[64 * 8], pri[8];
+    double w = 0.5, sw = 0.0;
+    for (int g = 0; g < G; g++) { w *= 2.0; pri[g] = w; sw += w * (K - 1); }
+    for (int g = 0; g < G; g++) pri[g] = migrprior * pri[g] / sw;
+    for (int i = 0; i < N; i++) {
+        if (!popflags[i]) continue;
+        const int home = population[i] - 1;
+        double mx = 0.0;
+        for (int k = 0; k < K; k++)
+            for (int g = 0; g < G; g++) {
+                const double p = g > 0 ? exp((g - 1) * log(0.5)) : 1.0;
+                double s = 0.0;
+                for (int l = 0; l < L; l++) {
+                    const int a0 = geno[((size_t)i * 2) * L + l];
+                    const int a1 = geno[((size_t)i * 2 + 1) * L + l];
+                    const float *Pl = P + (size_t)l * K * A;
+                    double like;
+                    if (a0 >= 0 && a1 >= 0) {
+                        double pk0 = Pl[k * A + a0], ph0 = Pl[home * A + a0];
+                        double pk1 = Pl[k * A + a1], ph1 = Pl[home * A + a1];
+                        like = g == 0 ? pk0 * pk1
+                                      : 0.5 * p * pk0 * ph1 + 0.5 * p * ph0 * pk1 +
+                                            (1.0 - p) * ph0 * ph1;
+                    } else if (a0 >= 0) {
+                        like = p * Pl[k * A + a0] + (1.0 - p) * Pl[home * A + a0];
+                    } else if (a1 >= 0) {
+                        like = p * Pl[home * A + a1] + (1.0 - p) * Pl[home * A + a1];
+                    } else {
+                        continue;
+                    }
+                    s += log(like > SQRT_UNDERFLO ? like : SQRT_UNDERFLO);
+                }
+                post[k * G + g] = s;
+                if ((k == 0 && g == 0) || s > mx) mx = s;
+            }
+        double sum = 0.0;
+        for (int g = 0; g < G; g++)
+            for (int k = 0; k < K; k++) {
+                double *v = &post[k * G + g];
+                *v = exp(*v - mx);
+                if (k == home) *v = g == 0 ? *v * (1.0 - migrprior) : 0.0;
+                else *v *= pri[g];
+                sum += *v;
+            }
+        if ((int)rep >= burnin)
+            for (int j = 0; j < K * G; j++) usepop[(size_t)i * K * G + j] += post[j] / sum;
+        uint32_t u[4];
+        philox4((uint32_t)i, 0, rep, ORC_S_POPINFO, key, u);
+        const double r = (double)(u[0] >> 1) / 2147483648.0 * sum;
+        double cum = 0.0;
+        int pk = home, pg = 0, done = 0;
+        for (int g = 0; g < G && !done; g++)
+            for (int k = 0; k < K; k++) {
+                cum += post[k * G + g];
+                if (r < cum) { pk = k; pg = g; done = 1; break; }
+            }
+        double q[64];
+        for (int k = 0; k < K; k++) q[k] = 0.0;
+        const double p = exp(pg * log(0.5));
+        q[pk] = p;
+        q[home] += 1.0 - p;
+        for (int k = 0; k < K; k++) {
+            Q[(size_t)i * K + k] = (float)q[k];
+            logQ[(size_t)i * K + k] = q[k] > 0.0 ? (float)log(q[k]) : -INFINITY;
+        }
+    }
+}

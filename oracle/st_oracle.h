@@ -29,7 +29,7 @@ extern "C" {
 enum {
     ORC_S_INITZ = 1, ORC_S_Z = 2, ORC_S_P = 3, ORC_S_QG = 4, ORC_S_QM = 5,
     ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10,
-    ORC_S_LAMBDA = 11, ORC_S_NOADMIX = 12
+    ORC_S_LAMBDA = 11, ORC_S_NOADMIX = 12, ORC_S_POPINFO = 13
 };
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
@@ -107,6 +107,16 @@ void orc_update_fst(int K, int onefst, double fpriormean, double fpriorsd,
  * (i, 0) of ORC_S_NOADMIX.  Q, logQ become one-hot (0 / -inf). */
 void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const float *logP,
                           uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick);
+
+/* --- USEPOPINFO Q (Updates/UpdateQ.c:499-706 UpdateQWithPops) ----------- */
+/* For flagged individuals (popflags[i] != 0, population[i] in 1..K): the
+ * migrant-model posterior over (gen, k), added to usepop [N][K][G+1] when
+ * rep >= burnin, and Q/logQ from the pick (u = (w>>1)/2^31 at (i, 0) of
+ * ORC_S_POPINFO).  P [L][K][A] as stored (float). */
+void orc_update_q_withpops(int N, int L, int K, int A, const int32_t *geno, const float *P,
+                           const int32_t *population, const int32_t *popflags, int gensback,
+                           double migrprior, uint64_t key, uint32_t rep, int burnin, float *Q,
+                           float *logQ, double *usepop);
 
 /* --- lambda (Updates/UpdateLambda.c:8-102) ------------------------------- */
 /* logP [L][K][A] (log P as stored), eps [L][A]; popspecific: one value per

@@ -21,7 +21,7 @@ LAYOUT_AUTO, LAYOUT_U8, LAYOUT_B2G = 0, 1, 2
 
 (F_Q, F_LOGQ, F_TESTQ, F_LOGTESTQ, F_P, F_LOGP, F_EPS, F_F, F_ALPHA, F_LAMBDA, F_Z, F_N,
  F_M, F_LOGDIFF, F_QSUM, F_PSUM, F_SUMEPS, F_FSTSUM, F_SUMALPHA, F_SUMLAMBDA, F_ANCESTDIST,
- F_STATS, F_REP, F_ERR, F_DIMS, F_MALA_EPS) = range(1, 27)
+ F_STATS, F_REP, F_ERR, F_DIMS, F_MALA_EPS, F_USEPOPPROBS) = range(1, 28)
 
 # stats block offsets (csrc/st_types.h)
 ST_LIKE, ST_SUMLIKES, ST_SUMSQ, ST_NLIKE, ST_METROHITS = 0, 1, 2, 3, 4
@@ -39,7 +39,8 @@ class StError(RuntimeError):
 class DataDesc(C.Structure):
     _fields_ = [("num_inds", C.c_int32), ("num_loci", C.c_int32), ("lines", C.c_int32),
                 ("layout", C.c_int32), ("geno", C.c_void_p), ("packed", C.c_void_p),
-                ("num_alleles", C.c_void_p), ("popflags", C.c_void_p)]
+                ("num_alleles", C.c_void_p), ("popflags", C.c_void_p),
+                ("population", C.c_void_p)]
 
 
 class Model(C.Structure):
@@ -51,8 +52,8 @@ class Model(C.Structure):
         [(n, C.c_double) for n in ("alpha", "alphamax", "alphapropsd", "alphapriora",
                                    "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
         [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r", "mala",
-                                  "mala_target", "admburnin")] + \
-        [("reserved", C.c_int32 * 5)]
+                                  "mala_target", "admburnin", "gensback", "popflag_given")] + \
+        [("reserved", C.c_int32 * 2), ("migrprior", C.c_double)]
 
 
 _lib = None
@@ -189,7 +190,7 @@ class Data:
     """Genotypes in HBM (reference layout in, packed on the device)."""
 
     def __init__(self, ctx, num_alleles, geno=None, packed=None, popflags=None, layout=LAYOUT_AUTO,
-                 num_inds=None, num_loci=None):
+                 num_inds=None, num_loci=None, population=None):
         self.ctx = ctx
         na = np.ascontiguousarray(num_alleles, np.int32)
         d = DataDesc()
@@ -206,10 +207,13 @@ class Data:
         d.lines = 2
         d.layout = layout
         d.num_alleles = na.ctypes.data
-        pf = None
+        pf = pp = None
         if popflags is not None:
             pf = np.ascontiguousarray(popflags, np.int32)
             d.popflags = pf.ctypes.data
+        if population is not None:
+            pp = np.ascontiguousarray(population, np.int32)
+            d.population = pp.ctypes.data
         self.N, self.L = d.num_inds, d.num_loci
         self.A = int(max(1, na.max()))
         self.num_alleles = na
@@ -230,7 +234,7 @@ _DT = {F_Q: np.float32, F_LOGQ: np.float32, F_TESTQ: np.float32, F_LOGTESTQ: np.
        F_LOGDIFF: np.float64, F_QSUM: np.float64, F_PSUM: np.float64, F_SUMEPS: np.float64,
        F_FSTSUM: np.float64, F_SUMALPHA: np.float64, F_SUMLAMBDA: np.float64,
        F_ANCESTDIST: np.int32, F_STATS: np.float64, F_REP: np.int32, F_ERR: np.int32,
-       F_DIMS: np.int32, F_MALA_EPS: np.float32}
+       F_DIMS: np.int32, F_MALA_EPS: np.float32, F_USEPOPPROBS: np.float64}
 
 
 class Chain:
@@ -249,7 +253,7 @@ class Chain:
                 F_P: (L, K, A), F_LOGP: (L, K, A), F_EPS: (L, A), F_SUMEPS: (L, A),
                 F_Z: (N, 2, L), F_N: (L, K, A), F_M: (N, K), F_LOGDIFF: (N,),
                 F_QSUM: (N, K), F_PSUM: (L, K, A), F_STATS: (256,), F_DIMS: (8,),
-                F_MALA_EPS: (N,)}.get(f, None)
+                F_MALA_EPS: (N,), F_USEPOPPROBS: (N, K, -1)}.get(f, None)
 
     def get(self, f):
         n = lib().st_field_bytes(self.h, f)

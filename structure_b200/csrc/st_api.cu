@@ -36,6 +36,7 @@ struct st_data {
   int32_t* numalleles = nullptr;
   int32_t* popflags = nullptr;
   std::vector<int32_t> na_h;
+  std::vector<int32_t> popflags_h, population_h;   // population empty: no POPDATA
   std::vector<int64_t> cnt_h;    // [L][A] allele copies observed
   std::vector<int64_t> tot_h;    // [L] non-missing copies
   size_t bytes = 0;
@@ -275,7 +276,12 @@ int check_model(st_ctx* ctx, const st_model* m) {
   if (m->noadmix && m->admburnin >= m->burnin)
     return seterr(ctx, ST_ERR_ARG, "ADMBURNIN must finish before BURNIN (src/Util.c:70)");
   if (m->linkage) return seterr(ctx, ST_ERR_UNSUPPORTED, "LINKAGE=1 is not on the GPU path");
-  if (m->usepopinfo) return seterr(ctx, ST_ERR_UNSUPPORTED, "USEPOPINFO=1 is not on the GPU path");
+  if (m->usepopinfo && (m->gensback < 0 || m->gensback > 7))
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "GENSBACK must be in 0..7");
+  if (m->usepopinfo && (m->migrprior < 0.0 || m->migrprior > 1.0))
+    return seterr(ctx, ST_ERR_ARG, "MIGRPRIOR must be in [0, 1] (src/Init.c:22-26)");
+  if (m->usepopinfo && m->mala)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move does not combine with USEPOPINFO");
   if (m->locprior) return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR=1 is not on the GPU path");
   if (m->recessivealleles)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "RECESSIVEALLELES=1 is not on the GPU path");
@@ -478,6 +484,8 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
   std::vector<int32_t> pf(N, 0);
   if (d->popflags) pf.assign(d->popflags, d->popflags + N);
   cudaMemcpy(s->popflags, pf.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice);
+  s->popflags_h = pf;
+  if (d->population) s->population_h.assign(d->population, d->population + N);
 
   if (s->layout == kLayoutB2G) {
     const int wpr = (N + 15) / 16;
@@ -552,6 +560,8 @@ extern "C" int st_model_defaults(st_model* m) {
   m->maxpops = 2;
   m->burnin = 10000;
   m->admburnin = 2500;   // src/params.c:610 (BURNIN/4 of the preset BURNIN)
+  m->gensback = 2;       // src/params.c:627
+  m->migrprior = 0.05;   // src/params.c:629
   m->numreps = 20000;
   m->freqscorr = 1;
   m->onefst = 0;
@@ -594,6 +604,30 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   h.popalphas = model->popalphas; h.unifprioralpha = model->unifprioralpha;
   h.inferlambda = model->inferlambda; h.popspecificlambda = model->popspecificlambda;
   h.noadmix = model->noadmix; h.admburnin = model->admburnin;
+  h.usepopinfo = model->usepopinfo; h.gensback = model->gensback; h.migrprior = model->migrprior;
+  h.alpha_n = N;
+  // USEPOPINFO flags as src/Init.c:15-70 CheckPopPriors leaves them: everybody
+  // without a POPFLAG column, then nobody whose population is outside 1..K
+  std::vector<int32_t> pflag, pop1, initpop;
+  if (model->usepopinfo) {
+    if (data->population_h.empty()) {
+      delete c;
+      return seterr(ctx, ST_ERR_ARG, "USEPOPINFO needs population data (st_data_desc.population)");
+    }
+    pop1 = data->population_h;
+    pflag.resize(N);
+    int unflagged = 0;
+    for (int i = 0; i < N; i++) {
+      pflag[i] = model->popflag_given ? data->popflags_h[i] : 1;
+      if (pflag[i] && (pop1[i] < 1 || pop1[i] > K)) pflag[i] = 0;
+      if (!pflag[i]) unflagged++;
+    }
+    h.alpha_n = unflagged;
+    if (model->inferalpha && !model->noadmix && unflagged == 0) h.inferalpha = 0;   // NOALPHA
+    initpop.resize(N);
+    for (int i = 0; i < N; i++) initpop[i] = (pop1[i] >= 1 && pop1[i] <= K) ? pop1[i] - 1 : -1;
+    popinfo_plan(N, L, &h.pi_lchunks, &h.pi_lchunk_len);
+  }
   h.computeprob = model->computeprob; h.pfrompopflagonly = model->pfrompopflagonly;
   h.ancestdist = model->ancestdist; h.numboxes = model->numboxes > 0 ? model->numboxes : 1;
   h.metrofreq = model->metrofreq; h.burnin = model->burnin;
@@ -653,6 +687,15 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       {&ctr, (size_t)kCtrCount * 4}, {&rep, 4}, {&err, 4}, {&chain, sizeof(ChainDev)},
       {&prefix, 16}};
   if (model->store_z) bufs.push_back({&Z, (size_t)N * 2 * L});
+  void *pi_flag = nullptr, *pi_pop = nullptr, *pi_init = nullptr, *pi_use = nullptr,
+       *pi_part = nullptr;
+  if (model->usepopinfo) {
+    const size_t KG = (size_t)K * (model->gensback + 1);
+    for (Buf b : std::vector<Buf>{{&pi_flag, (size_t)N * 4}, {&pi_pop, (size_t)N * 4},
+                                  {&pi_init, (size_t)N * 4}, {&pi_use, (size_t)N * KG * 8},
+                                  {&pi_part, (size_t)h.pi_lchunks * N * KG * 8}})
+      bufs.push_back(b);
+  }
   void* napart = nullptr;
   if (model->noadmix) {
     noadmix_plan(N, L, &h.na_lchunks, &h.na_lchunk_len);
@@ -692,6 +735,13 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   c->d_prefix = (int*)prefix;
   data->chains++;
   h.napart = (double*)napart;
+  if (model->usepopinfo) {
+    h.popflags = (int32_t*)pi_flag;
+    h.population = (const int32_t*)pi_pop;
+    h.initpop = (const int32_t*)pi_init;
+    h.usepop = (double*)pi_use;
+    h.pipart = (double*)pi_part;
+  }
   h.mala = model->mala ? 1 : 0;
   h.mala_target = (model->mala_target > 0 ? model->mala_target : 574) / 1000.0f;
   if (model->mala) {
@@ -748,6 +798,12 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     // adapted per individual during burn-in
     e0.assign(N, (float)(1.0 / sqrt(2.0 * L + 1.0)));
     cudaMemcpyAsync(h.mEps, e0.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+  }
+  if (h.usepopinfo) {
+    cudaMemcpyAsync(pi_flag, pflag.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(pi_pop, pop1.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(pi_init, initpop.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(pi_use, 0, (size_t)N * K * (h.gensback + 1) * 8, s);
   }
   int zero = 0;
   cudaMemcpyAsync(c->d_prefix, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
@@ -808,8 +864,18 @@ static bool alpha_moves(const ChainDev& h, int rep) {
   return !(h.noadmix && (rep >= h.admburnin || rep > h.burnin));
 }
 
+static int popinfo_step(st_chain* c) {
+  Bracket br(c->ctx, ST_K_IND);
+  c->ctx->launches++;   // two kernels
+  return cuda_check(c->ctx, launch_popinfo(c->h, c->d_chain, c->ctx->stream), "popinfo");
+}
+
 static int update_q_impl(st_chain* c, int stages) {
   const int rep = c->host_rep;
+  // USEPOPINFO individuals first (src/Updates/UpdateQ.c:734-736), then the
+  // others by the model's own update, which leaves the flagged ones alone
+  if (c->h.usepopinfo)
+    if (int rc = popinfo_step(c)) return rc;
   if (!alpha_moves(c->h, rep)) stages &= ~kIndAlpha;
   if (noadmix_q(c->h, rep)) {
     {
@@ -1006,6 +1072,7 @@ extern "C" size_t st_field_bytes(st_chain* c, int f) {
     case ST_F_REP: case ST_F_ERR: return 4;
     case ST_F_DIMS: return 32;
     case ST_F_MALA_EPS: return h.mala ? (size_t)h.N * 4 : 0;
+    case ST_F_USEPOPPROBS: return h.usepopinfo ? (size_t)h.N * h.K * (h.gensback + 1) * 8 : 0;
   }
   return 0;
 }
@@ -1034,6 +1101,7 @@ static void* field_ptr(st_chain* c, int f) {
     case ST_F_STATS: return h.stats;
     case ST_F_ERR: return h.err;
     case ST_F_MALA_EPS: return h.mEps;
+    case ST_F_USEPOPPROBS: return h.usepop;
   }
   return nullptr;
 }
@@ -1281,6 +1349,9 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
     Bracket br(ctx, ST_K_LOCUS);
     ST_CUDA(ctx, launch_locus(ll, b->G, kLocEps | kLocFst | kLocCollect, kBlockLoc));
   }
+  for (st_chain* c : b->chains)
+    if (c->h.usepopinfo)
+      if (int rc = popinfo_step(c)) return rc;
   if (metro) {
     {
       Bracket br(ctx, ST_K_IND);
@@ -1516,6 +1587,7 @@ std::vector<CkField> ckpt_fields(st_chain* c) {
   if (h.Z) f.push_back({h.Z, (size_t)h.N * 2 * h.L});
   if (h.AncestDist) f.push_back({h.AncestDist, NK * (size_t)h.numboxes * 4});
   if (h.mala) f.push_back({h.mEps, (size_t)h.N * 4});
+  if (h.usepopinfo) f.push_back({h.usepop, (size_t)h.N * h.K * (h.gensback + 1) * 8});
   return f;
 }
 

@@ -46,6 +46,9 @@ cudaError_t launch_lambda(const LaunchSet& ls, int block);
 // NOADMIX: per-individual population log likelihoods and the one-hot pick
 void noadmix_plan(int N, int L, int* lchunks, int* lchunk_len);
 cudaError_t launch_noadmix(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
+// USEPOPINFO: migrant-model Q of individuals with prior population information
+void popinfo_plan(int N, int L, int* lchunks, int* lchunk_len);
+cudaError_t launch_popinfo(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
 
 // CTA counts per chain for each launch kind (host-side mirror of the tiling).

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(kNaBlock) noadmix_ll_kernel(const ChainDev* __
   const ChainDev& ch = *chp;
   const int N = ch.N, L = ch.L, K = ch.K, A = ch.A;
   const int i = blockIdx.x * kNaBlock + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || (ch.usepopinfo && ch.popflags[i])) return;   // flagged: migrant model
   double ll[KC];
 #pragma unroll
   for (int k = 0; k < KC; k++) ll[k] = 0.0;
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kNaBlock) noadmix_pick_kernel(const ChainDev* 
   const ChainDev& ch = *chp;
   const int N = ch.N, K = ch.K;
   const int i = blockIdx.x * kNaBlock + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || (ch.usepopinfo && ch.popflags[i])) return;
   double p[kMaxPops];
   double mx = 0.0;
   for (int k = 0; k < K; k++) {

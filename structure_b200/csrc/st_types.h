@@ -15,7 +15,8 @@ constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
 // Philox stream ids (counter word 3 = id << 24).
 enum Stream : uint32_t {
   kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
-  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11, kSNoAdmix = 12
+  kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11, kSNoAdmix = 12,
+  kSPopInfo = 13
 };
 
 // Device error word bits.
@@ -97,6 +98,16 @@ struct ChainDev {
   int noadmix, admburnin;
   double* napart;                       // [na_lchunks][N][K]
   int na_lchunks, na_lchunk_len;
+  // USEPOPINFO: individuals flagged with a given population follow the
+  // migrant model; the others the usual updates
+  int usepopinfo, gensback;
+  double migrprior;
+  double alpha_n;                       // individuals the alpha update counts
+  const int32_t* population;            // [N] given population, 1-based
+  double* usepop;                       // [N][K][gensback+1] posterior sums
+  double* pipart;                       // [pi_lchunks][N][K][gensback+1]
+  int pi_lchunks, pi_lchunk_len;
+  const int32_t* initpop;               // [N] initial Z population or -1, or null
   // optional Langevin move on Q (Z summed out)
   int mala;
   float mala_target;

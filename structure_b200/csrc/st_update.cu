@@ -347,6 +347,10 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
   const uint32_t key = ch.key;
   const bool collect = (stages & kIndCollect) && (rep + 1 > ch.burnin);
   const size_t qi = (size_t)(ivalid ? i : 0) * K + (k < K ? k : 0);
+  // USEPOPINFO: flagged individuals keep the migrant-model Q drawn before this
+  // kernel in both the Gibbs and the Metropolis sweep and are left out of the
+  // alpha update (src/Updates/UpdateQ.c:247,407,727-729, UpdateAlpha.c:37)
+  const bool flagged = ch.usepopinfo && ivalid && ch.popflags[i];
   int errb = 0;
   if (threadIdx.x == 0) sHits = 0;
   __syncthreads();
@@ -369,7 +373,10 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
     const double e = kvalid ? exp(lg - M) : 0.0;
     const double S = group_sum(e, G);
     const double ls = M + log(S);
-    if (kvalid) {
+    if (kvalid && flagged && mode == kIndGibbs) {
+      qf = ch.Q[qi];
+      lqf = ch.logQ[qi];
+    } else if (kvalid) {
       const double lq = lg - ls;
       lqf = (float)lq;
       qf = (float)exp(lq);
@@ -382,7 +389,7 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
     if (ivalid)
       for (int g = 0; g < ch.ngroups; g++) ld += ch.ldpart[(size_t)g * N + i];
     bool acc = false;
-    if (ivalid) {
+    if (ivalid && !flagged) {
       const U4 w = philox_s((uint32_t)i, 0, (uint32_t)rep, kSQMA, key);
       acc = u01(w.x, w.y) < exp(ld);
     }
@@ -415,8 +422,9 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
     const int nwarps = blockDim.x >> 5;
     for (int idx = threadIdx.x; idx < nwarps * nslot; idx += blockDim.x) sA[idx] = 0.0;
     __syncthreads();
-    const double lq = kvalid ? (double)lqf : 0.0;
-    const double lc = kvalid ? (lq > kLogSqrtUnderflo ? lq : kLogSqrtUnderflo) : 0.0;
+    const bool counted = kvalid && !flagged;
+    const double lq = counted ? (double)lqf : 0.0;
+    const double lc = counted ? (lq > kLogSqrtUnderflo ? lq : kLogSqrtUnderflo) : 0.0;
     warp_slot_sums(lq, G, sA, nslot, k < K ? k : -1);
     double tsum = lc;
     for (int off = 1; off < 32; off <<= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, off);
@@ -455,15 +463,15 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
               double sumalphas = 0.0;
               for (int q = 0; q < K; q++) sumalphas += alpha[q];
               logprobdiff -= (alpha[pop] - 1.0) * sTot[pop] +
-                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(alpha[pop])) * N;
+                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(alpha[pop])) * ch.alpha_n;
               sumalphas += newalpha - alpha[pop];
               logprobdiff += (newalpha - 1.0) * sTot[pop] +
-                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(newalpha)) * N;
+                             (lanczos_lgamma_fast(sumalphas) - lanczos_lgamma_fast(newalpha)) * ch.alpha_n;
             } else {
               logprobdiff += (newalpha - 1.0) * T +
-                             (lanczos_lgamma_fast(K * newalpha) - K * lanczos_lgamma_fast(newalpha)) * N;
+                             (lanczos_lgamma_fast(K * newalpha) - K * lanczos_lgamma_fast(newalpha)) * ch.alpha_n;
               logprobdiff -= (alpha[pop] - 1.0) * T +
-                             (lanczos_lgamma_fast(K * alpha[pop]) - K * lanczos_lgamma_fast(alpha[pop])) * N;
+                             (lanczos_lgamma_fast(K * alpha[pop]) - K * lanczos_lgamma_fast(alpha[pop])) * ch.alpha_n;
             }
             ch.stats[kStAlphaLpd + pop] = logprobdiff;
             const double unifrv = rnd31(philox_s((uint32_t)pop, 1, (uint32_t)rep, kSAlpha, key));

@@ -180,6 +180,8 @@ zpass_u8_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, i
       } else if (mode == kZInit) {
         if (miss) { if (ch.Z && (flags & kZfStoreZ)) ch.Z[((size_t)i * 2 + line) * L + l] = kZMissing; continue; }
         z = (int)(((uint64_t)(wsel[line] >> 1) * (uint64_t)K) >> 31);
+        // USEPOPINFO: start at the given population (src/Init.c:74-117)
+        if (ch.initpop && ch.initpop[i] >= 0) z = ch.initpop[i];
       } else if (mode == kZRecount) {
         if (miss) continue;
         z = ch.Z[((size_t)i * 2 + line) * L + l];

@@ -250,6 +250,9 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
           } else if (MODE == kZInit) {
             z0 = (int)(((uint64_t)((h ? r4.z : r4.x) >> 1) * (uint64_t)K) >> 31);
             z1 = (int)(((uint64_t)((h ? r4.w : r4.y) >> 1) * (uint64_t)K) >> 31);
+            // USEPOPINFO: start at the given population (src/Init.c:74-117)
+            if (ch.initpop && valid && i0 + row < i1 && ch.initpop[i0 + row] >= 0)
+              z0 = z1 = ch.initpop[i0 + row];
           } else if (MODE == kZRecount) {
             if (valid && !miss) {
               const int ii = i0 + row;

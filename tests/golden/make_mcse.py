@@ -19,6 +19,9 @@ Runs:
   c1l -- the same data and run with lambda inferred (INFERLAMBDA=1).
   c1n -- the same data under the no-admixture model (NOADMIX=1, ADMBURNIN=500);
          24 chains (the variance of ln P(D) varies more between chains here).
+  c1p -- the same data with prior population information for half of the
+         individuals (USEPOPINFO=1, populations = the generating Q's largest
+         component, GENSBACK=2, MIGRPRIOR=0.05).
   c2s -- N=200, L=1,000 biallelic SNPs, K=3 F model (F = .10, .20, .30), 3%
          genotypes missing; alpha and F inferred; 2,000 burn-in + 4,000 sweeps;
          8 chains.
@@ -54,6 +57,12 @@ def runs():
                     K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
                                     alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
                                     noadmix=1, admburnin=500), chains=24),
+        "c1p": dict(geno=c1["geno"], raw=c1["geno_raw"], numalleles=c1["numalleles"], Q=c1["Q"],
+                    K=3, model=dict(burnin=1000, numreps=10000, freqscorr=0, inferalpha=1,
+                                    alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
+                                    usepopinfo=1, popflag=1, gensback=2, migrprior=0.05),
+                    population=(c1["Q"].argmax(1) + 1).astype(np.int32),
+                    popflags=(np.random.default_rng(5).random(200) < 0.5).astype(np.int32)),
         "c2s": dict(geno=c2["geno"], raw=c2["geno"], numalleles=c2["numalleles"], Q=c2["Q"],
                     K=3, model=dict(burnin=2000, numreps=4000, freqscorr=1, inferalpha=1,
                                     alpha=1.0, alphapropsd=0.025, metrofreq=10, lambda_=1.0,
@@ -62,19 +71,23 @@ def runs():
 
 
 def _chain(job):
-    name, r, raw, K, model = job
+    name, r, raw, K, model, pf, pp = job
     from oracle.oracle import RefLib, ref_model
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)                     # the reference prints to stdout
     ref = RefLib()
     N, _, L = raw.shape
     m = ref_model(N=N, L=L, K=K, maxalleles=2, **model)
-    ch = ref.chain_new(m, raw, seed=1000 * (2 if name == "c2s" else 1) + r)
+    ch = ref.chain_new(m, raw, popflags=pf, population=pp,
+                       seed=1000 * (2 if name == "c2s" else 1) + r)
     ref.lib.stref_chain_sweeps(ch, model["burnin"] + model["numreps"])
-    v = ref.chain_view(ch, N, L, K)
-    return dict(sumlikes=v["sumlikes"], sumsqlikes=v["sumsqlikes"], QSum=v["QSum"],
-                sumAlpha=v["sumAlpha"], FstSum=v["FstSum"], Alpha=v["Alpha"], Fst=v["Fst"],
-                sumlambda=v["sumlambda"])
+    v = ref.chain_view(ch, N, L, K, model.get("gensback", 2))
+    out = dict(sumlikes=v["sumlikes"], sumsqlikes=v["sumsqlikes"], QSum=v["QSum"],
+               sumAlpha=v["sumAlpha"], FstSum=v["FstSum"], Alpha=v["Alpha"], Fst=v["Fst"],
+               sumlambda=v["sumlambda"])
+    if v["usepop"] is not None:
+        out["usepop"] = v["usepop"]
+    return out
 
 
 def main():
@@ -84,13 +97,16 @@ def main():
         if only and name not in only:
             continue
         nch = run.get("chains", CHAINS)
-        jobs = [(name, r, run["raw"], run["K"], run["model"]) for r in range(nch)]
+        jobs = [(name, r, run["raw"], run["K"], run["model"], run.get("popflags"),
+                 run.get("population")) for r in range(nch)]
         with ctx.Pool(min(nch, os.cpu_count() or 1)) as pool:
             res = pool.map(_chain, jobs)
         out = {k: np.array([x[k] for x in res]) for k in res[0]}
         np.savez_compressed(os.path.join(HERE, f"mcse_{name}.npz"),
                             geno=run["geno"].astype(np.int8), numalleles=run["numalleles"],
                             Qtrue=run["Q"], K=run["K"], nlike=run["model"]["numreps"],
+                            **({"popflags": run["popflags"], "population": run["population"]}
+                               if "population" in run else {}),
                             **{f"model_{k}": v for k, v in run["model"].items()}, **out)
         print(name, "lnL means", out["sumlikes"] / run["model"]["numreps"])
 

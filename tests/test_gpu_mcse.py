@@ -61,18 +61,24 @@ def _run_device(ctx, z, model, mala=0):
     geno = z["geno"].astype(np.int32)
     K = int(z["K"])
     R = len(z["sumlikes"])
-    data = api.Data(ctx, z["numalleles"], geno=geno)
+    data = api.Data(ctx, z["numalleles"], geno=geno,
+                    popflags=z["popflags"] if "popflags" in z.files else None,
+                    population=z["population"] if "population" in z.files else None)
     mk = dict(maxpops=K, burnin=model["burnin"], numreps=model["numreps"],
               freqscorr=model["freqscorr"], inferalpha=model["inferalpha"], alpha=model["alpha"],
               alphapropsd=model["alphapropsd"], metrofreq=model["metrofreq"],
               lambda_=model["lambda_"], mala=mala)
-    for k in ("fpriormean", "fpriorsd", "inferlambda", "noadmix", "admburnin"):
+    for k in ("fpriormean", "fpriorsd", "inferlambda", "noadmix", "admburnin", "usepopinfo",
+              "gensback", "migrprior"):
         if k in model:
             mk[k] = model[k]
+    if "popflag" in model:
+        mk["popflag_given"] = model["popflag"]
     chains = [api.Chain(ctx, data, api.model_defaults(**mk), 77000 + r) for r in range(R)]
     b = api.Batch(ctx, chains)
     b.sweep(model["burnin"] + model["numreps"])
-    res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[], sumlambda=[])
+    res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[], sumlambda=[],
+               usepop=[])
     for c in chains:
         assert c.sync() == 0
         if mala:
@@ -86,6 +92,8 @@ def _run_device(ctx, z, model, mala=0):
         res["sumAlpha"].append(c.get(api.F_SUMALPHA))
         res["FstSum"].append(c.get(api.F_FSTSUM))
         res["sumlambda"].append(c.get(api.F_SUMLAMBDA))
+        if model.get("usepopinfo"):
+            res["usepop"].append(c.get(api.F_USEPOPPROBS))
     b.close()
     for c in chains:
         c.close()
@@ -93,7 +101,8 @@ def _run_device(ctx, z, model, mala=0):
     return {k: np.array(v) for k, v in res.items()}
 
 
-@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c1n", 0), ("c2s", 0), ("c2s", 1)])
+@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c1n", 0), ("c1p", 0), ("c2s", 0),
+                                       ("c2s", 1)])
 def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
     """mala=1: the same chains with the Langevin move on Q added to every
     sweep still sample the reference's posterior."""
@@ -119,6 +128,16 @@ def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
         ld, lr = dev["sumlambda"][:, 0] / n, z["sumlambda"][:, 0] / n
         print("  lambda   ", ld.mean(), lr.mean(), "z", float(_z(ld, lr)))
         assert _z(ld, lr) <= 5.0, (ld.mean(), lr.mean())
+    if model.get("usepopinfo"):
+        # posterior probability of the given population (UsePopProbs, gen 0)
+        # of the flagged individuals, summed over the collecting sweeps
+        f = z["popflags"].astype(bool)
+        hp = z["population"][f] - 1
+        ud = dev["usepop"][..., 0][:, f][:, np.arange(f.sum()), hp] / n
+        ur = z["usepop"][..., 0][:, f][:, np.arange(f.sum()), hp] / n
+        zu = _z(ud, ur, floor=0.002)
+        print("  P(home)  ", ud.mean(), ur.mean(), "max z", zu.max())
+        assert zu.max() <= 6.0
     zq = _z(sd["Q"], sr["Q"], floor=0.002)
     assert zq.max() <= 6.0, zq.max()
     assert np.abs(sd["Q"].mean(0) - sr["Q"].mean(0)).mean() <= 0.01

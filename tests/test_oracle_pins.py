@@ -401,3 +401,39 @@ def test_update_q_noadmix_matches_reference(orc, ref):
     np.testing.assert_array_equal(Qr.argmax(1), pick)
     np.testing.assert_array_equal(Qo, Qr.astype(np.float32))
     assert len(set(pick)) > 1
+
+
+@pytest.mark.parametrize("gensback,migr", [(2, 0.05), (0, 0.3), (3, 0.01)])
+def test_update_q_withpops_matches_reference(orc, ref, gensback, migr):
+    """UpdateQWithPops (USEPOPINFO migrant model) fed the oracle's rand()
+    words: same Q for every flagged individual, same posterior sums."""
+    from structure_b200 import synth
+    from oracle.oracle import S_POPINFO
+    d = synth.microsat(N=40, L=60, K=3, seed=33)
+    geno, na = d["geno"], d["numalleles"].astype(np.int32)
+    N, _, L = geno.shape
+    K, A = 3, int(na.max())
+    rng = np.random.default_rng(gensback)
+    P = np.zeros((L, K, A), np.float32)
+    for l in range(L):
+        P[l, :, :na[l]] = rng.dirichlet(np.full(na[l], 0.6), K)
+    pop = rng.integers(1, K + 1, N).astype(np.int32)
+    flags = (rng.random(N) < 0.6).astype(np.int32)
+    Q0 = rng.dirichlet(np.ones(K), N).astype(np.float32)
+    key, rep, burnin = 0x7070, 12, 10
+    Qo, _, upo = orc.update_q_withpops(geno, P, pop, flags, gensback, migr, key, rep, burnin,
+                                       Q0, np.log(Q0))
+    words = [int(orc.stream(i, 0, rep, S_POPINFO, key)[0]) >> 1 for i in range(N) if flags[i]]
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, usepopinfo=1, gensback=gensback,
+                    migrprior=migr, burnin=burnin, popflag=1)
+    Qr = Q0.astype(np.float64).copy()
+    up = np.zeros(N * K * (gensback + 1))
+    ref.rand_queue(words)
+    ref.lib.UpdateQWithPops(geno.copy(), Qr, P.astype(np.float64), None, np.ones(K), rep,
+                            ref.individuals_pop(N, flags, pop), up, None)
+    ref.rand_queue(None)
+    f = flags.astype(bool)
+    np.testing.assert_array_equal(Qo[f], Qr[f].astype(np.float32))
+    np.testing.assert_array_equal(Qo[~f], Q0[~f])
+    np.testing.assert_allclose(upo.reshape(-1), up, rtol=1e-9, atol=1e-12)
+    assert (Qr[f] < 1).any() or gensback == 0
