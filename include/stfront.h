@@ -65,6 +65,20 @@ int stf_geno(const stf_run *r, int32_t *geno, int32_t *numalleles, int32_t *tran
 int stf_individuals(const stf_run *r, int32_t *pop, int32_t *popflag, int32_t *location,
                     int32_t *phenotype, char *labels);
 
+/* USEPOPINFO=1: the prior-population checks of src/Init.c:15-70
+ * CheckPopPriors, after stf_read_data and before the popflags are taken
+ * for the engine: everyone flagged when the file has no POPFLAG column,
+ * flags dropped for populations outside 1..MAXPOPS (their number in
+ * *dropped, may be NULL), INFERALPHA set to 0 when nobody is left without
+ * prior information (NOALPHA).  STF_ERR_PARAMS for a MIGRPRIOR outside
+ * [0, 1] or no POPDATA.  A no-op with USEPOPINFO=0.                        */
+int stf_check_pop_priors(stf_run *r, int32_t *dropped);
+/* USEPOPINFO=1: the UsePopProbs sums [N][MAXPOPS][GENSBACK+1] of the run
+ * (copied), printed for flagged individuals in place of their Q
+ * (src/output.c:800-829 PrintGeogQ).  Required before stf_write_results
+ * with USEPOPINFO=1.                                                       */
+int stf_set_usepopprobs(stf_run *r, const double *usepop);
+
 /* Writes OUTFILE_f (and OUTFILE_q when PRINTQHAT=1) from the run's sums, in
  * the reference layouts: QSum [N][K], PSum [L][K][MAXALLELES], SumEpsilon
  * [L][MAXALLELES] (may be NULL without FREQSCORR), FstSum [K], sumAlpha [K],

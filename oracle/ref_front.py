@@ -11,7 +11,8 @@ process globals and exits on errors, so each scenario runs in its own process:
     python oracle/ref_front.py <workdir> <spec.json>
 
 spec: {"argv": [...], "read_data": bool, "sums": "<npz in workdir>" or null,
-       "rep": int}.  The working directory is <workdir> (the reference opens
+       "rep": int}; with USEPOPINFO=1 the sums carry "usepop" [N][K][GENSBACK+1]
+and CheckPopPriors (src/Init.c:15-70) runs before OutPutResults.  The working directory is <workdir> (the reference opens
 its files relative to it).  Results go to <workdir>/ref_out.json and
 <workdir>/ref_data.npz; OutPutResults writes OUTFILE_f (and OUTFILE_q).
 """
@@ -90,6 +91,13 @@ def main(workdir, specpath):
         if spec.get("sums"):
             z = np.load(os.path.join(workdir, spec["sums"]))
             K = g("MAXPOPS").value
+            usepop = None
+            if g("USEPOPINFO").value:
+                # src/Init.c:417: the prior-population checks run before the
+                # chain and decide which individuals print the migrant model
+                lib.CheckPopPriors.argtypes = [C.c_void_p]
+                lib.CheckPopPriors(inds)
+                usepop = np.ascontiguousarray(z["usepop"], np.float64)
             d = lambda a: np.ascontiguousarray(a, np.float64).ctypes.data_as(C.c_void_p)
             keep = {k: np.ascontiguousarray(z[k], np.float64) for k in
                     ("QSum", "PSum", "SumEps", "FstSum", "sumAlpha", "sumlambda")}
@@ -105,7 +113,8 @@ def main(workdir, specpath):
                                           C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                           C.c_void_p, C.c_int, C.c_void_p]
             lib.OutPutResults(geno, int(spec["rep"]), 1, inds, P(keep["PSum"]), P(keep["QSum"]),
-                              P(keep["FstSum"]), P(ad) if ad is not None else None, None,
+                              P(keep["FstSum"]), P(ad) if ad is not None else None,
+                              P(usepop) if usepop is not None else None,
                               float(z["sumlikes"]), float(z["sumsqlikes"]), P(keep["sumAlpha"]),
                               P(zeros["sumR"]), P(zeros["varR"]), na, tr, 1, names,
                               P(zeros["R"]), P(keep["SumEps"]), P(zeros["lambda"]),

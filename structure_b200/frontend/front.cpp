@@ -187,6 +187,9 @@ struct stf_run {
   std::vector<int32_t> geno, numalleles, translation;
   std::vector<std::string> markername;
   std::vector<Individual> ind;
+  // USEPOPINFO (stf_check_pop_priors / stf_set_usepopprobs)
+  bool noalpha = false;
+  std::vector<double> usepop;   // [N][MAXPOPS][GENSBACK+1]
 };
 
 namespace {
@@ -595,6 +598,51 @@ extern "C" int stf_individuals(const stf_run* r, int32_t* pop, int32_t* popflag,
   return STF_OK;
 }
 
+// The prior-population checks of src/Init.c:15-70 CheckPopPriors: MIGRPRIOR
+// in [0, 1] and POPDATA present, every individual flagged when the file has
+// no POPFLAG column, flags dropped where the population is outside
+// 1..MAXPOPS, and alpha switched off (INFERALPHA=0) when no individual is
+// left without prior information in the admixture model.
+extern "C" int stf_check_pop_priors(stf_run* r, int32_t* dropped) {
+  if (!r || !r->have_data) return STF_ERR_ARG;
+  if (dropped) *dropped = 0;
+  if (!I(r, "USEPOPINFO")) return STF_OK;
+  const double migr = D(r, "MIGRPRIOR");
+  if (migr < 0.0 || migr > 1.0)
+    return fail(r, STF_ERR_PARAMS,
+                "MIGRPRIOR (which is currently set to %1.3f) must be in the range [0.0, 1.0]",
+                migr);
+  if (!I(r, "POPDATA"))
+    return fail(r, STF_ERR_PARAMS, "Can't apply USEPOPINFO because no POPDATA in input data file");
+  const int K = I(r, "MAXPOPS");
+  if (!I(r, "POPFLAG"))
+    for (Individual& d : r->ind) d.popflag = 1;
+  int nopop = 0;
+  for (Individual& d : r->ind) {
+    if (d.popflag && (d.population < 1 || d.population > K)) {
+      d.popflag = 0;
+      if (dropped) ++*dropped;
+    }
+    if (d.popflag == 0) nopop++;
+  }
+  if (I(r, "INFERALPHA") && !I(r, "NOADMIX") && nopop == 0) {
+    r->noalpha = true;
+    r->num["INFERALPHA"] = 0;
+  }
+  return STF_OK;
+}
+
+extern "C" int stf_set_usepopprobs(stf_run* r, const double* usepop) {
+  if (!r || !r->have_data) return STF_ERR_ARG;
+  if (!usepop) {
+    r->usepop.clear();
+    return STF_OK;
+  }
+  const size_t n = (size_t)r->N * I(r, "MAXPOPS") * (I(r, "GENSBACK") + 1);
+  r->usepop.assign(usepop, usepop + n);
+  return STF_OK;
+}
+
 // ===========================================================================
 // results (src/output.c:1354-1423 and the printers it calls)
 // ===========================================================================
@@ -791,7 +839,7 @@ void sums(const stf_run* r, Out& o, const Sums& s) {
       o.f("Mean value of ln likelihood = %1.1f\n", s.sumlikes / reps);
     }
   }
-  if (!I(r, "NOADMIX") && K > 1) {
+  if (!I(r, "NOADMIX") && !r->noalpha && K > 1) {
     if (I(r, "POPALPHAS")) {
       o.f("\n");
       for (int k = 0; k < K; k++)
@@ -860,19 +908,46 @@ void ancest_interval(const stf_run* r, Out& o, const int32_t* AD, int i, int rep
   }
 }
 
+// Posterior of the migrant model for an individual with prior information:
+// P(from the given population) | for every other population, P(migrant
+// ancestry from it) for 0..GENSBACK generations back, with one to three
+// stars when P(given population) is below 0.5, 0.3, 0.1
+// (src/output.c:800-829 PrintGeogQ).
+void geog_q(const stf_run* r, Out& o, int i, int reps) {
+  const int K = I(r, "MAXPOPS"), G = I(r, "GENSBACK") + 1;
+  const int home = r->ind[i].population - 1;
+  const double* u = r->usepop.data() + (size_t)i * K * G;
+  const double ph = u[(size_t)home * G] / reps;
+  o.f("%1.3f | ", ph);
+  for (int k = 0; k < K; k++)
+    if (k != home) {
+      o.f("Pop %d: ", k + 1);
+      for (int g = 0; g < G; g++) o.f("%1.3f ", u[(size_t)k * G + g] / reps);
+      o.f(" | ");
+    }
+  o.f(" ");
+  if (ph < 0.1) o.f("*");
+  if (ph < 0.3) o.f("*");
+  if (ph < 0.5) o.f("*");
+}
+
 void ancestry(const stf_run* r, Out& o, const Sums& s) {
   const int K = I(r, "MAXPOPS"), reps = s.rep - I(r, "BURNIN");
   const bool label = I(r, "LABEL") == 1, popdata = I(r, "POPDATA") == 1;
+  const bool usepop = I(r, "USEPOPINFO") != 0;
   o.f("\n");
   o.f("Inferred ancestry of individuals:\n");
+  if (usepop) o.f("Probability of being from assumed population | prob of other pops\n");
   o.f("    ");
   if (label) o.f(" %8s", "Label");
   o.f(" (%%Miss) ");
   if (popdata) o.f("Pop");
-  o.f(":  ");
-  o.f("Inferred clusters");
-  if (I(r, "ANCESTDIST"))
-    o.f(" (and %d%c probability intervals)", (int)(100.0 * D(r, "ANCESTPINT")), '%');
+  if (!usepop) {
+    o.f(":  ");
+    o.f("Inferred clusters");
+    if (I(r, "ANCESTDIST"))
+      o.f(" (and %d%c probability intervals)", (int)(100.0 * D(r, "ANCESTPINT")), '%');
+  }
   o.f("\n");
   for (int i = 0; i < r->N; i++) {
     const int miss = (100 * missing_ind(r, i)) / (r->LINES * r->L);
@@ -883,8 +958,12 @@ void ancestry(const stf_run* r, Out& o, const Sums& s) {
     o.f("  ");
     if (popdata) o.f("%2d ", r->ind[i].population);
     o.f(":  ");
-    for (int k = 0; k < K; k++) o.f("%1.3f ", s.QSum[(size_t)i * K + k] / reps);
-    if (I(r, "ANCESTDIST") && s.AncestDist) ancest_interval(r, o, s.AncestDist, i, s.rep);
+    if (usepop && r->ind[i].popflag) {
+      geog_q(r, o, i, reps);
+    } else {
+      for (int k = 0; k < K; k++) o.f("%1.3f ", s.QSum[(size_t)i * K + k] / reps);
+      if (I(r, "ANCESTDIST") && s.AncestDist) ancest_interval(r, o, s.AncestDist, i, s.rep);
+    }
     o.f("\n");
   }
 }
@@ -984,6 +1063,8 @@ extern "C" int stf_write_results(stf_run* r, int rep, const double* QSum, const 
                                  double sumsqlikes) {
   if (!r || !r->have_data || !QSum || !PSum || !FstSum || !sumAlpha) return STF_ERR_ARG;
   if (rep - I(r, "BURNIN") < 1) return fail(r, STF_ERR_ARG, "no collected sweeps to report");
+  if (I(r, "USEPOPINFO") && r->usepop.empty())
+    return fail(r, STF_ERR_ARG, "USEPOPINFO=1: give the UsePopProbs sums (stf_set_usepopprobs)");
   const Sums s{rep, QSum, PSum, SumEpsilon, FstSum, sumAlpha, sumlambda, AncestDist, sumlikes,
                sumsqlikes};
   Out o;

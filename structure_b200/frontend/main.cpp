@@ -5,9 +5,11 @@
 // through libstgpu (include/stgpu.h), prints progress every UPDATEFREQ
 // sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
 //
-// Options the GPU path does not implement (LINKAGE, USEPOPINFO, LOCPRIOR,
-// RECESSIVEALLELES, PLOIDY other than 2) stop the
-// program with a message instead of running a different model.
+// USEPOPINFO=1 runs the migrant model for individuals with prior population
+// information and prints its posterior in OUTFILE_f (src/output.c:800-829).
+// Options the GPU path does not implement (LINKAGE, LOCPRIOR,
+// RECESSIVEALLELES, PLOIDY other than 2) stop the program with a message
+// instead of running a different model.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -42,7 +44,7 @@ int die(const char* what, const char* msg) {
 int main(int argc, char** argv) {
   stf_run* r = nullptr;
   if (stf_open(argc, argv, &r) != STF_OK) return die("parameters", stf_last_error(r));
-  const char* unsupported[] = {"LINKAGE", "USEPOPINFO", "LOCPRIOR", "RECESSIVEALLELES"};
+  const char* unsupported[] = {"LINKAGE", "LOCPRIOR", "RECESSIVEALLELES"};
   for (const char* k : unsupported)
     if (pi(r, k)) {
       fprintf(stderr, "%s=1 is not available on the GPU path.\n", k);
@@ -61,8 +63,16 @@ int main(int argc, char** argv) {
   stf_geno(r, geno.data(), na.data(), tr.data());
   for (int32_t& g : geno)
     if (g < 0) g = -9;   // the engine's missing code
-  std::vector<int32_t> popflag(N);
-  stf_individuals(r, nullptr, popflag.data(), nullptr, nullptr, nullptr);
+  std::vector<int32_t> popflag(N), pop(N), flag_before(N);
+  stf_individuals(r, nullptr, flag_before.data(), nullptr, nullptr, nullptr);
+  if (stf_check_pop_priors(r, nullptr) != STF_OK) return die("parameters", stf_last_error(r));
+  stf_individuals(r, pop.data(), popflag.data(), nullptr, nullptr, nullptr);
+  if (pi(r, "USEPOPINFO"))
+    for (int i = 0; i < N; i++)
+      if (!popflag[i] && (flag_before[i] || !pi(r, "POPFLAG")))
+        printf("Warning: population prior for individual %d is %d, which is not\n"
+               "  in the range 1..%d.  Population prior for this individual will\n"
+               "  be ignored\n", i + 1, pop[i], K);
   int amin = 1 << 30, amax = 0;
   double asum = 0.0;
   for (int v : na) {
@@ -95,6 +105,7 @@ int main(int argc, char** argv) {
   d.geno = geno.data();
   d.num_alleles = na.data();
   d.popflags = popflag.data();
+  d.population = pop.data();
   rc = st_data_upload(ctx, &d, &data);
   if (rc != ST_OK) return die("GPU", st_last_error(ctx));
   st_model m;
@@ -124,6 +135,10 @@ int main(int argc, char** argv) {
   m.lambda = pd(r, "LAMBDA");
   m.fpriormean = pd(r, "FPRIORMEAN");
   m.fpriorsd = pd(r, "FPRIORSD");
+  m.usepopinfo = pi(r, "USEPOPINFO");
+  m.popflag_given = 1;   // the flags above already hold CheckPopPriors' result
+  m.gensback = pi(r, "GENSBACK");
+  m.migrprior = pd(r, "MIGRPRIOR");
   rc = st_chain_create(ctx, data, &m, (uint64_t)seed, &c);
   if (rc != ST_OK) return die("GPU", st_last_error(ctx));
 
@@ -169,6 +184,11 @@ int main(int argc, char** argv) {
   if (m.ancestdist) {
     AD.resize(NK * (size_t)m.numboxes);
     st_get_state(c, ST_F_ANCESTDIST, AD.data(), AD.size() * 4);
+  }
+  if (m.usepopinfo) {
+    std::vector<double> up(NK * (size_t)(m.gensback + 1));
+    st_get_state(c, ST_F_USEPOPPROBS, up.data(), up.size() * 8);
+    stf_set_usepopprobs(r, up.data());
   }
   printf("\nMCMC completed\n");
   rc = stf_write_results(r, total, QSum.data(), PSum.data(), SumEps.data(), FstSum.data(),

@@ -48,6 +48,8 @@ def _front():
     L.stf_individuals.argtypes = [vp, vp, vp, vp, vp, vp]
     L.stf_write_results.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.c_double,
                                     C.c_double]
+    L.stf_check_pop_priors.argtypes = [vp, vp]
+    L.stf_set_usepopprobs.argtypes = [vp, vp]
     L.stf_close.argtypes = [vp]
     return L
 
@@ -97,8 +99,17 @@ class Ours:
         return dict(A=A, geno=geno, numalleles=na, translation=tr, pop=pop, popflag=pf,
                     labels=labels)
 
+    def check_pop_priors(self):
+        n = np.zeros(1, np.int32)
+        rc = self.L.stf_check_pop_priors(self.h, n.ctypes.data)
+        assert rc == 0, self.L.stf_last_error(self.h)
+        return int(n[0])
+
     def write(self, rep, z):
         f = lambda a: np.ascontiguousarray(a, np.float64)
+        if "usepop" in z:
+            self._up = f(z["usepop"])
+            assert self.L.stf_set_usepopprobs(self.h, self._up.ctypes.data) == 0
         self._keep = {k: f(z[k]) for k in ("QSum", "PSum", "SumEps", "FstSum", "sumAlpha",
                                            "sumlambda")}
         ad = np.ascontiguousarray(z["AncestDist"], np.int32) if "AncestDist" in z else None
@@ -157,9 +168,11 @@ Basic Program Parameters
 """
 
 EXTRA_TMPL = """EXTRA PARAMS (written by the test)
-#define NOADMIX     0 // (B)
+#define NOADMIX     {noadmix} // (B)
 #define LINKAGE     0 // (B)
-#define USEPOPINFO  0 // (B)
+#define USEPOPINFO  {usepopinfo} // (B)
+#define MIGRPRIOR {migrprior} // (d)
+#define GENSBACK  {gensback} // (int)
 #define LOCPRIOR    0 //(B)
 #define FREQSCORR   {freqscorr} // (B)
 #define ONEFST      {onefst} // (B)
@@ -191,7 +204,8 @@ def _scenario(d, **kw):
     p = dict(K=3, burnin=100, numreps=400, infile="data file.str", outfile="results", N=40, L=25,
              missing=-9, onerow=0, label=1, popdata=1, popflag=0, extracols=0, markernames=1,
              mapdist=0, freqscorr=1, onefst=0, popalphas=0, updatefreq=0, printqhat=0,
-             ancestdist=0, numboxes=100, seed=4242)
+             ancestdist=0, numboxes=100, seed=4242, noadmix=0, usepopinfo=0, migrprior=0.05,
+             gensback=2)
     p.update(kw)
     with open(os.path.join(d, "mainparams"), "w") as f:
         f.write(MAIN_TMPL.format(**p))
@@ -236,6 +250,10 @@ def _random_sums(p, A, seed=1):
     z = dict(QSum=Q, PSum=P, SumEps=rng.random((L, A)) * reps, FstSum=rng.random(K) * 0.3 * reps,
              sumAlpha=rng.random(K) * reps, sumlambda=np.ones(K) * reps,
              sumlikes=-1234.56 * reps, sumsqlikes=1234.56 ** 2 * reps + 50.0 * (reps - 1))
+    if p["usepopinfo"]:
+        u = rng.dirichlet(np.ones(K * (p["gensback"] + 1)), N) * reps
+        z["usepop"] = u.reshape(N, K, p["gensback"] + 1)
+        z["usepop"][:5, :, 0] = 0.0    # low posterior of the given population: stars
     if p["ancestdist"]:
         ad = np.zeros((N, K, p["numboxes"]), np.int32)
         for i in range(N):
@@ -311,18 +329,28 @@ def test_data_matches_reference(tmp_path, layout):
 
 
 OUTPUTS = [dict(), dict(freqscorr=0, popalphas=1), dict(onefst=1, printqhat=1),
-           dict(ancestdist=1, label=0), dict(popdata=0, markernames=0, K=2)]
+           dict(ancestdist=1, label=0), dict(popdata=0, markernames=0, K=2),
+           dict(usepopinfo=1, popflag=1, migrprior=0.1), dict(usepopinfo=1, gensback=1),
+           dict(usepopinfo=1, K=4, ancestdist=1), dict(noadmix=1)]
 
 
 @needs_ref
 @pytest.mark.parametrize("opts", OUTPUTS, ids=["f", "indep-popalphas", "onefst-qhat", "ancest",
-                                                "nopop"])
+                                                "nopop", "usepop-flags", "usepop-all",
+                                                "usepop-noalpha", "noadmix"])
 def test_results_file_matches_reference_byte_for_byte(tmp_path, opts):
     d = str(tmp_path)
     p = _scenario(d, **opts)
     argv = ["structure", "-K", str(p["K"])]
     ours = Ours(d, argv)
     o = ours.data()
+    dropped = ours.check_pop_priors()
+    if p["usepopinfo"]:
+        # populations are 1..4 in the file: 4 is outside 1..K for K=3
+        flagged = (o["popflag"] == 1) if p["popflag"] else np.ones(p["N"], bool)
+        assert dropped == int((flagged & (o["pop"] > p["K"])).sum())
+        if p["K"] == 4 and not p["popflag"]:
+            assert ours.int("INFERALPHA") == 0      # NOALPHA: everybody has prior info
     z = _random_sums(p, o["A"])
     np.savez(os.path.join(d, "sums.npz"), **z)
     rep = p["burnin"] + p["numreps"]

@@ -29,9 +29,11 @@ def _snp_data(d, p):
         f.write("\n".join(rows) + "\n")
 
 
-@pytest.mark.parametrize("kind", ["microsat", "snp"])
+@pytest.mark.parametrize("kind", ["microsat", "snp", "usepopinfo"])
 def test_cli_run_writes_results(tmp_path, kind):
     d = str(tmp_path)
+    if kind == "usepopinfo":
+        return _usepopinfo_run(d)
     if kind == "microsat":
         p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200)
     else:
@@ -58,3 +60,33 @@ def test_cli_run_writes_results(tmp_path, kind):
     assert len(fst) == 3 and all(0 < f < 1 for f in fst)
     assert "SEED=99" in text
     assert open(os.path.join(d, "seed.txt")).read().strip() == "99"
+
+
+def _usepopinfo_run(d):
+    """USEPOPINFO=1 with a POPFLAG column: individuals i % 2 == 1 carry prior
+    information; population 4 is outside 1..3, so those lose it with a
+    warning.  Flagged rows print the migrant-model posterior, the others Q."""
+    p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200, usepopinfo=1,
+                  popflag=1)
+    r = subprocess.run([CLI, "-D", "7"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    pops = [1 + i % 4 for i in range(p["N"])]
+    flagged = [i % 2 == 1 and pops[i] <= 3 for i in range(p["N"])]
+    assert r.stdout.count("Warning: population prior for individual") == \
+        sum(i % 2 == 1 and pops[i] == 4 for i in range(p["N"]))
+    text = open(os.path.join(d, "results_f")).read()
+    assert "USEPOPINFO turned on" in text and "MIGRPRIOR = 0.0500" in text
+    assert "Probability of being from assumed population | prob of other pops" in text
+    rows = re.findall(r"^\s*(\d+)\s+\S+\s+\(\s*\d+\)\s+\d+ :  (.*)$", text, re.M)
+    assert len(rows) == p["N"]
+    for idx, body in rows:
+        i = int(idx) - 1
+        if flagged[i]:
+            ph = float(body.split("|")[0])
+            groups = re.findall(r"Pop \d+: ((?:[0-9.]+ ){3})", body)
+            others = [float(v) for g in groups for v in g.split()]
+            assert len(others) == 2 * 3
+            assert ph + sum(others) == pytest.approx(1.0, abs=0.01)
+        else:
+            q = [float(x) for x in body.split()[:3]]
+            assert sum(q) == pytest.approx(1.0, abs=0.003)
