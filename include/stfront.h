@@ -79,6 +79,15 @@ int stf_check_pop_priors(stf_run *r, int32_t *dropped);
  * with USEPOPINFO=1.                                                       */
 int stf_set_usepopprobs(stf_run *r, const double *usepop);
 
+/* LOCPRIOR=1: the number of locations (distinct location ids of the data,
+ * numbered in increasing order as src/Util.c:237-275 GetNumLocations does),
+ * and the LocPrior sums of the run, n = 1 with admixture or
+ * 1 + MAXPOPS * (locations + 1) without (r, nu, gamma; st_get_state
+ * ST_F_SUMLOCPRIOR).  Required before stf_write_results with LOCPRIOR=1,
+ * where sumAlpha then holds MAXPOPS * (locations + 1) values with admixture. */
+int stf_num_locations(const stf_run *r);
+int stf_set_locprior_sums(stf_run *r, const double *sums, size_t n);
+
 /* Writes OUTFILE_f (and OUTFILE_q when PRINTQHAT=1) from the run's sums, in
  * the reference layouts: QSum [N][K], PSum [L][K][MAXALLELES], SumEpsilon
  * [L][MAXALLELES] (may be NULL without FREQSCORR), FstSum [K], sumAlpha [K],

@@ -104,6 +104,10 @@ typedef struct st_data_desc {
     const int32_t *num_alleles;/* [num_loci] NumAlleles */
     const int32_t *popflags;   /* [num_inds] Individual[].PopFlag or NULL */
     const int32_t *population; /* [num_inds] Individual[].Population (POPDATA) or NULL */
+    const int32_t *location;   /* [num_inds] Individual[].Location (LOCDATA, or the
+                                * population with LOCISPOP), >= 0, or NULL; locations
+                                * are numbered 0.. in increasing order of these ids
+                                * (src/Util.c:237-275 GetNumLocations)               */
 } st_data_desc;
 
 int st_data_upload(st_ctx *ctx, const st_data_desc *desc, st_data **out);
@@ -119,7 +123,7 @@ typedef struct st_model {
     int32_t noadmix;           /* NOADMIX: each individual from one population */
     int32_t linkage;           /* LINKAGE: must be 0 */
     int32_t usepopinfo;        /* USEPOPINFO (needs population data) */
-    int32_t locprior;          /* LOCPRIOR: must be 0 */
+    int32_t locprior;          /* LOCPRIOR (needs location data; with NOADMIX, K >= 2) */
     int32_t freqscorr;         /* FREQSCORR */
     int32_t onefst;            /* ONEFST */
     int32_t inferalpha;        /* INFERALPHA */
@@ -154,8 +158,12 @@ typedef struct st_model {
     int32_t gensback;          /* GENSBACK (USEPOPINFO) */
     int32_t popflag_given;     /* 1: popflags in the data are POPFLAG values; 0: every
                                 * individual with a population is flagged (POPFLAG=0) */
-    int32_t reserved[2];
+    int32_t updatelocprior;    /* UPDATELOCPRIOR (LOCPRIOR): 0 keeps r, nu, gamma fixed */
+    int32_t reserved;
     double migrprior;          /* MIGRPRIOR (USEPOPINFO) */
+    double locpriorinit;       /* LOCPRIORINIT: initial r */
+    double maxlocprior;        /* MAXLOCPRIOR: upper bound of r */
+    double locpriorstep;       /* LOCPRIORSTEP: half-width of the r proposal */
 } st_model;
 
 int st_model_defaults(st_model *m);
@@ -182,6 +190,10 @@ int st_update_fst(st_chain *c);    /* UpdateFstCL    src/Updates/UpdateFst.c:100
 int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183         */
 int st_update_lambda(st_chain *c); /* UpdateLambda / UpdatePopLambda (CPU only in the
                                       reference) src/Updates/UpdateLambda.c:8-102   */
+int st_update_locprior(st_chain *c);/* UpdateLocPrior (CPU only in the reference)
+                                      src/Updates/UpdateLocPrior.c:142-150; with
+                                      LOCPRIOR and admixture st_update_alpha runs
+                                      UpdateAlphaLocPrior (Updates/UpdateAlpha.c:257-305) */
 /* One Metropolis-adjusted Langevin move on every Q_i with Z summed out and P
  * fixed (chains created with st_model.mala; st_sweep runs it after the Q
  * update).  No reference counterpart.                                        */
@@ -268,7 +280,8 @@ enum st_field {
     ST_F_LOGP,         /* float [L][K][A] */
     ST_F_EPS,          /* double [L][A] */
     ST_F_F,            /* double [K] */
-    ST_F_ALPHA,        /* double [K] */
+    ST_F_ALPHA,        /* double [K]; LOCPRIOR with admixture [NUMLOCATIONS+1][K],
+                        * the global row first (src/structure.h:45 AlphaPos) */
     ST_F_LAMBDA,       /* double [K] */
     ST_F_Z,            /* uint8 [N][2][L], 0xFF = missing (needs store_z) */
     ST_F_N,            /* int32 [L][K][A] allele counts from the last Z pass (get) */
@@ -278,7 +291,7 @@ enum st_field {
     ST_F_PSUM,         /* double [L][K][A] */
     ST_F_SUMEPS,       /* double [L][A] */
     ST_F_FSTSUM,       /* double [K] */
-    ST_F_SUMALPHA,     /* double [K] */
+    ST_F_SUMALPHA,     /* double, as ST_F_ALPHA */
     ST_F_SUMLAMBDA,    /* double [K] */
     ST_F_ANCESTDIST,   /* int32 [N][K][NUMBOXES] */
     ST_F_STATS,        /* double [256]: like, sumlikes, sumsqlikes, ... */
@@ -286,8 +299,13 @@ enum st_field {
     ST_F_ERR,          /* int32: device error word */
     ST_F_DIMS,         /* int32 [8]: N, L, K, A, layout, G, nchunks, ngroups */
     ST_F_MALA_EPS,     /* float [N]: Langevin step sizes (chains with st_model.mala) */
-    ST_F_USEPOPPROBS   /* double [N][K][GENSBACK+1]: USEPOPINFO posterior sums
+    ST_F_USEPOPPROBS,  /* double [N][K][GENSBACK+1]: USEPOPINFO posterior sums
                         * (the reference's UsePopProbs, from sweep BURNIN on) */
+    ST_F_LOCPRIOR,     /* double: LOCPRIOR's LocPrior array, [1] = r with admixture,
+                        * [1 + K*(NUMLOCATIONS+1)] = r, nu [K], gamma [NUMLOCATIONS][K]
+                        * without (src/structure.c:354-365, structure.h:47) */
+    ST_F_SUMLOCPRIOR,  /* double, as ST_F_LOCPRIOR: sums from sweep BURNIN on */
+    ST_F_MYLOC         /* int32 [N]: each individual's location 0..NUMLOCATIONS-1 (get) */
 };
 int st_get_state(st_chain *c, int field, void *host, size_t bytes);
 int st_set_state(st_chain *c, int field, const void *host, size_t bytes);

@@ -25,7 +25,7 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _ci, _cd, _cu32, _cu64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
 
 (S_INITZ, S_Z, S_P, S_QG, S_QM, S_QMA, S_ALPHA, S_EPS, S_FST, S_MALA, S_LAMBDA,
- S_NOADMIX, S_POPINFO) = range(1, 14)
+ S_NOADMIX, S_POPINFO, S_LOCPRIOR, S_LOCALPHA) = range(1, 16)
 
 
 def rnd_words(w):
@@ -73,8 +73,14 @@ class Oracle:
         lib.orc_counts.argtypes = [_ci, _ci, _ci, _ci, _i32p, _i32p, _ci, _i32p, _i32p, _i32p]
         lib.orc_update_p.argtypes = [_ci, _ci, _ci, _i32p, _i32p, _ci, _f64p, _f64p, _f64p,
                                      _cu64, _cu32, _f32p, _f32p, C.POINTER(_ci)]
-        lib.orc_update_q_gibbs.argtypes = [_ci, _ci, _i32p, _f64p, _cu64, _cu32, _f32p, _f32p, C.POINTER(_ci)]
-        lib.orc_metro_propose.argtypes = [_ci, _ci, _f64p, _cu64, _cu32, _f32p, _f32p, C.POINTER(_ci)]
+        lib.orc_update_q_gibbs.argtypes = [_ci, _ci, _i32p, _f64p, _cu64, _cu32, _f32p, _f32p,
+                                           C.POINTER(_ci), C.c_void_p]
+        lib.orc_metro_propose.argtypes = [_ci, _ci, _f64p, _cu64, _cu32, _f32p, _f32p,
+                                          C.POINTER(_ci), C.c_void_p]
+        lib.orc_update_locprior.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _f64p, _f64p, _cd,
+                                            _cd, _cd, _cu64, _cu32, C.c_void_p]
+        lib.orc_update_alpha_locprior.argtypes = [_ci, _ci, _ci, _i32p, _f64p, _f64p, _cd, _cd,
+                                                  _cd, _cu64, _cu32, C.c_void_p]
         lib.orc_metro_logdiff.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _f32p, _f32p, _f64p]
         lib.orc_metro_accept.argtypes = [_ci, _ci, _f64p, _cu64, _cu32, _f32p, _f32p, _f32p, _f32p, _u8p]
         lib.orc_metro_accept.restype = _ci
@@ -94,7 +100,7 @@ class Oracle:
                                         _f64p]
         lib.orc_loglik_grad.restype = _cd
         lib.orc_update_q_noadmix.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _cu64, _cu32,
-                                             _f32p, _f32p, _i32p]
+                                             _f32p, _f32p, _i32p, C.c_void_p, C.c_void_p]
         lib.orc_update_q_withpops.argtypes = [_ci, _ci, _ci, _ci, _i32p, _f32p, _i32p, _i32p,
                                               _ci, _cd, _cu64, _cu32, _ci, _f32p, _f32p, _f64p]
         lib.orc_update_lambda.argtypes = [_ci, _ci, _ci, _i32p, _f32p, _f64p, _ci, _ci, _f64p,
@@ -167,21 +173,53 @@ class Oracle:
                               P, logP, C.byref(err))
         return P, logP, err.value
 
-    def update_q_gibbs(self, m, alpha, key, rep):
+    def update_q_gibbs(self, m, alpha, key, rep, arow=None):
+        """arow [N]: row of alpha [rows][K] per individual (LOCPRIOR)."""
         N, K = m.shape
         Q = np.zeros((N, K), np.float32)
         logQ = np.zeros((N, K), np.float32)
         err = _ci(0)
-        self.lib.orc_update_q_gibbs(N, K, m, alpha, key, rep, Q, logQ, C.byref(err))
+        ar = None if arow is None else np.ascontiguousarray(arow, np.int32)
+        self.lib.orc_update_q_gibbs(N, K, m, np.ascontiguousarray(alpha, np.float64).reshape(-1),
+                                    key, rep, Q, logQ, C.byref(err),
+                                    None if ar is None else ar.ctypes.data)
         return Q, logQ, err.value
 
-    def metro_propose(self, N, alpha, key, rep):
-        K = alpha.shape[0]
+    def metro_propose(self, N, alpha, key, rep, arow=None):
+        K = alpha.shape[-1]
         T = np.zeros((N, K), np.float32)
         lT = np.zeros((N, K), np.float32)
         err = _ci(0)
-        self.lib.orc_metro_propose(N, K, alpha, key, rep, T, lT, C.byref(err))
+        ar = None if arow is None else np.ascontiguousarray(arow, np.int32)
+        self.lib.orc_metro_propose(N, K, np.ascontiguousarray(alpha, np.float64).reshape(-1), key,
+                                   rep, T, lT, C.byref(err), None if ar is None else ar.ctypes.data)
         return T, lT, err.value
+
+    def update_locprior(self, myloc, Q, alpha, locp, noadmix, alphapropsd, step, maxlp, key,
+                        rep):
+        """UpdateLocPrior restated; returns (locp, rand words, normals) where
+        the words are the rand() values the reference would consume."""
+        N, K = Q.shape
+        nloc = int(np.max(myloc)) + 1
+        lp = np.ascontiguousarray(locp, np.float64).copy()
+        tr, keep = _trace(nloc, K)
+        self.lib.orc_update_locprior(N, K, nloc, int(noadmix), np.ascontiguousarray(myloc, np.int32),
+                                     np.ascontiguousarray(Q, np.float32),
+                                     np.ascontiguousarray(alpha, np.float64), lp, alphapropsd,
+                                     step, maxlp, key, rep, C.byref(tr))
+        return lp, keep[0][:tr.nr].copy(), keep[1][:tr.nn].copy()
+
+    def update_alpha_locprior(self, myloc, logQ, alpha, r, alphapropsd, alphamax, key, rep):
+        """UpdateAlphaLocPrior restated; logQ FP64.  Returns (alpha, words,
+        normals)."""
+        N, K = logQ.shape
+        nloc = int(np.max(myloc)) + 1
+        al = np.ascontiguousarray(alpha, np.float64).copy()
+        tr, keep = _trace(nloc, K)
+        self.lib.orc_update_alpha_locprior(N, K, nloc, np.ascontiguousarray(myloc, np.int32),
+                                           np.ascontiguousarray(logQ, np.float64), al, r,
+                                           alphapropsd, alphamax, key, rep, C.byref(tr))
+        return al, keep[0][:tr.nr].copy(), keep[1][:tr.nn].copy()
 
     def metro_logdiff(self, geno, Q, TestQ, P):
         N, _, L = geno.shape
@@ -258,13 +296,17 @@ class Oracle:
     def est_logprob(self, s, ss, reps):
         return self.lib.orc_est_logprob(s, ss, reps)
 
-    def update_q_noadmix(self, geno, logP, key, rep):
+    def update_q_noadmix(self, geno, logP, key, rep, locp=None, myloc=None):
         N, _, L = geno.shape
         _, K, A = logP.shape
         Q, lQ = np.zeros((N, K), np.float32), np.zeros((N, K), np.float32)
         pick = np.zeros(N, np.int32)
+        lp = None if locp is None else np.ascontiguousarray(locp, np.float64)
+        ml = None if myloc is None else np.ascontiguousarray(myloc, np.int32)
         self.lib.orc_update_q_noadmix(N, L, K, A, np.ascontiguousarray(geno, np.int32),
-                                      np.ascontiguousarray(logP, np.float32), key, rep, Q, lQ, pick)
+                                      np.ascontiguousarray(logP, np.float32), key, rep, Q, lQ, pick,
+                                      None if lp is None else lp.ctypes.data,
+                                      None if ml is None else ml.ctypes.data)
         return Q, lQ, pick
 
     def update_q_withpops(self, geno, P, population, popflags, gensback, migrprior, key, rep,
@@ -318,6 +360,16 @@ class Oracle:
         return ll, dq, dp, lli
 
 
+class Trace(C.Structure):
+    _fields_ = [("rw", C.c_void_p), ("nr", _ci), ("nv", C.c_void_p), ("nn", _ci)]
+
+
+def _trace(nloc, K):
+    rw = np.zeros(8 + 4 * (nloc + 1), np.int32)
+    nv = np.zeros((nloc + 1) * K + 4, np.float64)
+    return Trace(rw.ctypes.data, 0, nv.ctypes.data, 0), (rw, nv)
+
+
 class RefModel(C.Structure):
     _fields_ = [(n, _ci) for n in ("N", "L", "K", "maxalleles", "freqscorr", "onefst",
                                    "inferalpha", "popalphas", "unifprioralpha", "metrofreq",
@@ -327,7 +379,8 @@ class RefModel(C.Structure):
                                   "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
               [("inferlambda", _ci), ("popspecificlambda", _ci), ("noadmix", _ci),
                ("admburnin", _ci), ("usepopinfo", _ci), ("gensback", _ci), ("popflag", _ci),
-               ("migrprior", _cd)]
+               ("migrprior", _cd), ("locprior", _ci), ("updatelocprior", _ci),
+               ("locpriorinit", _cd), ("maxlocprior", _cd), ("locpriorstep", _cd)]
 
 
 class RefView(C.Structure):
@@ -336,7 +389,9 @@ class RefView(C.Structure):
                                             "sumAlpha", "PSum", "QSum", "like", "sumlikes",
                                             "sumsqlikes")] + \
               [("maxalleles", _ci), ("rep", _ci)] + \
-              [(n, C.POINTER(_cd)) for n in ("lambda_", "sumlambda", "UsePopProbs")]
+              [(n, C.POINTER(_cd)) for n in ("lambda_", "sumlambda", "UsePopProbs", "LocPrior",
+                                            "sumLocPrior")] + \
+              [("LocPriorLen", _ci), ("numlocations", _ci)]
 
 
 def ref_model(**kw):
@@ -345,7 +400,8 @@ def ref_model(**kw):
              pfrompopflagonly=0, ancestdist=0, numboxes=1000, alpha=1.0, alphamax=10.0,
              alphapropsd=0.025, alphapriora=0.05, alphapriorb=0.001, lambda_=1.0,
              fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0, noadmix=0,
-             admburnin=0, usepopinfo=0, gensback=2, popflag=0, migrprior=0.05)
+             admburnin=0, usepopinfo=0, gensback=2, popflag=0, migrprior=0.05, locprior=0,
+             updatelocprior=1, locpriorinit=1.0, maxlocprior=20.0, locpriorstep=0.1)
     d.update(kw)
     return RefModel(**d)
 
@@ -369,7 +425,17 @@ class RefLib:
         lib.stref_individuals.argtypes = [_ci, C.c_void_p]
         lib.stref_individuals.restype = C.c_void_p
         lib.stref_free.argtypes = [C.c_void_p]
-        lib.stref_chain_new.argtypes = [C.POINTER(RefModel), _i32p, C.c_void_p, C.c_void_p, _cu64]
+        lib.stref_chain_new.argtypes = [C.POINTER(RefModel), _i32p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, _cu64]
+        lib.stref_individuals_loc.argtypes = [_ci, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.stref_individuals_loc.restype = C.c_void_p
+        lib.stref_numlocations.restype = _ci
+        lib.stref_set_numlocations.argtypes = [_ci]
+        lib.UpdateLocPrior.argtypes = [_f64p, _f64p, _f64p, C.c_void_p]
+        lib.UpdateAlphaLocPrior.argtypes = [_f64p, _f64p, _f64p, C.c_void_p]
+        lib.UpdateQAdmixture.argtypes = [_f64p, _i32p, _f64p, C.c_void_p, C.c_void_p]
+        lib.UpdateQMetro.argtypes = [_i32p, C.c_void_p, _f64p, _f64p, _f64p, _ci, C.c_void_p,
+                                     C.c_void_p, _f64p]
         lib.stref_individuals_pop.argtypes = [_ci, C.c_void_p, C.c_void_p]
         lib.stref_individuals_pop.restype = C.c_void_p
         lib.UpdateQWithPops.argtypes = [_i32p, _f64p, _f64p, C.c_void_p, _f64p, _ci, C.c_void_p,
@@ -443,13 +509,25 @@ class RefLib:
         self.lib.stref_normal_queue(v.ctypes.data, v.size)
 
     # -- chain -----------------------------------------------------------------
-    def chain_new(self, model, geno, popflags=None, seed=1, population=None):
+    def chain_new(self, model, geno, popflags=None, seed=1, population=None, location=None):
         pf = None if popflags is None else np.ascontiguousarray(popflags, np.int32)
         pp = None if population is None else np.ascontiguousarray(population, np.int32)
-        self._keep += [pf, pp]
+        lc = None if location is None else np.ascontiguousarray(location, np.int32)
+        self._keep += [pf, pp, lc]
         return self.lib.stref_chain_new(C.byref(model), np.ascontiguousarray(geno, np.int32),
                                         None if pf is None else pf.ctypes.data,
-                                        None if pp is None else pp.ctypes.data, seed)
+                                        None if pp is None else pp.ctypes.data,
+                                        None if lc is None else lc.ctypes.data, seed)
+
+    def individuals_loc(self, N, location, popflags=None, population=None):
+        """Individuals with locations; runs GetNumLocations (NUMLOCATIONS,
+        myloc).  Returns (handle, NUMLOCATIONS)."""
+        pf = np.zeros(N, np.int32) if popflags is None else np.ascontiguousarray(popflags, np.int32)
+        pp = np.zeros(N, np.int32) if population is None else np.ascontiguousarray(population, np.int32)
+        lc = np.ascontiguousarray(location, np.int32)
+        self._keep += [pf, pp, lc]
+        h = self.lib.stref_individuals_loc(N, pf.ctypes.data, pp.ctypes.data, lc.ctypes.data)
+        return h, self.lib.stref_numlocations()
 
     def individuals_pop(self, N, popflags, population):
         pf = np.ascontiguousarray(popflags, np.int32)
@@ -465,15 +543,21 @@ class RefLib:
         def arr(p, n, dt=np.float64):
             return np.ctypeslib.as_array(p, shape=(n,)).copy()
 
+        # LOCPRIOR with admixture: alpha global + one row per location
+        na = K * (v.numlocations + 1) if v.LocPriorLen == 1 else K
+
         return dict(
             A=A, rep=v.rep,
             Q=arr(v.Q, N * K).reshape(N, K), P=arr(v.P, L * K * A).reshape(L, K, A),
             Z=arr(v.Z, N * 2 * L).reshape(N, 2, L), Geno=arr(v.Geno, N * 2 * L).reshape(N, 2, L),
             NumAlleles=arr(v.NumAlleles, L), Eps=arr(v.Eps, L * A).reshape(L, A),
-            Fst=arr(v.Fst, K), Alpha=arr(v.Alpha, K), QSum=arr(v.QSum, N * K).reshape(N, K),
+            Fst=arr(v.Fst, K), Alpha=arr(v.Alpha, na), QSum=arr(v.QSum, N * K).reshape(N, K),
             PSum=arr(v.PSum, L * K * A).reshape(L, K, A), SumEps=arr(v.SumEps, L * A).reshape(L, A),
-            FstSum=arr(v.FstSum, K), sumAlpha=arr(v.sumAlpha, K),
+            FstSum=arr(v.FstSum, K), sumAlpha=arr(v.sumAlpha, na),
             like=v.like[0], sumlikes=v.sumlikes[0], sumsqlikes=v.sumsqlikes[0],
             lambda_=arr(v.lambda_, K), sumlambda=arr(v.sumlambda, K),
             usepop=(arr(v.UsePopProbs, N * K * (gensback + 1)).reshape(N, K, gensback + 1)
-                    if v.UsePopProbs else None))
+                    if v.UsePopProbs else None),
+            LocPrior=arr(v.LocPrior, v.LocPriorLen) if v.LocPriorLen else None,
+            sumLocPrior=arr(v.sumLocPrior, v.LocPriorLen) if v.LocPriorLen else None,
+            numlocations=v.numlocations)

@@ -33,6 +33,8 @@
 #include "Updates/UpdateEpsilon.h"
 #include "Updates/UpdateFst.h"
 #include "Updates/UpdateLambda.h"
+#include "Updates/UpdateLocPrior.h"
+#include "Util.h"
 
 /* ---- OpenCL host helpers (Kernels.c) as no-ops ------------------------- */
 int InitCLDict(CLDict *d) { (void)d; return EXIT_SUCCESS; }
@@ -141,6 +143,8 @@ typedef struct stref_model {
     int noadmix, admburnin;
     int usepopinfo, gensback, popflag;
     double migrprior;
+    int locprior, updatelocprior;
+    double locpriorinit, maxlocprior, locpriorstep;
 } stref_model;
 
 void stref_set_globals(const stref_model *m)
@@ -155,14 +159,16 @@ void stref_set_globals(const stref_model *m)
     METROFREQ = m->metrofreq; BURNIN = m->burnin; NUMREPS = m->numreps;
     COMPUTEPROB = m->computeprob; PFROMPOPFLAGONLY = m->pfrompopflagonly;
     ANCESTDIST = m->ancestdist; NUMBOXES = m->numboxes > 0 ? m->numboxes : 1000;
-    USEPOPINFO = m->usepopinfo; NOADMIX = m->noadmix; LOCPRIOR = 0; LINKAGE = 0;
+    USEPOPINFO = m->usepopinfo; NOADMIX = m->noadmix; LOCPRIOR = m->locprior; LINKAGE = 0;
+    UPDATELOCPRIOR = m->updatelocprior; LOCPRIORINIT = m->locpriorinit;
+    MAXLOCPRIOR = m->maxlocprior; LOCPRIORSTEP = m->locpriorstep;
     RECESSIVEALLELES = 0;
     INFERLAMBDA = m->inferlambda; POPSPECIFICLAMBDA = m->popspecificlambda;
     STARTATPOPINFO = 0; POPDATA = m->usepopinfo ? 1 : 0; POPFLAG = m->popflag;
     MIGRPRIOR = m->migrprior;
     INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = m->admburnin;
     NOALPHA = 0; PHASED = 0; PHASEINFO = 0; MARKOVPHASE = 0; NOQS = 0;
-    LOCDATA = 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0;
+    LOCDATA = m->locprior ? 1 : 0; LOCISPOP = 0; PRINTQHAT = 0; ECHODATA = 0;
     GENSBACK = m->usepopinfo ? m->gensback : 2;
 }
 
@@ -182,6 +188,21 @@ struct IND *stref_individuals_pop(int N, const int32_t *popflags, const int32_t 
 }
 void stref_free(void *p) { free(p); }
 
+/* individuals with a location (LOCDATA) as well; src/Util.c:237-275
+ * GetNumLocations sets NUMLOCATIONS and each myloc */
+struct IND *stref_individuals_loc(int N, const int32_t *popflags, const int32_t *population,
+                                  const int32_t *location)
+{
+    struct IND *ind = stref_individuals_pop(N, popflags, population);
+    if (location) {
+        for (int i = 0; i < N; i++) ind[i].Location = location[i];
+        GetNumLocations(ind);
+    }
+    return ind;
+}
+int stref_numlocations(void) { return NUMLOCATIONS; }
+void stref_set_numlocations(int n) { NUMLOCATIONS = n; }
+
 /* ---- one reference chain, driven in structure.c order ------------------ */
 typedef struct stref_chain {
     stref_model m;
@@ -189,6 +210,8 @@ typedef struct stref_chain {
     double *Q, *P, *Eps, *SumEps, *Fst, *FstSum, *Alpha, *sumAlpha;
     double *lambda, *sumlambda, *PSum, *QSum, *R, *sumR, *varR;
     double *sumIndLikes, *indLikesNorm, *randomArr, *Phase, *UsePopProbs;
+    double *LocPrior, *sumLocPrior;
+    int LocPriorLen, numlocations;
     double like, sumlikes, sumsqlikes;
     size_t nrand;
     struct IND *Individual;
@@ -203,7 +226,8 @@ static void fill_uniform(double *a, size_t n)
 /* geno: raw int32 [N][2][L] with -9 missing; recoded in a private copy by the
  * reference's own Initialization -> CountAlleles. */
 stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
-                             const int32_t *popflags, const int32_t *population, uint64_t seed)
+                             const int32_t *popflags, const int32_t *population,
+                             const int32_t *location, uint64_t seed)
 {
     stref_chain *c = calloc(1, sizeof(stref_chain));
     int N = m->N, L = m->L, K = m->K;
@@ -230,8 +254,19 @@ stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
     c->SumEps = calloc((size_t)L * A, sizeof(double));
     c->Fst = calloc((size_t)K, sizeof(double));
     c->FstSum = calloc((size_t)K, sizeof(double));
-    c->Alpha = calloc((size_t)K, sizeof(double));
-    c->sumAlpha = calloc((size_t)K, sizeof(double));
+    c->Individual = stref_individuals_loc(N, popflags, population,
+                                          m->locprior ? location : NULL);
+    c->numlocations = m->locprior ? NUMLOCATIONS : 0;
+    /* src/structure.c:354-375: LocPrior = r (admixture) or r, nu, gamma
+     * (no admixture); alpha global + one row per location (admixture) */
+    size_t na = (m->locprior && !m->noadmix) ? (size_t)K * (c->numlocations + 1) : (size_t)K;
+    c->Alpha = calloc(na, sizeof(double));
+    c->sumAlpha = calloc(na, sizeof(double));
+    if (m->locprior) {
+        c->LocPriorLen = m->noadmix ? 1 + K * (c->numlocations + 1) : 1;
+        c->LocPrior = calloc((size_t)c->LocPriorLen, sizeof(double));
+        c->sumLocPrior = calloc((size_t)c->LocPriorLen, sizeof(double));
+    }
     c->lambda = calloc((size_t)K, sizeof(double));
     c->sumlambda = calloc((size_t)K, sizeof(double));
     c->R = calloc((size_t)N, sizeof(double));
@@ -241,7 +276,6 @@ stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
     c->sumIndLikes = calloc((size_t)N, sizeof(double));
     c->indLikesNorm = calloc((size_t)N, sizeof(double));
     if (m->ancestdist) c->AncestDist = calloc((size_t)N * K * NUMBOXES, sizeof(int));
-    c->Individual = stref_individuals_pop(N, popflags, population);
     if (m->usepopinfo)
         c->UsePopProbs = calloc((size_t)N * K * (GENSBACK + 1), sizeof(double));
     size_t nr = (size_t)N * L * 2;
@@ -256,8 +290,8 @@ stref_chain *stref_chain_new(const stref_model *m, const int32_t *geno,
                    c->Z, c->Z1, c->Eps, c->SumEps, c->Fst, c->PSum, c->Q, c->QSum,
                    c->FstSum, c->AncestDist, c->UsePopProbs, c->Alpha, c->sumAlpha, c->sumR,
                    c->varR, &c->sumlikes, &c->sumsqlikes, &savefreq, c->R,
-                   c->lambda, c->sumlambda, c->Phase, NULL, NULL, NULL, 0,
-                   c->sumIndLikes, c->indLikesNorm, &dict);
+                   c->lambda, c->sumlambda, c->Phase, NULL, c->LocPrior, c->sumLocPrior,
+                   c->LocPriorLen, c->sumIndLikes, c->indLikesNorm, &dict);
     c->rep = 0;
     return c;
 }
@@ -267,6 +301,7 @@ int stref_chain_sweeps(stref_chain *c, int nsweeps)
 {
     stref_set_globals(&c->m);
     MAXALLELES = c->m.maxalleles;
+    NUMLOCATIONS = c->numlocations;
     int N = c->m.N, L = c->m.L, K = c->m.K, A = MAXALLELES;
     for (int s = 0; s < nsweeps; s++, c->rep++) {
         int rep = c->rep;
@@ -276,10 +311,15 @@ int stref_chain_sweeps(stref_chain *c, int nsweeps)
         if (METROFREQ > 0 && rep % METROFREQ == 0)
             fill_uniform(c->randomArr, (size_t)N * MAXRANDOM);
         UpdateQ(c->Geno, NULL, c->Q, c->P, c->Z, c->Alpha, rep, c->Individual,
-                c->UsePopProbs, NULL, NULL, c->randomArr);
+                c->UsePopProbs, NULL, c->LocPrior, c->randomArr);
+        if (LOCPRIOR && UPDATELOCPRIOR)     /* structure.c:535-537 */
+            UpdateLocPrior(c->Q, c->LocPrior, c->Alpha, c->Individual);
         fill_uniform(c->randomArr, (size_t)N * L * 2);
         UpdateZ(c->Z, c->Q, c->P, c->Geno, c->randomArr);
-        if (INFERALPHA) UpdateAlpha(c->Q, c->Alpha, c->Individual, rep);
+        if (LOCPRIOR && NOADMIX == 0)       /* structure.c:577-590 */
+            UpdateAlphaLocPrior(c->Q, c->Alpha, c->LocPrior, c->Individual);
+        else if (INFERALPHA)
+            UpdateAlpha(c->Q, c->Alpha, c->Individual, rep);
         if (INFERLAMBDA) {       /* structure.c:586-593 */
             if (POPSPECIFICLAMBDA) UpdatePopLambda(c->P, c->lambda, c->NumAlleles);
             else UpdateLambda(c->P, c->Eps, c->lambda, c->NumAlleles);
@@ -293,8 +333,8 @@ int stref_chain_sweeps(stref_chain *c, int nsweeps)
                            c->Fst, c->FstSum, c->NumAlleles, c->AncestDist, c->Alpha,
                            c->sumAlpha, c->sumR, c->varR, &c->like, &c->sumlikes,
                            &c->sumsqlikes, c->R, c->Eps, c->SumEps, 0.0, c->lambda,
-                           c->sumlambda, NULL, NULL, NULL, 0, c->sumIndLikes,
-                           c->indLikesNorm, rep);
+                           c->sumlambda, NULL, c->LocPrior, c->sumLocPrior,
+                           c->LocPriorLen, c->sumIndLikes, c->indLikesNorm, rep);
     }
     return c->rep;
 }
@@ -305,6 +345,8 @@ typedef struct stref_view {
     double *PSum, *QSum, *like, *sumlikes, *sumsqlikes;
     int maxalleles, rep;
     double *lambda, *sumlambda, *UsePopProbs;
+    double *LocPrior, *sumLocPrior;
+    int LocPriorLen, numlocations;
 } stref_view;
 
 void stref_chain_view(stref_chain *c, stref_view *v)
@@ -317,6 +359,8 @@ void stref_chain_view(stref_chain *c, stref_view *v)
     v->like = &c->like; v->sumlikes = &c->sumlikes; v->sumsqlikes = &c->sumsqlikes;
     v->maxalleles = c->m.maxalleles; v->rep = c->rep;
     v->lambda = c->lambda; v->sumlambda = c->sumlambda; v->UsePopProbs = c->UsePopProbs;
+    v->LocPrior = c->LocPrior; v->sumLocPrior = c->sumLocPrior;
+    v->LocPriorLen = c->LocPriorLen; v->numlocations = c->numlocations;
 }
 
 void stref_chain_free(stref_chain *c)
@@ -325,7 +369,7 @@ void stref_chain_free(stref_chain *c)
                   c->Q, c->P, c->Eps, c->SumEps, c->Fst, c->FstSum, c->Alpha,
                   c->sumAlpha, c->lambda, c->sumlambda, c->PSum, c->QSum, c->R,
                   c->sumR, c->varR, c->sumIndLikes, c->indLikesNorm, c->randomArr,
-                  c->Phase, c->Individual, c->UsePopProbs};
+                  c->Phase, c->Individual, c->UsePopProbs, c->LocPrior, c->sumLocPrior};
     for (size_t j = 0; j < sizeof(ps) / sizeof(ps[0]); j++) free(ps[j]);
     free(c);
 }

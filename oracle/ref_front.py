@@ -12,7 +12,9 @@ process globals and exits on errors, so each scenario runs in its own process:
 
 spec: {"argv": [...], "read_data": bool, "sums": "<npz in workdir>" or null,
        "rep": int}; with USEPOPINFO=1 the sums carry "usepop" [N][K][GENSBACK+1]
-and CheckPopPriors (src/Init.c:15-70) runs before OutPutResults.  The working directory is <workdir> (the reference opens
+and CheckPopPriors (src/Init.c:15-70) runs before OutPutResults; with
+LOCPRIOR=1 they carry "sumLocPrior" (and sumAlpha of K * (locations + 1)
+values with admixture).  The working directory is <workdir> (the reference opens
 its files relative to it).  Results go to <workdir>/ref_out.json and
 <workdir>/ref_data.npz; OutPutResults writes OUTFILE_f (and OUTFILE_q).
 """
@@ -92,6 +94,14 @@ def main(workdir, specpath):
             z = np.load(os.path.join(workdir, spec["sums"]))
             K = g("MAXPOPS").value
             usepop = None
+            slp, lplen = None, 0
+            if g("LOCDATA").value > 0 or g("LOCISPOP").value:
+                # src/structure.c:350-352
+                lib.GetNumLocations.argtypes = [C.c_void_p]
+                lib.GetNumLocations(inds)
+            if g("LOCPRIOR").value:
+                slp = np.ascontiguousarray(z["sumLocPrior"], np.float64)
+                lplen = slp.size
             if g("USEPOPINFO").value:
                 # src/Init.c:417: the prior-population checks run before the
                 # chain and decide which individuals print the migrant model
@@ -118,7 +128,8 @@ def main(workdir, specpath):
                               float(z["sumlikes"]), float(z["sumsqlikes"]), P(keep["sumAlpha"]),
                               P(zeros["sumR"]), P(zeros["varR"]), na, tr, 1, names,
                               P(zeros["R"]), P(keep["SumEps"]), P(zeros["lambda"]),
-                              P(keep["sumlambda"]), None, 0, P(zeros["sil"]), P(zeros["iln"]),
+                              P(keep["sumlambda"]), P(slp) if slp is not None else None, lplen,
+                              P(zeros["sil"]), P(zeros["iln"]),
                               len(argv), cargv)
     with open(os.path.join(workdir, "ref_out.json"), "w") as f:
         json.dump(out, f)

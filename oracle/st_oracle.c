@@ -351,24 +351,29 @@ static void dirichlet_tree(const double *lg, int K, float *Q, float *logQ)
 }
 
 void orc_update_q_gibbs(int N, int K, const int32_t *m, const double *alpha,
-                        uint64_t key, uint32_t rep, float *Q, float *logQ, int *err)
+                        uint64_t key, uint32_t rep, float *Q, float *logQ, int *err,
+                        const int32_t *arow)
 {
     double lg[64];
     for (int i = 0; i < N; i++) {
+        /* LOCPRIOR: the individual's location row of alpha (UpdateQ.c:409-413) */
+        const double *al = alpha + (arow ? (size_t)arow[i] * K : 0);
         for (int k = 0; k < K; k++)
-            lg[k] = orc_loggamma(alpha[k] + (double)m[(size_t)i * K + k],
+            lg[k] = orc_loggamma(al[k] + (double)m[(size_t)i * K + k],
                                  (uint32_t)(i * K + k), rep, ORC_S_QG, key, err);
         dirichlet_tree(lg, K, Q + (size_t)i * K, logQ + (size_t)i * K);
     }
 }
 
 void orc_metro_propose(int N, int K, const double *alpha, uint64_t key,
-                       uint32_t rep, float *TestQ, float *logTestQ, int *err)
+                       uint32_t rep, float *TestQ, float *logTestQ, int *err,
+                       const int32_t *arow)
 {
     double lg[64];
     for (int i = 0; i < N; i++) {
+        const double *al = alpha + (arow ? (size_t)arow[i] * K : 0);   /* UpdateQ.c:255-257 */
         for (int k = 0; k < K; k++)
-            lg[k] = orc_loggamma(alpha[k], (uint32_t)(i * K + k), rep, ORC_S_QM, key, err);
+            lg[k] = orc_loggamma(al[k], (uint32_t)(i * K + k), rep, ORC_S_QM, key, err);
         dirichlet_tree(lg, K, TestQ + (size_t)i * K, logTestQ + (size_t)i * K);
     }
 }
@@ -855,13 +860,15 @@ void orc_update_lambda(int L, int K, int A, const int32_t *numalleles, const flo
 /* Updates/UpdateQ.c:310-383 UpdateQNoAdmix with mymath.c:80-100 PickAnOption */
 /* ------------------------------------------------------------------------ */
 void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const float *logP,
-                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick)
+                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick,
+                          const double *locp, const int32_t *myloc)
 {
     double p[64];
     for (int i = 0; i < N; i++) {
         double mx = 0.0;
         for (int k = 0; k < K; k++) {
-            double s = 0.0;
+            /* LOCPRIOR: the product starts at gamma[myloc][k] (UpdateQ.c:339-345) */
+            double s = locp ? log(locp[1 + (size_t)K * (myloc[i] + 1) + k]) : 0.0;
             for (int l = 0; l < L; l++)
                 for (int line = 0; line < 2; line++) {
                     int a = geno[((size_t)i * 2 + line) * L + l];
@@ -962,6 +969,177 @@ void orc_update_q_withpops(int N, int L, int K, int A, const int32_t *geno, cons
         for (int k = 0; k < K; k++) {
             Q[(size_t)i * K + k] = (float)q[k];
             logQ[(size_t)i * K + k] = q[k] > 0.0 ? (float)log(q[k]) : -INFINITY;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* LOCPRIOR                                                                 */
+/* ------------------------------------------------------------------------ */
+/* Uniform draws in the form of ran.c:128-147 RandomReal / RandomInteger on a
+ * 31-bit rand() word (here w >> 1 of a Philox word); the words and normals
+ * are appended to the trace in the order the reference consumes them. */
+static double lp_real(uint32_t w, double lo, double hi, orc_trace *tr)
+{
+    uint32_t v = w >> 1;
+    if (tr) tr->rw[tr->nr++] = (int32_t)v;
+    double d = (double)v / 2147483648.0;
+    return lo + d * (hi - lo);
+}
+
+static int lp_int(uint32_t w, int lo, int hi, orc_trace *tr)
+{
+    uint32_t v = w >> 1;
+    if (tr) tr->rw[tr->nr++] = (int32_t)v;
+    double d = (double)v / 2147483648.0;
+    return lo + (int)(d * (hi - lo + 1));
+}
+
+static double lp_normal(uint32_t idx, uint32_t rep, uint64_t key, orc_trace *tr)
+{
+    double z = orc_normal(idx, rep, ORC_S_LOCALPHA, key);
+    if (tr) tr->nv[tr->nn++] = z;
+    return z;
+}
+
+/* Updates/UpdateLocPrior.c:12-140: UpdateLocPriorNoAdmix (r, nu, gamma) and
+ * UpdateLocPriorAdmix (r only).  locp is the reference's LocPrior array:
+ * [0] r, [1 + k] nu (eta), [1 + K*(loc+1) + k] gamma of location loc.
+ * alpha [(nloc+1)][K]: the global row, then one row per location.
+ * Draws: r at (0, 0) of ORC_S_LOCPRIOR (word 0 the proposal, word 1 the
+ * acceptance), nu at (0, 1) (words: pop1, pop2, step, acceptance), gamma of
+ * location loc at (loc, 2) (same words). */
+void orc_update_locprior(int N, int K, int nloc, int noadmix, const int32_t *myloc,
+                         const float *Q, const double *alpha, double *locp,
+                         double alphapropsd, double step, double maxlp, uint64_t key,
+                         uint32_t rep, orc_trace *tr)
+{
+    uint32_t w[4];
+    const double cur = locp[0];
+    philox4(0, 0, rep, ORC_S_LOCPRIOR, key, w);
+    const double nw = lp_real(w[0], cur - step, cur + step, tr);
+    if (!noadmix) {
+        if (nw > 0.0 && nw < maxlp) {
+            const double d = nw - cur;
+            double diff = 0.0;
+            for (int k = 0; k < K; k++) {
+                const double ga = alpha[k];
+                for (int loc = 0; loc < nloc; loc++) {
+                    const double la = alpha[(size_t)K * (loc + 1) + k];
+                    diff += ga * d * log(la) - d * la - orc_lgamma(ga * nw) +
+                            orc_lgamma(ga * cur) + ga * nw * log(nw) - ga * cur * log(cur);
+                }
+            }
+            if (diff > 0.0 || lp_real(w[1], 0.0, 1.0, tr) < exp(diff)) locp[0] = nw;
+        }
+        return;
+    }
+    double *eta = locp + 1;
+    double *gam = locp + 1 + K;     /* gam[loc*K + k] */
+    if (nw > 0.0 && nw < maxlp) {
+        double ld = orc_lgamma(nw) - orc_lgamma(cur);
+        for (int k = 0; k < K; k++) ld += orc_lgamma(cur * eta[k]) - orc_lgamma(nw * eta[k]);
+        ld *= nloc;
+        for (int loc = 0; loc < nloc; loc++)
+            for (int k = 0; k < K; k++) ld += (nw - cur) * eta[k] * log(gam[(size_t)loc * K + k]);
+        if (ld >= 0.0 || lp_real(w[1], 0.0, 1.0, tr) < exp(ld)) locp[0] = nw;
+    }
+    const double r = locp[0];
+    philox4(0, 1, rep, ORC_S_LOCPRIOR, key, w);
+    int p1 = lp_int(w[0], 0, K - 1, tr), p2 = lp_int(w[1], 0, K - 2, tr);
+    if (p2 >= p1) p2++;
+    double dd = lp_real(w[2], 0.0, alphapropsd, tr);
+    double e1 = eta[p1] + dd, e2 = eta[p2] - dd;
+    if (e1 < 1.0 && e2 > 0.0) {
+        double ld = nloc * (orc_lgamma(r * eta[p1]) + orc_lgamma(r * eta[p2]) -
+                            orc_lgamma(r * e1) - orc_lgamma(r * e2));
+        for (int loc = 0; loc < nloc; loc++)
+            ld += r * ((e1 - eta[p1]) * log(gam[(size_t)loc * K + p1]) +
+                       (e2 - eta[p2]) * log(gam[(size_t)loc * K + p2]));
+        if (ld >= 0.0 || lp_real(w[3], 0.0, 1.0, tr) < exp(ld)) {
+            eta[p1] = e1;
+            eta[p2] = e2;
+        }
+    }
+    for (int loc = 0; loc < nloc; loc++) {
+        double dc1, dc2;
+        philox4((uint32_t)loc, 2, rep, ORC_S_LOCPRIOR, key, w);
+        p1 = lp_int(w[0], 0, K - 1, tr);
+        p2 = lp_int(w[1], 0, K - 2, tr);
+        if (p2 >= p1) p2++;
+        dd = lp_real(w[2], 0.0, alphapropsd, tr);
+        double *gl = gam + (size_t)loc * K;
+        const double g1 = gl[p1] + dd, g2 = gl[p2] - dd;
+        if (!(g1 < 1.0 && g2 > 0.0)) continue;
+        dc1 = dc2 = 0.0;    /* sum of Q over the location's individuals */
+        for (int i = 0; i < N; i++)
+            if (myloc[i] == loc) {
+                dc1 += (double)Q[(size_t)i * K + p1];
+                dc2 += (double)Q[(size_t)i * K + p2];
+            }
+        const double l1 = log(g1) - log(gl[p1]), l2 = log(g2) - log(gl[p2]);
+        const double ld = (r * eta[p1] - 1.0) * l1 + (r * eta[p2] - 1.0) * l2 + dc1 * l1 + dc2 * l2;
+        if (ld >= 0.0 || lp_real(w[3], 0.0, 1.0, tr) < exp(ld)) {
+            gl[p1] = g1;
+            gl[p2] = g2;
+        }
+    }
+}
+
+/* Updates/UpdateAlpha.c:118-139,257-305 UpdateAlphaLocPrior with
+ * LogProbQ_LocPrior_loc: the global alphas (a normal step each, accepted on
+ * the Gamma(alpha_k r, r) densities of the location alphas), then each
+ * location's alphas in turn against Pr(Q of its individuals | alpha_loc).
+ * logQ [N][K] in FP64.  Draws: the normal of global alpha k at (k, 0) of
+ * ORC_S_LOCALPHA and its acceptance at (k, 1) word 0; location loc, pop k:
+ * index K*(loc+1)+k likewise. */
+static double lp_logprob_loc(int N, int K, const int32_t *myloc, const double *logQ,
+                             const double *al, int loc)
+{
+    double like = 0.0, sa = 0.0, sg = 0.0;
+    int n = 0;
+    for (int i = 0; i < N; i++) {
+        if (myloc[i] != loc) continue;
+        for (int k = 0; k < K; k++) like += (al[k] - 1.0) * logQ[(size_t)i * K + k];
+        n++;
+    }
+    for (int k = 0; k < K; k++) {
+        sa += al[k];
+        sg += orc_lgamma(al[k]);
+    }
+    return like + (orc_lgamma(sa) - sg) * (double)n;
+}
+
+void orc_update_alpha_locprior(int N, int K, int nloc, const int32_t *myloc, const double *logQ,
+                               double *alpha, double r, double alphapropsd, double alphamax,
+                               uint64_t key, uint32_t rep, orc_trace *tr)
+{
+    uint32_t w[4];
+    for (int k = 0; k < K; k++) {
+        const double old = alpha[k];
+        const double nw = old + alphapropsd * lp_normal((uint32_t)k, rep, key, tr);
+        if (nw >= alphamax || nw <= 0.0) continue;
+        double diff = 0.0;
+        for (int loc = 0; loc < nloc; loc++)
+            diff += (nw - old) * r * log(alpha[(size_t)K * (loc + 1) + k]) - orc_lgamma(nw * r) +
+                    orc_lgamma(old * r) + (nw - old) * r * log(r);
+        philox4((uint32_t)k, 1, rep, ORC_S_LOCALPHA, key, w);
+        if (diff > 0.0 || lp_real(w[0], 0.0, 1.0, tr) < exp(diff)) alpha[k] = nw;
+    }
+    for (int loc = 0; loc < nloc; loc++) {
+        double *al = alpha + (size_t)K * (loc + 1);
+        double lp = lp_logprob_loc(N, K, myloc, logQ, al, loc);
+        for (int k = 0; k < K; k++) {
+            const uint32_t idx = (uint32_t)(K * (loc + 1) + k);
+            const double ga = alpha[k], old = al[k];
+            const double nw = old + alphapropsd * lp_normal(idx, rep, key, tr);
+            if (nw <= 0.0) continue;
+            al[k] = nw;
+            const double lpn = lp_logprob_loc(N, K, myloc, logQ, al, loc);
+            const double diff = (ga * r - 1.0) * log(nw / old) - r * (nw - old) + lpn - lp;
+            philox4(idx, 1, rep, ORC_S_LOCALPHA, key, w);
+            if (diff >= 0.0 || lp_real(w[0], 0.0, 1.0, tr) < exp(diff)) lp = lpn;
+            else al[k] = old;
         }
     }
 }

@@ -29,7 +29,8 @@ extern "C" {
 enum {
     ORC_S_INITZ = 1, ORC_S_Z = 2, ORC_S_P = 3, ORC_S_QG = 4, ORC_S_QM = 5,
     ORC_S_QMA = 6, ORC_S_ALPHA = 7, ORC_S_EPS = 8, ORC_S_FST = 9, ORC_S_MALA = 10,
-    ORC_S_LAMBDA = 11, ORC_S_NOADMIX = 12, ORC_S_POPINFO = 13
+    ORC_S_LAMBDA = 11, ORC_S_NOADMIX = 12, ORC_S_POPINFO = 13, ORC_S_LOCPRIOR = 14,
+    ORC_S_LOCALPHA = 15
 };
 
 /* Random123 Philox4x32-10 (Salmon et al., SC'11). */
@@ -66,10 +67,14 @@ void orc_update_p(int L, int K, int A, const int32_t *numalleles, const int32_t 
                   float *P, float *logP, int *err);
 
 /* --- Q (Updates/UpdateQ.c:387-424 Gibbs, 199-307 Metro) ----------------- */
+/* arow [N] (or NULL = row 0 for everyone): the row of alpha [rows][K] each
+ * individual draws with (LOCPRIOR: 1 + its location, UpdateQ.c:255,409) */
 void orc_update_q_gibbs(int N, int K, const int32_t *m, const double *alpha,
-                        uint64_t key, uint32_t rep, float *Q, float *logQ, int *err);
+                        uint64_t key, uint32_t rep, float *Q, float *logQ, int *err,
+                        const int32_t *arow);
 void orc_metro_propose(int N, int K, const double *alpha, uint64_t key,
-                       uint32_t rep, float *TestQ, float *logTestQ, int *err);
+                       uint32_t rep, float *TestQ, float *logTestQ, int *err,
+                       const int32_t *arow);
 void orc_metro_logdiff(int N, int L, int K, int A, const int32_t *geno,
                        const float *Q, const float *TestQ, const float *P,
                        double *logdiff);
@@ -105,8 +110,10 @@ void orc_update_fst(int K, int onefst, double fpriormean, double fpriorsd,
 /* ll_ik = sum over loci and copies of logP[l][k][allele] (FP64); pick k with
  * u*sum <= cumulative exp(ll - max), u = (w>>1)/2^31 of the Philox word at
  * (i, 0) of ORC_S_NOADMIX.  Q, logQ become one-hot (0 / -inf). */
+/* LOCPRIOR (locp, myloc non-NULL): ll_ik starts at log gamma[myloc_i][k]. */
 void orc_update_q_noadmix(int N, int L, int K, int A, const int32_t *geno, const float *logP,
-                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick);
+                          uint64_t key, uint32_t rep, float *Q, float *logQ, int32_t *pick,
+                          const double *locp, const int32_t *myloc);
 
 /* --- USEPOPINFO Q (Updates/UpdateQ.c:499-706 UpdateQWithPops) ----------- */
 /* For flagged individuals (popflags[i] != 0, population[i] in 1..K): the
@@ -154,6 +161,24 @@ void orc_mala_step(int N, int L, int K, const int32_t *geno, float *Q, float *lo
                    const float *P, const double *alpha, int popalphas, float *eps,
                    uint64_t key, uint32_t rep, int burnin, double target,
                    double *logr, uint8_t *acc);
+
+/* --- LOCPRIOR (Updates/UpdateLocPrior.c, Updates/UpdateAlpha.c:257-305) --- */
+/* The rand() words (w >> 1) and normals the reference would consume, in its
+ * order, are appended to a trace when one is given (rw / nv sized by the
+ * caller: 2 + 4 * (nloc + 1) words, (nloc + 1) * K normals are enough). */
+typedef struct orc_trace {
+    int32_t *rw;
+    int32_t nr;
+    double *nv;
+    int32_t nn;
+} orc_trace;
+void orc_update_locprior(int N, int K, int nloc, int noadmix, const int32_t *myloc,
+                         const float *Q, const double *alpha, double *locp,
+                         double alphapropsd, double step, double maxlp, uint64_t key,
+                         uint32_t rep, orc_trace *tr);
+void orc_update_alpha_locprior(int N, int K, int nloc, const int32_t *myloc, const double *logQ,
+                               double *alpha, double r, double alphapropsd, double alphamax,
+                               uint64_t key, uint32_t rep, orc_trace *tr);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,8 @@ LAYOUT_AUTO, LAYOUT_U8, LAYOUT_B2G = 0, 1, 2
 
 (F_Q, F_LOGQ, F_TESTQ, F_LOGTESTQ, F_P, F_LOGP, F_EPS, F_F, F_ALPHA, F_LAMBDA, F_Z, F_N,
  F_M, F_LOGDIFF, F_QSUM, F_PSUM, F_SUMEPS, F_FSTSUM, F_SUMALPHA, F_SUMLAMBDA, F_ANCESTDIST,
- F_STATS, F_REP, F_ERR, F_DIMS, F_MALA_EPS, F_USEPOPPROBS) = range(1, 28)
+ F_STATS, F_REP, F_ERR, F_DIMS, F_MALA_EPS, F_USEPOPPROBS, F_LOCPRIOR, F_SUMLOCPRIOR,
+ F_MYLOC) = range(1, 31)
 
 # stats block offsets (csrc/st_types.h)
 ST_LIKE, ST_SUMLIKES, ST_SUMSQ, ST_NLIKE, ST_METROHITS = 0, 1, 2, 3, 4
@@ -40,7 +41,7 @@ class DataDesc(C.Structure):
     _fields_ = [("num_inds", C.c_int32), ("num_loci", C.c_int32), ("lines", C.c_int32),
                 ("layout", C.c_int32), ("geno", C.c_void_p), ("packed", C.c_void_p),
                 ("num_alleles", C.c_void_p), ("popflags", C.c_void_p),
-                ("population", C.c_void_p)]
+                ("population", C.c_void_p), ("location", C.c_void_p)]
 
 
 class Model(C.Structure):
@@ -53,7 +54,9 @@ class Model(C.Structure):
                                    "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
         [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r", "mala",
                                   "mala_target", "admburnin", "gensback", "popflag_given")] + \
-        [("reserved", C.c_int32 * 2), ("migrprior", C.c_double)]
+        [("updatelocprior", C.c_int32), ("reserved", C.c_int32), ("migrprior", C.c_double),
+         ("locpriorinit", C.c_double), ("maxlocprior", C.c_double),
+         ("locpriorstep", C.c_double)]
 
 
 _lib = None
@@ -93,6 +96,7 @@ def lib():
         "st_collect": ([vp], C.c_int),
         "st_update_q_mala": ([vp], C.c_int),
         "st_update_lambda": ([vp], C.c_int),
+        "st_update_locprior": ([vp], C.c_int),
         "st_chain_save": ([vp, C.c_char_p], C.c_int),
         "st_chain_load": ([vp, C.c_char_p], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
@@ -190,7 +194,7 @@ class Data:
     """Genotypes in HBM (reference layout in, packed on the device)."""
 
     def __init__(self, ctx, num_alleles, geno=None, packed=None, popflags=None, layout=LAYOUT_AUTO,
-                 num_inds=None, num_loci=None, population=None):
+                 num_inds=None, num_loci=None, population=None, location=None):
         self.ctx = ctx
         na = np.ascontiguousarray(num_alleles, np.int32)
         d = DataDesc()
@@ -214,6 +218,9 @@ class Data:
         if population is not None:
             pp = np.ascontiguousarray(population, np.int32)
             d.population = pp.ctypes.data
+        if location is not None:
+            lc = np.ascontiguousarray(location, np.int32)
+            d.location = lc.ctypes.data
         self.N, self.L = d.num_inds, d.num_loci
         self.A = int(max(1, na.max()))
         self.num_alleles = na
@@ -234,7 +241,8 @@ _DT = {F_Q: np.float32, F_LOGQ: np.float32, F_TESTQ: np.float32, F_LOGTESTQ: np.
        F_LOGDIFF: np.float64, F_QSUM: np.float64, F_PSUM: np.float64, F_SUMEPS: np.float64,
        F_FSTSUM: np.float64, F_SUMALPHA: np.float64, F_SUMLAMBDA: np.float64,
        F_ANCESTDIST: np.int32, F_STATS: np.float64, F_REP: np.int32, F_ERR: np.int32,
-       F_DIMS: np.int32, F_MALA_EPS: np.float32, F_USEPOPPROBS: np.float64}
+       F_DIMS: np.int32, F_MALA_EPS: np.float32, F_USEPOPPROBS: np.float64,
+       F_LOCPRIOR: np.float64, F_SUMLOCPRIOR: np.float64, F_MYLOC: np.int32}
 
 
 class Chain:
@@ -280,6 +288,7 @@ class Chain:
     def DataCollection(self): self.ctx.check(lib().st_collect(self.h))
     def UpdateQMala(self): self.ctx.check(lib().st_update_q_mala(self.h))
     def UpdateLambda(self): self.ctx.check(lib().st_update_lambda(self.h))
+    def UpdateLocPrior(self): self.ctx.check(lib().st_update_locprior(self.h))
 
     def save(self, path):
         """Checkpoint the whole chain state to `path` (st_chain_save)."""

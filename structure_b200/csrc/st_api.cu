@@ -37,6 +37,7 @@ struct st_data {
   int32_t* popflags = nullptr;
   std::vector<int32_t> na_h;
   std::vector<int32_t> popflags_h, population_h;   // population empty: no POPDATA
+  std::vector<int32_t> location_h;                 // empty: no location data
   std::vector<int64_t> cnt_h;    // [L][A] allele copies observed
   std::vector<int64_t> tot_h;    // [L] non-missing copies
   size_t bytes = 0;
@@ -282,7 +283,13 @@ int check_model(st_ctx* ctx, const st_model* m) {
     return seterr(ctx, ST_ERR_ARG, "MIGRPRIOR must be in [0, 1] (src/Init.c:22-26)");
   if (m->usepopinfo && m->mala)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move does not combine with USEPOPINFO");
-  if (m->locprior) return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR=1 is not on the GPU path");
+  if (m->locprior && m->noadmix && m->maxpops < 2)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "LOCPRIOR with NOADMIX needs MAXPOPS >= 2");
+  if (m->locprior && m->mala)
+    return seterr(ctx, ST_ERR_UNSUPPORTED, "the Langevin move does not combine with LOCPRIOR");
+  if (m->locprior && (m->maxlocprior <= 0.0 || m->locpriorstep <= 0.0 || m->locpriorinit <= 0.0 ||
+                      m->locpriorinit >= m->maxlocprior))
+    return seterr(ctx, ST_ERR_ARG, "LOCPRIORINIT must be in (0, MAXLOCPRIOR), LOCPRIORSTEP > 0");
   if (m->recessivealleles)
     return seterr(ctx, ST_ERR_UNSUPPORTED, "RECESSIVEALLELES=1 is not on the GPU path");
   if (m->freqscorr && (m->fpriormean <= 0 || m->fpriorsd <= 0))
@@ -486,6 +493,17 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
   cudaMemcpy(s->popflags, pf.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice);
   s->popflags_h = pf;
   if (d->population) s->population_h.assign(d->population, d->population + N);
+  if (d->location) {
+    for (int i = 0; i < N; i++)
+      if (d->location[i] < 0) {
+        cudaFree(s->numalleles);
+        cudaFree(s->popflags);
+        delete s;
+        // src/Util.c:241-246
+        return seterr(ctx, ST_ERR_ARG, "individual %d has negative location %d", i, d->location[i]);
+      }
+    s->location_h.assign(d->location, d->location + N);
+  }
 
   if (s->layout == kLayoutB2G) {
     const int wpr = (N + 15) / 16;
@@ -562,6 +580,10 @@ extern "C" int st_model_defaults(st_model* m) {
   m->admburnin = 2500;   // src/params.c:610 (BURNIN/4 of the preset BURNIN)
   m->gensback = 2;       // src/params.c:627
   m->migrprior = 0.05;   // src/params.c:629
+  m->updatelocprior = 1; // src/params.c:660-667
+  m->locpriorinit = 1.0;
+  m->maxlocprior = 20.0;
+  m->locpriorstep = 0.1;
   m->numreps = 20000;
   m->freqscorr = 1;
   m->onefst = 0;
@@ -623,11 +645,47 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       if (!pflag[i]) unflagged++;
     }
     h.alpha_n = unflagged;
-    if (model->inferalpha && !model->noadmix && unflagged == 0) h.inferalpha = 0;   // NOALPHA
+    if (model->inferalpha && !model->noadmix && unflagged == 0) {   // NOALPHA
+      h.inferalpha = 0;
+      h.noalpha = 1;
+    }
     initpop.resize(N);
     for (int i = 0; i < N; i++) initpop[i] = (pop1[i] >= 1 && pop1[i] <= K) ? pop1[i] - 1 : -1;
     popinfo_plan(N, L, &h.pi_lchunks, &h.pi_lchunk_len);
   }
+  // LOCPRIOR: locations numbered in increasing order of their ids
+  // (src/Util.c:237-275 GetNumLocations), individuals grouped by location
+  std::vector<int32_t> myloc, loc_start, loc_inds;
+  if (model->locprior) {
+    if (data->location_h.empty()) {
+      delete c;
+      return seterr(ctx, ST_ERR_ARG, "LOCPRIOR needs location data (st_data_desc.location)");
+    }
+    std::vector<int32_t> ids(data->location_h);
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    h.nloc = (int)ids.size();
+    myloc.resize(N);
+    loc_start.assign(h.nloc + 1, 0);
+    for (int i = 0; i < N; i++) {
+      myloc[i] = (int32_t)(std::lower_bound(ids.begin(), ids.end(), data->location_h[i]) - ids.begin());
+      loc_start[myloc[i] + 1]++;
+    }
+    for (int l = 0; l < h.nloc; l++) loc_start[l + 1] += loc_start[l];
+    loc_inds.resize(N);
+    std::vector<int32_t> fill(loc_start.begin(), loc_start.end() - 1);
+    for (int i = 0; i < N; i++) loc_inds[fill[myloc[i]]++] = i;
+    h.locprior = 1;
+    h.lp_admix = model->noadmix ? 0 : 1;
+    h.updatelocprior = model->updatelocprior ? 1 : 0;
+    h.locpriorstep = model->locpriorstep;
+    h.maxlocprior = model->maxlocprior;
+    h.lp_len = model->noadmix ? 1 + K * (h.nloc + 1) : 1;
+    // with admixture UpdateAlphaLocPrior replaces UpdateAlpha whatever
+    // INFERALPHA says (src/structure.c:577-590)
+    if (h.lp_admix) h.inferalpha = 0;
+  }
+  const size_t arows = h.lp_admix ? (size_t)h.nloc + 1 : 1;
   h.computeprob = model->computeprob; h.pfrompopflagonly = model->pfrompopflagonly;
   h.ancestdist = model->ancestdist; h.numboxes = model->numboxes > 0 ? model->numboxes : 1;
   h.metrofreq = model->metrofreq; h.burnin = model->burnin;
@@ -678,11 +736,11 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       *likepart, *redpart, *ctr, *rep, *err, *chain, *prefix;
   std::vector<Buf> bufs = {
       {&Q, NK * 4}, {&logQ, NK * 4}, {&TQ, NK * 4}, {&lTQ, NK * 4}, {&P, LKA * 4},
-      {&logP, LKA * 4}, {&eps, LA * 8}, {&F, (size_t)K * 8}, {&alpha, (size_t)K * 8},
+      {&logP, LKA * 4}, {&eps, LA * 8}, {&F, (size_t)K * 8}, {&alpha, arows * K * 8},
       {&lambda, (size_t)K * 8}, {&npart, LKA * 4},
       {&mpart, NK * 4}, {&ldpart, (size_t)h.ngroups * N * 8},
       {&QSum, NK * 8}, {&PSum, LKA * 8}, {&SumEps, LA * 8}, {&FstSum, (size_t)K * 8},
-      {&sumAlpha, (size_t)K * 8}, {&sumlambda, (size_t)K * 8}, {&stats, (size_t)kStSize * 8},
+      {&sumAlpha, arows * K * 8}, {&sumlambda, (size_t)K * 8}, {&stats, (size_t)kStSize * 8},
       {&likepart, (size_t)zctas * 8}, {&redpart, (size_t)nred * 8},
       {&ctr, (size_t)kCtrCount * 4}, {&rep, 4}, {&err, 4}, {&chain, sizeof(ChainDev)},
       {&prefix, 16}};
@@ -696,6 +754,13 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
                                   {&pi_part, (size_t)h.pi_lchunks * N * KG * 8}})
       bufs.push_back(b);
   }
+  void *lp_myloc = nullptr, *lp_start = nullptr, *lp_inds = nullptr, *lp_p = nullptr,
+       *lp_sum = nullptr;
+  if (model->locprior)
+    for (Buf b : std::vector<Buf>{{&lp_myloc, (size_t)N * 4}, {&lp_start, (size_t)(h.nloc + 1) * 4},
+                                  {&lp_inds, (size_t)N * 4}, {&lp_p, (size_t)h.lp_len * 8},
+                                  {&lp_sum, (size_t)h.lp_len * 8}})
+      bufs.push_back(b);
   void* napart = nullptr;
   if (model->noadmix) {
     noadmix_plan(N, L, &h.na_lchunks, &h.na_lchunk_len);
@@ -735,6 +800,13 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   c->d_prefix = (int*)prefix;
   data->chains++;
   h.napart = (double*)napart;
+  if (model->locprior) {
+    h.myloc = (const int32_t*)lp_myloc;
+    h.loc_start = (const int32_t*)lp_start;
+    h.loc_inds = (const int32_t*)lp_inds;
+    h.locp = (double*)lp_p;
+    h.sumlocp = (double*)lp_sum;
+  }
   if (model->usepopinfo) {
     h.popflags = (int32_t*)pi_flag;
     h.population = (const int32_t*)pi_pop;
@@ -772,8 +844,9 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   cudaMemcpyAsync(h.eps, ev.data(), LA * 8, cudaMemcpyHostToDevice, s);
   std::fill(kv.begin(), kv.end(), model->freqscorr ? model->fpriormean : 0.5);
   cudaMemcpyAsync(h.F, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
-  std::fill(kv.begin(), kv.end(), model->alpha);
-  cudaMemcpyAsync(h.alpha, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
+  // alpha = ALPHA, for every location row too (src/Init.c:350-368)
+  std::vector<double> av(arows * K, model->alpha);
+  cudaMemcpyAsync(h.alpha, av.data(), arows * K * 8, cudaMemcpyHostToDevice, s);
   std::fill(kv.begin(), kv.end(), model->lambda);
   cudaMemcpyAsync(h.lambda, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(h.P, 0, LKA * 4, s);
@@ -784,7 +857,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   cudaMemsetAsync(h.PSum, 0, LKA * 8, s);
   cudaMemsetAsync(h.SumEps, 0, LA * 8, s);
   cudaMemsetAsync(h.FstSum, 0, K * 8, s);
-  cudaMemsetAsync(h.sumAlpha, 0, K * 8, s);
+  cudaMemsetAsync(h.sumAlpha, 0, arows * K * 8, s);
   cudaMemsetAsync(h.sumlambda, 0, K * 8, s);
   cudaMemsetAsync(h.stats, 0, kStSize * 8, s);
   cudaMemsetAsync(h.ctr, 0, kCtrCount * 4, s);
@@ -798,6 +871,17 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     // adapted per individual during burn-in
     e0.assign(N, (float)(1.0 / sqrt(2.0 * L + 1.0)));
     cudaMemcpyAsync(h.mEps, e0.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+  }
+  std::vector<double> lpv;
+  if (h.locprior) {
+    // LocPrior = 1/K everywhere, r = LOCPRIORINIT (src/Init.c:359-368)
+    lpv.assign(h.lp_len, 1.0 / K);
+    lpv[0] = model->locpriorinit;
+    cudaMemcpyAsync(lp_myloc, myloc.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(lp_start, loc_start.data(), (size_t)(h.nloc + 1) * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(lp_inds, loc_inds.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(lp_p, lpv.data(), (size_t)h.lp_len * 8, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(lp_sum, 0, (size_t)h.lp_len * 8, s);
   }
   if (h.usepopinfo) {
     cudaMemcpyAsync(pi_flag, pflag.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
@@ -858,7 +942,8 @@ extern "C" int st_update_fst(st_chain* c) {
 // one-population update from sweep ADMBURNIN+1 (or BURNIN+1), admixture Gibbs
 // before it; alpha moves only before sweep ADMBURNIN (or BURNIN+1).
 static bool noadmix_q(const ChainDev& h, int rep) {
-  return h.noadmix && (rep > h.admburnin || rep > h.burnin);
+  // "don't use ADMBURNIN with LOCPRIOR models" (src/Updates/UpdateQ.c:731)
+  return h.noadmix && (rep > h.admburnin || rep > h.burnin || h.locprior);
 }
 static bool alpha_moves(const ChainDev& h, int rep) {
   return !(h.noadmix && (rep >= h.admburnin || rep > h.burnin));
@@ -907,10 +992,13 @@ extern "C" int st_update_z(st_chain* c) {
   return zpass(c, kZNormal, c->model.store_z ? kZfStoreZ : 0);
 }
 
+static int alpha_locprior_step(st_chain* c);
+
 extern "C" int st_update_alpha(st_chain* c) {
   if (!c) return ST_ERR_ARG;
-  if (!c->h.inferalpha) return seterr(c->ctx, ST_ERR_STATE, "UpdateAlpha needs INFERALPHA=1");
   cudaSetDevice(c->ctx->device);
+  if (c->h.lp_admix) return alpha_locprior_step(c);   // UpdateAlphaLocPrior
+  if (!c->h.inferalpha) return seterr(c->ctx, ST_ERR_STATE, "UpdateAlpha needs INFERALPHA=1");
   return ind(c, kIndNone, kIndAlpha);
 }
 
@@ -990,6 +1078,28 @@ extern "C" int st_update_q_mala(st_chain* c) {
   return mala_step(c);
 }
 
+// UpdateLocPrior after the Q update (src/structure.c:535-537; with
+// UPDATELOCPRIOR=0 the kernels only add the sums) and, with admixture,
+// UpdateAlphaLocPrior in place of UpdateAlpha (src/structure.c:577-590).
+static int locprior_step(st_chain* c) {
+  Bracket br(c->ctx, ST_K_OTHER);
+  if (c->h.noadmix) c->ctx->launches++;   // two kernels
+  return cuda_check(c->ctx, launch_locprior(c->h, c->d_chain, c->ctx->stream), "locprior");
+}
+static int alpha_locprior_step(st_chain* c) {
+  Bracket br(c->ctx, ST_K_OTHER);
+  c->ctx->launches++;   // two kernels
+  return cuda_check(c->ctx, launch_alpha_locprior(c->h, c->d_chain, c->ctx->stream),
+                    "alpha locprior");
+}
+
+extern "C" int st_update_locprior(st_chain* c) {
+  if (!c) return ST_ERR_ARG;
+  if (!c->h.locprior) return seterr(c->ctx, ST_ERR_STATE, "UpdateLocPrior needs LOCPRIOR=1");
+  cudaSetDevice(c->ctx->device);
+  return locprior_step(c);
+}
+
 static int sweep_once(st_chain* c) {
   const int zflags = (c->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
                      (c->model.store_z ? kZfStoreZ : 0);
@@ -998,6 +1108,8 @@ static int sweep_once(st_chain* c) {
   if (!rc && c->h.inferlambda) rc = lambda_step(c);
   if (!rc && c->h.inferlambda) rc = locus(c, kLocEps | kLocFst | kLocCollect);
   if (!rc) rc = update_q_impl(c, kIndAlpha | kIndCollect);
+  if (!rc && c->h.locprior) rc = locprior_step(c);
+  if (!rc && c->h.lp_admix) rc = alpha_locprior_step(c);
   if (!rc && c->h.mala && c->h.K > 1) rc = mala_step(c);
   if (!rc) rc = zpass(c, kZNormal, zflags);
   if (!rc) c->host_rep++;
@@ -1059,8 +1171,9 @@ extern "C" size_t st_field_bytes(st_chain* c, int f) {
     case ST_F_Q: case ST_F_LOGQ: case ST_F_TESTQ: case ST_F_LOGTESTQ: return NK * 4;
     case ST_F_P: case ST_F_LOGP: return LKA * 4;
     case ST_F_EPS: case ST_F_SUMEPS: return LA * 8;
-    case ST_F_F: case ST_F_ALPHA: case ST_F_LAMBDA: case ST_F_FSTSUM: case ST_F_SUMALPHA:
-    case ST_F_SUMLAMBDA: return (size_t)h.K * 8;
+    case ST_F_F: case ST_F_LAMBDA: case ST_F_FSTSUM: case ST_F_SUMLAMBDA: return (size_t)h.K * 8;
+    case ST_F_ALPHA: case ST_F_SUMALPHA:
+      return (size_t)h.K * (h.lp_admix ? h.nloc + 1 : 1) * 8;
     case ST_F_Z: return (size_t)h.N * 2 * h.L;
     case ST_F_N: return LKA * 4;
     case ST_F_M: return NK * 4;
@@ -1073,6 +1186,8 @@ extern "C" size_t st_field_bytes(st_chain* c, int f) {
     case ST_F_DIMS: return 32;
     case ST_F_MALA_EPS: return h.mala ? (size_t)h.N * 4 : 0;
     case ST_F_USEPOPPROBS: return h.usepopinfo ? (size_t)h.N * h.K * (h.gensback + 1) * 8 : 0;
+    case ST_F_LOCPRIOR: case ST_F_SUMLOCPRIOR: return h.locprior ? (size_t)h.lp_len * 8 : 0;
+    case ST_F_MYLOC: return h.locprior ? (size_t)h.N * 4 : 0;
   }
   return 0;
 }
@@ -1102,6 +1217,9 @@ static void* field_ptr(st_chain* c, int f) {
     case ST_F_ERR: return h.err;
     case ST_F_MALA_EPS: return h.mEps;
     case ST_F_USEPOPPROBS: return h.usepop;
+    case ST_F_LOCPRIOR: return h.locp;
+    case ST_F_SUMLOCPRIOR: return h.sumlocp;
+    case ST_F_MYLOC: return (void*)h.myloc;
   }
   return nullptr;
 }
@@ -1171,7 +1289,7 @@ extern "C" int st_set_state(st_chain* c, int f, const void* host, size_t bytes) 
   cudaStream_t s = c->ctx->stream;
   ChainDev& h = c->h;
   if (f == ST_F_REP) return set_rep(c, *(const int32_t*)host);
-  if (f == ST_F_DIMS || f == ST_F_LOGDIFF)
+  if (f == ST_F_DIMS || f == ST_F_LOGDIFF || f == ST_F_MYLOC)
     return seterr(c->ctx, ST_ERR_ARG, "field %d is read-only", f);
   if (f == ST_F_N || f == ST_F_M) {
     // counts become partial slice 0; the other slices are cleared
@@ -1237,7 +1355,8 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
         c->host_rep != c0->host_rep || c->model.store_z != c0->model.store_z ||
         c->model.precision != c0->model.precision ||
         c->h.computeprob != c0->h.computeprob || c->h.noadmix != c0->h.noadmix ||
-        (c0->h.noadmix && (c->h.admburnin != c0->h.admburnin || c->h.burnin != c0->h.burnin))) {
+        (c0->h.noadmix && (c->h.admburnin != c0->h.admburnin || c->h.burnin != c0->h.burnin ||
+                           c->h.locprior != c0->h.locprior))) {
       delete b;
       return seterr(ctx, ST_ERR_ARG,
                     "batched chains must share the context, data path, METROFREQ, COMPUTEPROB, "
@@ -1386,6 +1505,12 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
       Bracket br(ctx, ST_K_IND);
       ST_CUDA(ctx, launch_ind(li, b->G, kIndGibbs, astage | kIndCollect, kBlockInd));
     }
+  }
+  for (st_chain* c : b->chains) {
+    if (c->h.locprior)
+      if (int rc = locprior_step(c)) return rc;
+    if (c->h.lp_admix)
+      if (int rc = alpha_locprior_step(c)) return rc;
   }
   for (st_chain* c : b->chains)
     if (c->h.mala && c->h.K > 1)
@@ -1573,21 +1698,28 @@ constexpr int32_t kCkptVersion = 1;
 
 struct CkField { void* p; size_t bytes; };
 
+// alpha values held: K, or K per row (global + locations) under LOCPRIOR
+size_t arow_n(const ChainDev& h) { return (size_t)h.K * (h.lp_admix ? h.nloc + 1 : 1); }
+
 std::vector<CkField> ckpt_fields(st_chain* c) {
   ChainDev& h = c->h;
   const size_t NK = (size_t)h.N * h.K, LKA = (size_t)h.L * h.K * h.A, LA = (size_t)h.L * h.A;
   std::vector<CkField> f = {
       {h.Q, NK * 4}, {h.logQ, NK * 4}, {h.TestQ, NK * 4}, {h.logTestQ, NK * 4},
       {h.P, LKA * 4}, {h.logP, LKA * 4}, {h.eps, LA * 8}, {h.F, (size_t)h.K * 8},
-      {h.alpha, (size_t)h.K * 8}, {h.lambda, (size_t)h.K * 8}, {h.npart, LKA * 4},
+      {h.alpha, arow_n(h) * 8}, {h.lambda, (size_t)h.K * 8}, {h.npart, LKA * 4},
       {h.mpart, NK * 4}, {h.ldpart, (size_t)h.ngroups * h.N * 8}, {h.QSum, NK * 8},
       {h.PSum, LKA * 8}, {h.SumEps, LA * 8}, {h.FstSum, (size_t)h.K * 8},
-      {h.sumAlpha, (size_t)h.K * 8}, {h.sumlambda, (size_t)h.K * 8},
+      {h.sumAlpha, arow_n(h) * 8}, {h.sumlambda, (size_t)h.K * 8},
       {h.stats, (size_t)kStSize * 8}, {h.err, 4}};
   if (h.Z) f.push_back({h.Z, (size_t)h.N * 2 * h.L});
   if (h.AncestDist) f.push_back({h.AncestDist, NK * (size_t)h.numboxes * 4});
   if (h.mala) f.push_back({h.mEps, (size_t)h.N * 4});
   if (h.usepopinfo) f.push_back({h.usepop, (size_t)h.N * h.K * (h.gensback + 1) * 8});
+  if (h.locprior) {
+    f.push_back({h.locp, (size_t)h.lp_len * 8});
+    f.push_back({h.sumlocp, (size_t)h.lp_len * 8});
+  }
   return f;
 }
 

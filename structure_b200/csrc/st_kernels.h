@@ -49,6 +49,12 @@ cudaError_t launch_noadmix(const ChainDev& h, const ChainDev* d_chain, cudaStrea
 // USEPOPINFO: migrant-model Q of individuals with prior population information
 void popinfo_plan(int N, int L, int* lchunks, int* lchunk_len);
 cudaError_t launch_popinfo(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
+
+// LOCPRIOR (st_locprior.cu): UpdateLocPrior (r, and nu / gamma without
+// admixture; also adds the LocPrior sums when collecting) and
+// UpdateAlphaLocPrior (global and location alphas, with their sums).
+cudaError_t launch_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
+cudaError_t launch_alpha_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
 
 // CTA counts per chain for each launch kind (host-side mirror of the tiling).

@@ -70,8 +70,11 @@ __global__ void __launch_bounds__(kNaBlock) noadmix_pick_kernel(const ChainDev* 
   if (i >= N || (ch.usepopinfo && ch.popflags[i])) return;
   double p[kMaxPops];
   double mx = 0.0;
+  // LOCPRIOR: the product starts at gamma of the individual's location
+  // (src/Updates/UpdateQ.c:339-345)
+  const double* gam = ch.locprior ? ch.locp + 1 + (size_t)K * (ch.myloc[i] + 1) : nullptr;
   for (int k = 0; k < K; k++) {
-    double s = 0.0;
+    double s = gam ? log(gam[k]) : 0.0;
     for (int c = 0; c < ch.na_lchunks; c++) s += ch.napart[((size_t)c * N + i) * K + k];
     p[k] = s;
     if (k == 0 || s > mx) mx = s;

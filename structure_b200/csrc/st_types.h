@@ -16,7 +16,7 @@ constexpr uint8_t kG8Missing = 0xFF;  // U8 genotype byte for a missing copy
 enum Stream : uint32_t {
   kSInitZ = 1, kSZ = 2, kSP = 3, kSQG = 4, kSQM = 5, kSQMA = 6,
   kSAlpha = 7, kSEps = 8, kSFst = 9, kSMala = 10, kSLambda = 11, kSNoAdmix = 12,
-  kSPopInfo = 13
+  kSPopInfo = 13, kSLocPrior = 14, kSLocAlpha = 15
 };
 
 // Device error word bits.
@@ -108,6 +108,16 @@ struct ChainDev {
   double* pipart;                       // [pi_lchunks][N][K][gensback+1]
   int pi_lchunks, pi_lchunk_len;
   const int32_t* initpop;               // [N] initial Z population or -1, or null
+  int noalpha;                          // USEPOPINFO with nobody unflagged: no alpha sums
+  // LOCPRIOR: locations 0..nloc-1 (myloc), the reference's LocPrior array
+  // locp ([0] r; no admixture: [1+k] nu, [1+K*(loc+1)+k] gamma) and, with
+  // admixture, alpha rows [nloc+1][K] (global first, then per location)
+  int locprior, lp_admix, updatelocprior, nloc, lp_len;
+  double locpriorstep, maxlocprior;
+  const int32_t* myloc;                 // [N]
+  const int32_t* loc_start;             // [nloc+1] individuals of each location in
+  const int32_t* loc_inds;              // [N]      loc_inds[loc_start[l] .. loc_start[l+1])
+  double *locp, *sumlocp;               // [lp_len]
   // optional Langevin move on Q (Z summed out)
   int mala;
   float mala_target;

@@ -359,7 +359,9 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
   if (mode == kIndGibbs || mode == kIndPropose) {
     double lg = -INFINITY;
     if (kvalid) {
-      double shape = ch.alpha[k];
+      // LOCPRIOR with admixture: the individual's location row of alpha
+      // (src/Updates/UpdateQ.c:255-257,409-413)
+      double shape = ch.alpha[(ch.lp_admix ? (size_t)(1 + ch.myloc[i]) * K : 0) + k];
       uint32_t stream = kSQM;
       if (mode == kIndGibbs) {
         int m = 0;
@@ -495,8 +497,10 @@ ind_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nc
     if (sHits && threadIdx.x == 0) atomicAdd(&ch.stats[kStMetroHits], (double)sHits);
     if (collect && tile == 0 && threadIdx.x == 0)
       for (int q = 0; q < K; q++) {
-        // src/output.c:79-83: no alpha sums under NOADMIX
-        if (!ch.inferalpha && !ch.noadmix) ch.sumAlpha[q] += ch.alpha[q];
+        // src/output.c:72-83: no alpha sums under NOADMIX or NOALPHA; with
+        // LOCPRIOR and admixture the location-alpha kernels add them
+        if (!ch.inferalpha && !ch.noadmix && !ch.noalpha && !ch.lp_admix)
+          ch.sumAlpha[q] += ch.alpha[q];
         ch.sumlambda[q] += ch.lambda[q];
       }
   }

@@ -7,6 +7,7 @@
 // of src/datain.c:65-333, alleles are recoded in order of first appearance
 // (src/datain.c:824-904), and OUTFILE_f carries the sections of
 // src/output.c:1354-1423 in the reference's text layout.
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstdarg>
@@ -190,6 +191,8 @@ struct stf_run {
   // USEPOPINFO (stf_check_pop_priors / stf_set_usepopprobs)
   bool noalpha = false;
   std::vector<double> usepop;   // [N][MAXPOPS][GENSBACK+1]
+  // LOCPRIOR (stf_set_locprior_sums): sumLocPrior, the reference's layout
+  std::vector<double> sumlocp;
 };
 
 namespace {
@@ -632,6 +635,35 @@ extern "C" int stf_check_pop_priors(stf_run* r, int32_t* dropped) {
   return STF_OK;
 }
 
+namespace {
+// Location ids in increasing order: location l of the engine is ids[l]
+// (src/Util.c:237-275 GetNumLocations; output.c:1009-1018 get_location_num).
+std::vector<int> location_ids(const stf_run* r) {
+  std::vector<int> ids;
+  for (const Individual& d : r->ind) ids.push_back(d.location);
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  return ids;
+}
+}  // namespace
+
+extern "C" int stf_num_locations(const stf_run* r) {
+  if (!r || !r->have_data) return STF_ERR_ARG;
+  return (int)location_ids(r).size();
+}
+
+extern "C" int stf_set_locprior_sums(stf_run* r, const double* sums, size_t n) {
+  if (!r || !r->have_data) return STF_ERR_ARG;
+  if (!sums) {
+    r->sumlocp.clear();
+    return STF_OK;
+  }
+  const size_t need = I(r, "NOADMIX") ? 1 + (size_t)I(r, "MAXPOPS") * (location_ids(r).size() + 1) : 1;
+  if (n != need) return fail(r, STF_ERR_ARG, "sumLocPrior: %zu values given, %zu expected", n, need);
+  r->sumlocp.assign(sums, sums + n);
+  return STF_OK;
+}
+
 extern "C" int stf_set_usepopprobs(stf_run* r, const double* usepop) {
   if (!r || !r->have_data) return STF_ERR_ARG;
   if (!usepop) {
@@ -839,6 +871,8 @@ void sums(const stf_run* r, Out& o, const Sums& s) {
       o.f("Mean value of ln likelihood = %1.1f\n", s.sumlikes / reps);
     }
   }
+  const bool locprior = I(r, "LOCPRIOR") != 0;
+  const std::vector<int> ids = locprior ? location_ids(r) : std::vector<int>();
   if (!I(r, "NOADMIX") && !r->noalpha && K > 1) {
     if (I(r, "POPALPHAS")) {
       o.f("\n");
@@ -846,6 +880,15 @@ void sums(const stf_run* r, Out& o, const Sums& s) {
         o.f("Mean value of alpha_%d       = %1.4f\n", k + 1, s.sumAlpha[k] / reps);
     } else {
       o.f("Mean value of alpha         = %1.4f\n", s.sumAlpha[0] / reps);
+    }
+    if (locprior) {
+      // src/output.c:1061-1071: rows of alpha after the global one
+      o.f("\nMean value of alpha_local for each location:\n");
+      for (size_t l = 0; l < ids.size(); l++) {
+        o.f("\tlocation %2i:", ids[l]);
+        for (int k = 0; k < K; k++) o.f("  %1.4f", s.sumAlpha[(size_t)K * (l + 1) + k] / reps);
+        o.f("\n");
+      }
     }
   }
   if (I(r, "INFERLAMBDA")) {
@@ -869,6 +912,22 @@ void sums(const stf_run* r, Out& o, const Sums& s) {
   if (I(r, "PFROMPOPFLAGONLY"))
     o.f("Allele frequencies updated using individuals with POPFLAG=1 ONLY.\n");
   o.f("\n");
+  if (locprior) {
+    // src/output.c:1120-1139
+    const double* sl = r->sumlocp.data();
+    o.f("Mean value of r = %1.4f\n", sl[0] / reps);
+    if (I(r, "NOADMIX")) {
+      o.f("Mean value of nu = ");
+      for (int k = 0; k < K; k++) o.f(" %1.4f", sl[1 + k] / reps);
+      o.f("\n");
+      o.f("Mean value of gamma for each location:\n");
+      for (size_t l = 0; l < ids.size(); l++) {
+        o.f("\tlocation %2i:", ids[l]);
+        for (int k = 0; k < K; k++) o.f("  %1.4f", sl[1 + (size_t)K * (l + 1) + k] / reps);
+        o.f("\n");
+      }
+    }
+  }
 }
 
 int missing_ind(const stf_run* r, int i) {
@@ -1065,6 +1124,8 @@ extern "C" int stf_write_results(stf_run* r, int rep, const double* QSum, const 
   if (rep - I(r, "BURNIN") < 1) return fail(r, STF_ERR_ARG, "no collected sweeps to report");
   if (I(r, "USEPOPINFO") && r->usepop.empty())
     return fail(r, STF_ERR_ARG, "USEPOPINFO=1: give the UsePopProbs sums (stf_set_usepopprobs)");
+  if (I(r, "LOCPRIOR") && r->sumlocp.empty())
+    return fail(r, STF_ERR_ARG, "LOCPRIOR=1: give the LocPrior sums (stf_set_locprior_sums)");
   const Sums s{rep, QSum, PSum, SumEpsilon, FstSum, sumAlpha, sumlambda, AncestDist, sumlikes,
                sumsqlikes};
   Out o;

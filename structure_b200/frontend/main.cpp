@@ -6,10 +6,12 @@
 // sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
 //
 // USEPOPINFO=1 runs the migrant model for individuals with prior population
-// information and prints its posterior in OUTFILE_f (src/output.c:800-829).
-// Options the GPU path does not implement (LINKAGE, LOCPRIOR,
-// RECESSIVEALLELES, PLOIDY other than 2) stop the program with a message
-// instead of running a different model.
+// information and prints its posterior in OUTFILE_f (src/output.c:800-829);
+// LOCPRIOR=1 uses the sampling locations (LOCDATA column, or the population
+// with LOCISPOP) and prints r, nu / gamma or the location alphas.
+// Options the GPU path does not implement (LINKAGE, RECESSIVEALLELES, PLOIDY
+// other than 2) stop the program with a message instead of running a
+// different model.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,7 +46,7 @@ int die(const char* what, const char* msg) {
 int main(int argc, char** argv) {
   stf_run* r = nullptr;
   if (stf_open(argc, argv, &r) != STF_OK) return die("parameters", stf_last_error(r));
-  const char* unsupported[] = {"LINKAGE", "LOCPRIOR", "RECESSIVEALLELES"};
+  const char* unsupported[] = {"LINKAGE", "RECESSIVEALLELES"};
   for (const char* k : unsupported)
     if (pi(r, k)) {
       fprintf(stderr, "%s=1 is not available on the GPU path.\n", k);
@@ -63,10 +65,10 @@ int main(int argc, char** argv) {
   stf_geno(r, geno.data(), na.data(), tr.data());
   for (int32_t& g : geno)
     if (g < 0) g = -9;   // the engine's missing code
-  std::vector<int32_t> popflag(N), pop(N), flag_before(N);
+  std::vector<int32_t> popflag(N), pop(N), flag_before(N), location(N);
   stf_individuals(r, nullptr, flag_before.data(), nullptr, nullptr, nullptr);
   if (stf_check_pop_priors(r, nullptr) != STF_OK) return die("parameters", stf_last_error(r));
-  stf_individuals(r, pop.data(), popflag.data(), nullptr, nullptr, nullptr);
+  stf_individuals(r, pop.data(), popflag.data(), location.data(), nullptr, nullptr);
   if (pi(r, "USEPOPINFO"))
     for (int i = 0; i < N; i++)
       if (!popflag[i] && (flag_before[i] || !pi(r, "POPFLAG")))
@@ -106,6 +108,7 @@ int main(int argc, char** argv) {
   d.num_alleles = na.data();
   d.popflags = popflag.data();
   d.population = pop.data();
+  if (pi(r, "LOCPRIOR")) d.location = location.data();
   rc = st_data_upload(ctx, &d, &data);
   if (rc != ST_OK) return die("GPU", st_last_error(ctx));
   st_model m;
@@ -139,6 +142,11 @@ int main(int argc, char** argv) {
   m.popflag_given = 1;   // the flags above already hold CheckPopPriors' result
   m.gensback = pi(r, "GENSBACK");
   m.migrprior = pd(r, "MIGRPRIOR");
+  m.locprior = pi(r, "LOCPRIOR");
+  m.updatelocprior = pi(r, "UPDATELOCPRIOR");
+  m.locpriorinit = pd(r, "LOCPRIORINIT");
+  m.maxlocprior = pd(r, "MAXLOCPRIOR");
+  m.locpriorstep = pd(r, "LOCPRIORSTEP");
   rc = st_chain_create(ctx, data, &m, (uint64_t)seed, &c);
   if (rc != ST_OK) return die("GPU", st_last_error(ctx));
 
@@ -171,19 +179,25 @@ int main(int argc, char** argv) {
     printf("\n");
   }
   const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A;
-  std::vector<double> QSum(NK), PSum(LKA), SumEps((size_t)L * A), FstSum(K), sumAlpha(K),
-      sumlambda(K);
+  std::vector<double> QSum(NK), PSum(LKA), SumEps((size_t)L * A), FstSum(K),
+      sumAlpha(st_field_bytes(c, ST_F_SUMALPHA) / 8), sumlambda(K);
   std::vector<int32_t> AD;
   st_get_state(c, ST_F_QSUM, QSum.data(), NK * 8);
   st_get_state(c, ST_F_PSUM, PSum.data(), LKA * 8);
   st_get_state(c, ST_F_SUMEPS, SumEps.data(), SumEps.size() * 8);
   st_get_state(c, ST_F_FSTSUM, FstSum.data(), K * 8);
-  st_get_state(c, ST_F_SUMALPHA, sumAlpha.data(), K * 8);
+  st_get_state(c, ST_F_SUMALPHA, sumAlpha.data(), sumAlpha.size() * 8);
   st_get_state(c, ST_F_SUMLAMBDA, sumlambda.data(), K * 8);
   st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
   if (m.ancestdist) {
     AD.resize(NK * (size_t)m.numboxes);
     st_get_state(c, ST_F_ANCESTDIST, AD.data(), AD.size() * 4);
+  }
+  if (m.locprior) {
+    std::vector<double> lp(st_field_bytes(c, ST_F_SUMLOCPRIOR) / 8);
+    st_get_state(c, ST_F_SUMLOCPRIOR, lp.data(), lp.size() * 8);
+    if (stf_set_locprior_sums(r, lp.data(), lp.size()) != STF_OK)
+      return die("output", stf_last_error(r));
   }
   if (m.usepopinfo) {
     std::vector<double> up(NK * (size_t)(m.gensback + 1));

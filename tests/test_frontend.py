@@ -49,6 +49,8 @@ def _front():
     L.stf_write_results.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.c_double,
                                     C.c_double]
     L.stf_check_pop_priors.argtypes = [vp, vp]
+    L.stf_num_locations.argtypes = [vp]
+    L.stf_set_locprior_sums.argtypes = [vp, vp, C.c_size_t]
     L.stf_set_usepopprobs.argtypes = [vp, vp]
     L.stf_close.argtypes = [vp]
     return L
@@ -110,6 +112,10 @@ class Ours:
         if "usepop" in z:
             self._up = f(z["usepop"])
             assert self.L.stf_set_usepopprobs(self.h, self._up.ctypes.data) == 0
+        if "sumLocPrior" in z:
+            self._lp = f(z["sumLocPrior"])
+            assert self.L.stf_set_locprior_sums(self.h, self._lp.ctypes.data, self._lp.size) == 0, \
+                self.L.stf_last_error(self.h)
         self._keep = {k: f(z[k]) for k in ("QSum", "PSum", "SumEps", "FstSum", "sumAlpha",
                                            "sumlambda")}
         ad = np.ascontiguousarray(z["AncestDist"], np.int32) if "AncestDist" in z else None
@@ -159,7 +165,7 @@ Basic Program Parameters
 #define LABEL     {label}     // (B) Input file contains individual labels
 #define POPDATA   {popdata}     // (B) Input file contains a population identifier
 #define POPFLAG   {popflag}     // (B) whether to use popinfo when USEPOPINFO==1
-#define LOCDATA   0     // (B) Input file contains a location identifier
+#define LOCDATA   {locdata}     // (B) Input file contains a location identifier
 #define PHENOTYPE 0     // (B)
 #define EXTRACOLS {extracols}     // (int) Number of additional columns
 #define MARKERNAMES      {markernames}  // (B) data file contains row of marker names
@@ -169,11 +175,13 @@ Basic Program Parameters
 
 EXTRA_TMPL = """EXTRA PARAMS (written by the test)
 #define NOADMIX     {noadmix} // (B)
+#define ADMBURNIN   {admburnin} // (int)
 #define LINKAGE     0 // (B)
 #define USEPOPINFO  {usepopinfo} // (B)
 #define MIGRPRIOR {migrprior} // (d)
 #define GENSBACK  {gensback} // (int)
-#define LOCPRIOR    0 //(B)
+#define LOCPRIOR    {locprior} //(B)
+#define LOCISPOP    {locispop} //(B)
 #define FREQSCORR   {freqscorr} // (B)
 #define ONEFST      {onefst} // (B)
 #define INFERALPHA  1 // (B)
@@ -205,7 +213,7 @@ def _scenario(d, **kw):
              missing=-9, onerow=0, label=1, popdata=1, popflag=0, extracols=0, markernames=1,
              mapdist=0, freqscorr=1, onefst=0, popalphas=0, updatefreq=0, printqhat=0,
              ancestdist=0, numboxes=100, seed=4242, noadmix=0, usepopinfo=0, migrprior=0.05,
-             gensback=2)
+             gensback=2, locdata=0, locprior=0, locispop=0, admburnin=50)
     p.update(kw)
     with open(os.path.join(d, "mainparams"), "w") as f:
         f.write(MAIN_TMPL.format(**p))
@@ -231,6 +239,8 @@ def _scenario(d, **kw):
             head.append(str(1 + i % 4))
         if p["popflag"]:
             head.append(str(i % 2))
+        if p["locdata"]:
+            head.append(str(3 * (i % 3) + 5))          # location ids 5, 8, 11
         head += ["7"] * p["extracols"]
         if p["onerow"]:
             rows.append(" ".join(head + [str(v) for v in g[i].T.reshape(-1)]))
@@ -250,6 +260,12 @@ def _random_sums(p, A, seed=1):
     z = dict(QSum=Q, PSum=P, SumEps=rng.random((L, A)) * reps, FstSum=rng.random(K) * 0.3 * reps,
              sumAlpha=rng.random(K) * reps, sumlambda=np.ones(K) * reps,
              sumlikes=-1234.56 * reps, sumsqlikes=1234.56 ** 2 * reps + 50.0 * (reps - 1))
+    if p["locprior"]:
+        nloc = 4 if p["locispop"] else 3               # populations 1..4 or locations 5, 8, 11
+        if not p["noadmix"]:
+            z["sumAlpha"] = rng.random(K * (nloc + 1)) * reps
+        n = 1 + K * (nloc + 1) if p["noadmix"] else 1
+        z["sumLocPrior"] = rng.random(n) * reps
     if p["usepopinfo"]:
         u = rng.dirichlet(np.ones(K * (p["gensback"] + 1)), N) * reps
         z["usepop"] = u.reshape(N, K, p["gensback"] + 1)
@@ -331,13 +347,16 @@ def test_data_matches_reference(tmp_path, layout):
 OUTPUTS = [dict(), dict(freqscorr=0, popalphas=1), dict(onefst=1, printqhat=1),
            dict(ancestdist=1, label=0), dict(popdata=0, markernames=0, K=2),
            dict(usepopinfo=1, popflag=1, migrprior=0.1), dict(usepopinfo=1, gensback=1),
-           dict(usepopinfo=1, K=4, ancestdist=1), dict(noadmix=1)]
+           dict(usepopinfo=1, K=4, ancestdist=1), dict(noadmix=1),
+           dict(locprior=1, locdata=1), dict(locprior=1, locdata=1, noadmix=1, popalphas=1),
+           dict(locprior=1, locispop=1, noadmix=1)]
 
 
 @needs_ref
 @pytest.mark.parametrize("opts", OUTPUTS, ids=["f", "indep-popalphas", "onefst-qhat", "ancest",
                                                 "nopop", "usepop-flags", "usepop-all",
-                                                "usepop-noalpha", "noadmix"])
+                                                "usepop-noalpha", "noadmix", "locprior",
+                                                "locprior-noadmix", "locispop"])
 def test_results_file_matches_reference_byte_for_byte(tmp_path, opts):
     d = str(tmp_path)
     p = _scenario(d, **opts)

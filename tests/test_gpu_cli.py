@@ -29,11 +29,13 @@ def _snp_data(d, p):
         f.write("\n".join(rows) + "\n")
 
 
-@pytest.mark.parametrize("kind", ["microsat", "snp", "usepopinfo"])
+@pytest.mark.parametrize("kind", ["microsat", "snp", "usepopinfo", "locprior", "locprior-noadmix"])
 def test_cli_run_writes_results(tmp_path, kind):
     d = str(tmp_path)
     if kind == "usepopinfo":
         return _usepopinfo_run(d)
+    if kind.startswith("locprior"):
+        return _locprior_run(d, kind.endswith("noadmix"))
     if kind == "microsat":
         p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200)
     else:
@@ -90,3 +92,27 @@ def _usepopinfo_run(d):
         else:
             q = [float(x) for x in body.split()[:3]]
             assert sum(q) == pytest.approx(1.0, abs=0.003)
+
+
+def _locprior_run(d, noadmix):
+    """LOCPRIOR=1 with a LOCDATA column (location ids 5, 8, 11)."""
+    p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200, locprior=1,
+                  locdata=1, noadmix=int(noadmix))
+    r = subprocess.run([CLI, "-D", "11"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    text = open(os.path.join(d, "results_f")).read()
+    assert "LOCPRIOR model used" in text
+    rv = float(re.search(r"Mean value of r = (\S+)", text).group(1))
+    assert 0 < rv < 20                                   # MAXLOCPRIOR
+    if noadmix:
+        assert "NO ADMIXTURE model assumed" in text
+        nu = [float(x) for x in re.search(r"Mean value of nu = (.*)$", text, re.M).group(1).split()]
+        assert len(nu) == 3 and sum(nu) == pytest.approx(1.0, abs=1e-3)
+        rows = re.findall(r"^\tlocation\s+(\d+):((?:\s+[0-9.]+){3})$", text, re.M)
+        assert [int(x) for x, _ in rows] == [5, 8, 11]
+        for _, g in rows:
+            assert sum(float(v) for v in g.split()) == pytest.approx(1.0, abs=1e-3)
+    else:
+        assert "Mean value of alpha_local for each location:" in text
+        rows = re.findall(r"^\tlocation\s+(\d+):((?:\s+[0-9.]+){3})$", text, re.M)
+        assert [int(x) for x, _ in rows] == [5, 8, 11]

@@ -41,11 +41,14 @@ def _align(Qm, Qtrue):
 
 def _summaries(sumlikes, sumsqlikes, QSum, sumAlpha, FstSum, n, Qtrue):
     out = {"lnL_mean": [], "lnL_var": [], "alpha": [], "F": [], "Q": []}
+    K = QSum.shape[2]
     for c in range(len(sumlikes)):
         m = sumlikes[c] / n
         out["lnL_mean"].append(m)
         out["lnL_var"].append(sumsqlikes[c] / n - m * m)
-        out["alpha"].append(sumAlpha[c][0] / n)
+        # one alpha, or (LOCPRIOR) the mean of the global row over populations,
+        # which does not depend on the chain's labels
+        out["alpha"].append(sumAlpha[c][:K].mean() / n)
         perm = _align(QSum[c] / n, Qtrue)
         out["Q"].append(QSum[c][:, perm] / n)
         out["F"].append(FstSum[c][perm] / n)
@@ -63,13 +66,14 @@ def _run_device(ctx, z, model, mala=0):
     R = len(z["sumlikes"])
     data = api.Data(ctx, z["numalleles"], geno=geno,
                     popflags=z["popflags"] if "popflags" in z.files else None,
-                    population=z["population"] if "population" in z.files else None)
+                    population=z["population"] if "population" in z.files else None,
+                    location=z["location"] if "location" in z.files else None)
     mk = dict(maxpops=K, burnin=model["burnin"], numreps=model["numreps"],
               freqscorr=model["freqscorr"], inferalpha=model["inferalpha"], alpha=model["alpha"],
               alphapropsd=model["alphapropsd"], metrofreq=model["metrofreq"],
               lambda_=model["lambda_"], mala=mala)
     for k in ("fpriormean", "fpriorsd", "inferlambda", "noadmix", "admburnin", "usepopinfo",
-              "gensback", "migrprior"):
+              "gensback", "migrprior", "locprior"):
         if k in model:
             mk[k] = model[k]
     if "popflag" in model:
@@ -78,7 +82,7 @@ def _run_device(ctx, z, model, mala=0):
     b = api.Batch(ctx, chains)
     b.sweep(model["burnin"] + model["numreps"])
     res = dict(sumlikes=[], sumsqlikes=[], QSum=[], sumAlpha=[], FstSum=[], sumlambda=[],
-               usepop=[])
+               usepop=[], sumLocPrior=[])
     for c in chains:
         assert c.sync() == 0
         if mala:
@@ -94,6 +98,8 @@ def _run_device(ctx, z, model, mala=0):
         res["sumlambda"].append(c.get(api.F_SUMLAMBDA))
         if model.get("usepopinfo"):
             res["usepop"].append(c.get(api.F_USEPOPPROBS))
+        if model.get("locprior"):
+            res["sumLocPrior"].append(c.get(api.F_SUMLOCPRIOR))
     b.close()
     for c in chains:
         c.close()
@@ -101,8 +107,8 @@ def _run_device(ctx, z, model, mala=0):
     return {k: np.array(v) for k, v in res.items()}
 
 
-@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c1n", 0), ("c1p", 0), ("c2s", 0),
-                                       ("c2s", 1)])
+@pytest.mark.parametrize("name,mala", [("c1", 0), ("c1l", 0), ("c1n", 0), ("c1p", 0),
+                                       ("c1lp", 0), ("c1nlp", 0), ("c2s", 0), ("c2s", 1)])
 def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
     """mala=1: the same chains with the Langevin move on Q added to every
     sweep still sample the reference's posterior."""
@@ -138,6 +144,11 @@ def test_whole_runs_agree_with_reference_within_mcse(ctx, name, mala):
         zu = _z(ud, ur, floor=0.002)
         print("  P(home)  ", ud.mean(), ur.mean(), "max z", zu.max())
         assert zu.max() <= 6.0
+    if model.get("locprior"):
+        # r, the concentration of the location priors (LocPrior[0])
+        rd, rr = dev["sumLocPrior"][:, 0] / n, z["sumLocPrior"][:, 0] / n
+        print("  r        ", rd.mean(), rr.mean(), "z", float(_z(rd, rr)))
+        assert _z(rd, rr) <= 5.0, (rd.mean(), rr.mean())
     zq = _z(sd["Q"], sr["Q"], floor=0.002)
     assert zq.max() <= 6.0, zq.max()
     assert np.abs(sd["Q"].mean(0) - sr["Q"].mean(0)).mean() <= 0.01

@@ -437,3 +437,116 @@ def test_update_q_withpops_matches_reference(orc, ref, gensback, migr):
     np.testing.assert_array_equal(Qo[~f], Q0[~f])
     np.testing.assert_allclose(upo.reshape(-1), up, rtol=1e-9, atol=1e-12)
     assert (Qr[f] < 1).any() or gensback == 0
+
+
+def _locations(rng, N, nloc_ids):
+    """Raw location ids with gaps (GetNumLocations compacts them, in
+    increasing order of id) and the expected myloc."""
+    ids = np.sort(rng.choice(np.arange(0, 3 * nloc_ids), nloc_ids, replace=False))
+    loc = ids[rng.integers(0, nloc_ids, N)].astype(np.int32)
+    loc[:nloc_ids] = ids                      # every id used
+    myloc = np.searchsorted(ids, loc).astype(np.int32)
+    return loc, myloc
+
+
+@pytest.mark.parametrize("noadmix", [0, 1])
+def test_update_locprior_matches_reference(orc, ref, noadmix):
+    """UpdateLocPrior (src/Updates/UpdateLocPrior.c: r, nu and gamma with no
+    admixture, r alone with admixture) fed the rand() words the oracle used,
+    in the reference's order: the same moves, bit for bit, over 30 sweeps of
+    proposals that are accepted and rejected."""
+    K, N = 4, 90
+    rng = np.random.default_rng(40 + noadmix)
+    loc, myloc = _locations(rng, N, 6)
+    nloc = int(myloc.max()) + 1
+    ref.set_globals(N=N, L=1, K=K, noadmix=noadmix, locprior=1, alphapropsd=0.05,
+                    maxlocprior=20.0, locpriorstep=0.4)
+    inds, n_ref = ref.individuals_loc(N, loc)      # GetNumLocations reads NUMINDS
+    assert n_ref == nloc
+    moves = 0
+    for trial in range(30):
+        if noadmix:
+            Q = np.eye(K)[rng.integers(0, K, N)].astype(np.float32)
+            locp = np.concatenate([[rng.uniform(0.3, 4.0)], rng.dirichlet(np.ones(K) * 3),
+                                   rng.dirichlet(np.ones(K) * 2, nloc).reshape(-1)])
+        else:
+            Q = rng.dirichlet(np.ones(K), N).astype(np.float32)
+            locp = np.array([rng.uniform(0.3, 4.0)])
+        alpha = rng.uniform(0.2, 2.0, (nloc + 1) * K)
+        mine, words, normals = orc.update_locprior(myloc, Q, alpha, locp, noadmix, 0.05, 0.4,
+                                                   20.0, KEY, 100 + trial)
+        assert len(normals) == 0
+        theirs = locp.copy()
+        ref.rand_queue(words)
+        ref.lib.UpdateLocPrior(Q.astype(np.float64), theirs, alpha.copy(), inds)
+        assert ref.lib.stref_rand_consumed() == len(words)
+        assert ref.lib.stref_rand_overrun() == 0
+        ref.rand_queue(None)
+        np.testing.assert_array_equal(mine, theirs)
+        moves += int(np.sum(mine != locp))
+    assert moves > 10
+
+
+def test_update_alpha_locprior_matches_reference(orc, ref):
+    """UpdateAlphaLocPrior (src/Updates/UpdateAlpha.c:257-305): global
+    alphas, then each location's alphas against the Q of its individuals,
+    fed the oracle's normals and rand() words: the same alphas, bit for
+    bit."""
+    K, N = 3, 80
+    rng = np.random.default_rng(77)
+    loc, myloc = _locations(rng, N, 5)
+    nloc = int(myloc.max()) + 1
+    ref.set_globals(N=N, L=1, K=K, noadmix=0, locprior=1, alphapropsd=0.3, alphamax=10.0)
+    inds, n_ref = ref.individuals_loc(N, loc)
+    assert n_ref == nloc
+    moved = 0
+    for trial in range(25):
+        Q = rng.dirichlet(np.full(K, 0.8), N)
+        alpha = rng.uniform(0.2, 3.0, (nloc + 1) * K)
+        r = rng.uniform(0.5, 5.0)
+        mine, words, normals = orc.update_alpha_locprior(myloc, np.log(Q), alpha, r, 0.3, 10.0,
+                                                         KEY, 300 + trial)
+        theirs = alpha.copy()
+        ref.normal_queue(normals)
+        ref.rand_queue(words)
+        ref.lib.UpdateAlphaLocPrior(Q.copy(), theirs, np.array([r]), inds)
+        assert ref.lib.stref_rand_consumed() == len(words)
+        assert ref.lib.stref_normal_consumed() == len(normals) == (nloc + 1) * K
+        ref.rand_queue(None)
+        ref.normal_queue(None)
+        np.testing.assert_array_equal(mine, theirs)
+        moved += int(np.sum(mine != alpha))
+    assert moved > 20
+
+
+def test_q_updates_with_location_priors_match_reference(orc, ref):
+    """LOCPRIOR in the Q updates: UpdateQNoAdmix starts each individual's
+    product at gamma of its location (src/Updates/UpdateQ.c:339-345)."""
+    from oracle.oracle import S_NOADMIX
+    d = synth.microsat(N=60, L=40, K=3, seed=8)
+    geno, na = d["geno"], d["numalleles"].astype(np.int32)
+    N, _, L = geno.shape
+    K, A = 3, int(na.max())
+    rng = np.random.default_rng(9)
+    loc, myloc = _locations(rng, N, 4)
+    nloc = int(myloc.max()) + 1
+    P = np.zeros((L, K, A))
+    for l in range(L):
+        P[l, :, :na[l]] = rng.dirichlet(np.full(na[l], 0.4), K)
+    logP = np.log(np.maximum(P, 1e-300)).astype(np.float32)
+    Pd = np.where(P > 0, np.exp(logP.astype(np.float64)), 0.0)
+    # strong location priors so that they change picks
+    locp = np.concatenate([[1.0], np.ones(K) / K, rng.dirichlet(np.ones(K) * 0.3, nloc).reshape(-1)])
+    key, rep = 0x5151, 4
+    Qo, _, pick = orc.update_q_noadmix(geno, logP, key, rep, locp=locp, myloc=myloc)
+    _, _, pick0 = orc.update_q_noadmix(geno, logP, key, rep)
+    words = [int(orc.stream(i, 0, rep, S_NOADMIX, key)[0]) >> 1 for i in range(N)]
+    ref.set_globals(N=N, L=L, K=K, maxalleles=A, noadmix=1, locprior=1)
+    inds, n_ref = ref.individuals_loc(N, loc)
+    assert n_ref == nloc
+    Qr = np.zeros((N, K))
+    ref.rand_queue(words)
+    ref.lib.UpdateQNoAdmix(geno.copy(), Qr, Pd.copy(), inds, locp.ctypes.data, None)
+    ref.rand_queue(None)
+    np.testing.assert_array_equal(Qr.argmax(1), pick)
+    assert (pick != pick0).any()
