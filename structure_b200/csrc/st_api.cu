@@ -397,6 +397,40 @@ extern "C" int st_ctx_memory(const st_ctx* ctx, size_t* in_use, size_t* budget) 
 
 // ===========================================================================
 // data
+// Allele counts of each locus of 2-bit packed data, 16 genotypes per word:
+// with lo / hi the low / high bit of every code, popcounts give the number
+// of codes 1 (lo & ~hi), 2 (hi & ~lo) and 3 = missing (lo & hi).  Built
+// twice: with the popcnt instruction where the host has it, else generic.
+namespace {
+template <int kTag>
+__attribute__((always_inline)) inline void count_b2g(const uint32_t* packed, int N, int L, int A, int64_t* cnt, int64_t* tot) {
+  const int wpr = (N + 15) / 16;
+  const uint32_t tail = (N & 15) ? (0x55555555u >> (2 * (16 - (N & 15)))) : 0x55555555u;
+  for (int l = 0; l < L; l++) {
+    const uint32_t* row = packed + (size_t)l * wpr;
+    int64_t n1 = 0, n2 = 0, n3 = 0;
+    for (int w = 0; w < wpr; w++) {
+      const uint32_t valid = w == wpr - 1 ? tail : 0x55555555u;
+      const uint32_t lo = row[w] & valid, hi = (row[w] >> 1) & valid;
+      n1 += __builtin_popcount(lo & ~hi);
+      n2 += __builtin_popcount(hi & ~lo);
+      n3 += __builtin_popcount(lo & hi);
+    }
+    const int64_t n0 = (int64_t)N - n1 - n2 - n3;
+    tot[l] = 2 * (n0 + n1 + n2);
+    cnt[(size_t)l * A + 0] = 2 * n0 + n1;
+    if (A > 1) cnt[(size_t)l * A + 1] = 2 * n2 + n1;
+  }
+}
+__attribute__((target("popcnt"))) void count_b2g_popcnt(const uint32_t* p, int N, int L, int A,
+                                                        int64_t* cnt, int64_t* tot) {
+  count_b2g<1>(p, N, L, A, cnt, tot);
+}
+void count_b2g_generic(const uint32_t* p, int N, int L, int A, int64_t* cnt, int64_t* tot) {
+  count_b2g<0>(p, N, L, A, cnt, tot);
+}
+}  // namespace
+
 // ===========================================================================
 extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out) {
   if (!ctx || !d || !out) return ST_ERR_ARG;
@@ -456,15 +490,8 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
       delete s;
       return seterr(ctx, ST_ERR_ARG, "packed genotypes need <= 2 alleles per locus");
     }
-    const int wpr = (N + 15) / 16;
-    for (int l = 0; l < L; l++)
-      for (int i = 0; i < N; i++) {
-        uint32_t g = (d->packed[(size_t)l * wpr + (i >> 4)] >> (2 * (i & 15))) & 3u;
-        if (g == 3u) continue;
-        s->tot_h[l] += 2;
-        s->cnt_h[(size_t)l * A + 0] += (g == 0) ? 2 : (g == 1 ? 1 : 0);
-        if (A > 1) s->cnt_h[(size_t)l * A + 1] += (g == 2) ? 2 : (g == 1 ? 1 : 0);
-      }
+    if (__builtin_cpu_supports("popcnt")) count_b2g_popcnt(d->packed, N, L, A, s->cnt_h.data(), s->tot_h.data());
+    else count_b2g_generic(d->packed, N, L, A, s->cnt_h.data(), s->tot_h.data());
   }
   int layout = d->layout;
   if (layout == ST_LAYOUT_AUTO) layout = b2g_ok ? ST_LAYOUT_B2G : ST_LAYOUT_U8;
@@ -784,9 +811,19 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
       bufs.push_back(b);
   }
   if (model->ancestdist) bufs.push_back({&AD, NK * (size_t)h.numboxes * 4});
-  for (auto& b : bufs) {
-    rc = ctx_alloc(ctx, b.bytes, b.p, &c->allocs, &c->bytes);
-    if (rc) { st_chain_destroy(c); return rc; }
+  // one device allocation per chain, carved into 256-byte aligned arrays
+  // (a few dozen cudaMalloc calls would dominate the chain's creation time)
+  size_t arena = 0;
+  for (auto& b : bufs) arena += (b.bytes + 255) & ~(size_t)255;
+  void* base = nullptr;
+  rc = ctx_alloc(ctx, arena, &base, &c->allocs, &c->bytes);
+  if (rc) { st_chain_destroy(c); return rc; }
+  {
+    char* at = (char*)base;
+    for (auto& b : bufs) {
+      *b.p = b.bytes ? (void*)at : nullptr;
+      at += (b.bytes + 255) & ~(size_t)255;
+    }
   }
   h.Q = (float*)Q; h.logQ = (float*)logQ; h.TestQ = (float*)TQ; h.logTestQ = (float*)lTQ;
   h.P = (float*)P; h.logP = (float*)logP; h.eps = (double*)eps; h.F = (double*)F;
