@@ -260,7 +260,7 @@ int zpass(st_chain* c, int mode, int flags) {
 int locus(st_chain* c, int stages) {
   Bracket br(c->ctx, ST_K_LOCUS);
   LaunchSet ls = single(c, ctas_locus(c->h, kBlockLoc));
-  return cuda_check(c->ctx, launch_locus(ls, c->h.G, stages, kBlockLoc), "locus");
+  return cuda_check(c->ctx, launch_locus(ls, stages, kBlockLoc), "locus");
 }
 
 int ind(st_chain* c, int mode, int stages) {
@@ -1495,15 +1495,14 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
   for (st_chain* c : b->chains) lam = lam || c->h.inferlambda;
   {
     Bracket br(ctx, ST_K_LOCUS);
-    ST_CUDA(ctx, launch_locus(ll, b->G, lam ? kLocP : kLocP | kLocEps | kLocFst | kLocCollect,
-                              kBlockLoc));
+    ST_CUDA(ctx, launch_locus(ll, lam ? kLocP : kLocP | kLocEps | kLocFst | kLocCollect, kBlockLoc));
   }
   if (lam) {
     for (st_chain* c : b->chains)
       if (c->h.inferlambda)
         if (int rc = lambda_step(c)) return rc;
     Bracket br(ctx, ST_K_LOCUS);
-    ST_CUDA(ctx, launch_locus(ll, b->G, kLocEps | kLocFst | kLocCollect, kBlockLoc));
+    ST_CUDA(ctx, launch_locus(ll, kLocEps | kLocFst | kLocCollect, kBlockLoc));
   }
   for (st_chain* c : b->chains)
     if (c->h.usepopinfo)

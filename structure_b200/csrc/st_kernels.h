@@ -39,7 +39,7 @@ int zpass_b2g_width(int KT);   // CTA width (warps) of the fast path for a K cla
 cudaError_t launch_zpass_b2g(const LaunchSet& ls, int KT, int W, int mode, int flags,
                              size_t smem);
 cudaError_t launch_zpass_u8(const LaunchSet& ls, int mode, int flags);
-cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block);
+cudaError_t launch_locus(const LaunchSet& ls, int stages, int block);
 cudaError_t launch_ind(const LaunchSet& ls, int G, int mode, int stages, int block);
 cudaError_t launch_collect(const LaunchSet& ls, int block);
 cudaError_t launch_lambda(const LaunchSet& ls, int block);

@@ -1,6 +1,6 @@
 // st_update.cu -- the per-locus and per-individual updates of a sweep.
 //
-// Locus kernel (G lanes per locus, lane k = population k):
+// Locus kernel (one thread per locus, a loop over the populations):
 //   P   : P[l][k][.] ~ Dirichlet(prior + n[l][k][.])        Updates/UpdateP.c:106-199
 //   eps : two-allele shift Metropolis on eps[l][.]           Updates/UpdateEpsilon.c:71-145
 //   F   : per-locus terms of FlikeFreqs(F') - FlikeFreqs(F), reduced over loci,
@@ -35,155 +35,159 @@ __device__ __forceinline__ void warp_slot_sums(double v, int G, double* s, int n
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Locus kernel
+// Locus kernel: one thread per locus, looping over the populations (every
+// lane busy whatever K is).  The per-population constants of the sweep --
+// (1-F_k)/F_k and the F proposals -- are formed once per CTA in shared memory.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 3)
 locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
-             int G, int stages) {
+             int stages) {
   __shared__ double sF[8 * kMaxPops];
   __shared__ double sTot[kMaxPops];
+  __shared__ double sFrac[kMaxPops];   // (1 - F_k) / F_k
+  __shared__ double sNF[kMaxPops];     // proposed F_j (F stage)
   const int c = find_chain(prefix, nchains, blockIdx.x);
   ChainDev& ch = chains[c];
   const int tile = blockIdx.x - prefix[c];
   const int L = ch.L, K = ch.K, A = ch.A;
-  const int gpb = blockDim.x / G;
-  const int gid = threadIdx.x / G, k = threadIdx.x - gid * G;
-  const int l = tile * gpb + gid;
+  const int l = tile * blockDim.x + threadIdx.x;
   const bool lvalid = l < L;
-  const bool kvalid = lvalid && k < K;
   const int rep = *ch.rep;
   const uint32_t key = ch.key;
   const bool collect = (stages & kLocCollect) && (rep + 1 > ch.burnin);
   const int na = lvalid ? ch.numalleles[l] : 0;
-  const size_t base = ((size_t)(lvalid ? l : 0) * K + (k < K ? k : 0)) * A;
+  const bool fstage = (stages & kLocFst) && ch.freqscorr;
+  const int numfst = ch.onefst ? 1 : K;
+  if (ch.freqscorr && (stages & (kLocP | kLocEps | kLocFst))) {
+    if (threadIdx.x < K) sFrac[threadIdx.x] = (1.0 - ch.F[threadIdx.x]) / ch.F[threadIdx.x];
+    if (fstage && threadIdx.x < numfst)
+      sNF[threadIdx.x] = ch.F[threadIdx.x] +
+          ch.fpriorsd * normal_draw((uint32_t)threadIdx.x, (uint32_t)rep, kSFst, key);
+    __syncthreads();
+  }
   int errb = 0;
 
   // ---- P ------------------------------------------------------------------
-  if ((stages & kLocP) && kvalid && na > 0) {
-    auto shape_of = [&](int a) {
-      int n = 0;
-      for (int cc = 0; cc < ch.cnt_chunks; cc++)
-        n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
-      if (ch.freqscorr)
-        return ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
-      return ch.lambda[k] + (double)n;
-    };
-    auto emit = [&](int a, double lg, double ls, int nac) {
-      double lp, p;
-      if (ls < kLogUnderflo) {
-        p = 1.0 / (double)nac;
-        lp = -log((double)nac);
+  if ((stages & kLocP) && lvalid && na > 0) {
+    for (int k = 0; k < K; k++) {
+      const size_t base = ((size_t)l * K + k) * A;
+      auto shape_of = [&](int a) {
+        int n = 0;
+        for (int cc = 0; cc < ch.cnt_chunks; cc++)
+          n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
+        if (ch.freqscorr) return ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
+        return ch.lambda[k] + (double)n;
+      };
+      auto emit = [&](int a, double lg, double ls, int nac) {
+        double lp, p;
+        if (ls < kLogUnderflo) {
+          p = 1.0 / (double)nac;
+          lp = -log((double)nac);
+        } else {
+          lp = lg - ls;
+          p = exp(lp);
+        }
+        const float pf = (float)p;
+        ch.P[base + a] = pf;
+        ch.logP[base + a] = (float)lp;
+        if (collect) ch.PSum[base + a] += (double)pf;
+        if (!(pf == pf)) errb |= kErrNaN;
+      };
+      if (na <= 2) {
+        // biallelic (and monomorphic) loci stay in registers
+        const double lg0 = log_gamma_draw(shape_of(0), (uint32_t)base, (uint32_t)rep, kSP, key, &errb);
+        const double lg1 = na > 1 ? log_gamma_draw(shape_of(1), (uint32_t)(base + 1), (uint32_t)rep,
+                                                   kSP, key, &errb)
+                                  : -INFINITY;
+        const double M = (na > 1 && lg1 > lg0) ? lg1 : lg0;
+        double S = exp(lg0 - M);
+        if (na > 1) S += exp(lg1 - M);
+        const double ls = M + log(S);
+        emit(0, lg0, ls, na);
+        if (na > 1) emit(1, lg1, ls, na);
       } else {
-        lp = lg - ls;
-        p = exp(lp);
+        double lg[kMaxAlleles];
+        const int nac = na < kMaxAlleles ? na : kMaxAlleles;
+        if (na > kMaxAlleles) errb |= kErrBounds;
+        for (int a = 0; a < nac; a++)
+          lg[a] = log_gamma_draw(shape_of(a), (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+        double M = lg[0];
+        for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
+        double S = 0.0;
+        for (int a = 0; a < nac; a++) S += exp(lg[a] - M);
+        const double ls = M + log(S);
+        for (int a = 0; a < nac; a++) emit(a, lg[a], ls, nac);
       }
-      const float pf = (float)p;
-      ch.P[base + a] = pf;
-      ch.logP[base + a] = (float)lp;
-      if (collect) ch.PSum[base + a] += (double)pf;
-      if (!(pf == pf)) errb |= kErrNaN;
-    };
-    if (na <= 2) {
-      // biallelic (and monomorphic) loci stay in registers
-      const double lg0 = log_gamma_draw(shape_of(0), (uint32_t)base, (uint32_t)rep, kSP, key, &errb);
-      const double lg1 = na > 1 ? log_gamma_draw(shape_of(1), (uint32_t)(base + 1), (uint32_t)rep,
-                                                 kSP, key, &errb)
-                                : -INFINITY;
-      const double M = (na > 1 && lg1 > lg0) ? lg1 : lg0;
-      double S = exp(lg0 - M);
-      if (na > 1) S += exp(lg1 - M);
-      const double ls = M + log(S);
-      emit(0, lg0, ls, na);
-      if (na > 1) emit(1, lg1, ls, na);
-    } else {
-      double lg[kMaxAlleles];
-      const int nac = na < kMaxAlleles ? na : kMaxAlleles;
-      if (na > kMaxAlleles) errb |= kErrBounds;
-      for (int a = 0; a < nac; a++)
-        lg[a] = log_gamma_draw(shape_of(a), (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
-      double M = lg[0];
-      for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
-      double S = 0.0;
-      for (int a = 0; a < nac; a++) S += exp(lg[a] - M);
-      const double ls = M + log(S);
-      for (int a = 0; a < nac; a++) emit(a, lg[a], ls, nac);
     }
   }
 
   // ---- eps ----------------------------------------------------------------
-  if ((stages & kLocEps) && ch.freqscorr) {
-    double t = 0.0;
-    bool inrange = false;
-    int a1 = 0, a2 = 0;
-    double e1 = 0.0, e2 = 0.0, d = 0.0;
-    if (lvalid && na > 1) {
+  if ((stages & kLocEps) && ch.freqscorr && lvalid) {
+    if (na > 1) {
       const U4 w = philox_s((uint32_t)l, 0, (uint32_t)rep, kSEps, key);
-      a1 = (int)(((double)(w.x >> 1) / 2147483648.0) * na);
-      a2 = (int)(((double)(w.y >> 1) / 2147483648.0) * (na - 1));
+      const int a1 = (int)(((double)(w.x >> 1) / 2147483648.0) * na);
+      int a2 = (int)(((double)(w.y >> 1) / 2147483648.0) * (na - 1));
       if (a2 >= a1) a2 += 1;
-      d = 0.0 + ((double)(w.z >> 1) / 2147483648.0) * (ch.invsqrtnuminds - 0.0);
-      e1 = ch.eps[(size_t)l * A + a1];
-      e2 = ch.eps[(size_t)l * A + a2];
-      inrange = (e1 + d < 1.0) && (e2 - d > 0.0);
-      if (inrange && k < K) {
-        const double frac = (1.0 - ch.F[k]) / ch.F[k];
-        const double lp1 = (double)ch.logP[base + a1];
-        const double lp2 = (double)ch.logP[base + a2];
-        double s = lanczos_lgamma_fast(frac * e1);
-        s += lanczos_lgamma_fast(frac * e2);
-        s -= lanczos_lgamma_fast(frac * (e1 + d));
-        s -= lanczos_lgamma_fast(frac * (e2 - d));
-        s += frac * d * lp1;
-        s -= frac * d * lp2;
-        t = s;
+      const double d = 0.0 + ((double)(w.z >> 1) / 2147483648.0) * (ch.invsqrtnuminds - 0.0);
+      const double e1 = ch.eps[(size_t)l * A + a1];
+      const double e2 = ch.eps[(size_t)l * A + a2];
+      if ((e1 + d < 1.0) && (e2 - d > 0.0)) {
+        double sum = 0.0;
+        for (int k = 0; k < K; k++) {
+          const double frac = sFrac[k];
+          const size_t base = ((size_t)l * K + k) * A;
+          const double lp1 = (double)ch.logP[base + a1];
+          const double lp2 = (double)ch.logP[base + a2];
+          double s = lanczos_lgamma_fast(frac * e1);
+          s += lanczos_lgamma_fast(frac * e2);
+          s -= lanczos_lgamma_fast(frac * (e1 + d));
+          s -= lanczos_lgamma_fast(frac * (e2 - d));
+          s += frac * d * lp1;
+          s -= frac * d * lp2;
+          sum += s;
+        }
+        const double lam = ch.lambda[0];
+        if (lam != 1.0) sum += log(pow((e1 + d) * (e2 - d) / e1 / e2, lam - 1.0));
+        const U4 u = philox_s((uint32_t)l, 1, (uint32_t)rep, kSEps, key);
+        if (rnd31(u) < exp(sum)) {
+          ch.eps[(size_t)l * A + a1] = e1 + d;
+          ch.eps[(size_t)l * A + a2] = e2 - d;
+        }
       }
     }
-    double sum = group_sum(t, G);
-    bool accept = false;
-    if (inrange) {
-      const double lam = ch.lambda[0];
-      if (lam != 1.0) sum += log(pow((e1 + d) * (e2 - d) / e1 / e2, lam - 1.0));
-      const U4 w = philox_s((uint32_t)l, 1, (uint32_t)rep, kSEps, key);
-      accept = rnd31(w) < exp(sum);
-    }
-    if (accept && k == 0) {
-      ch.eps[(size_t)l * A + a1] = e1 + d;
-      ch.eps[(size_t)l * A + a2] = e2 - d;
-    }
-    __syncwarp();
-    if (collect && k == 0 && lvalid)
+    if (collect)
       for (int a = 0; a < na; a++) ch.SumEps[(size_t)l * A + a] += ch.eps[(size_t)l * A + a];
   }
 
   // ---- F ------------------------------------------------------------------
-  if ((stages & kLocFst) && ch.freqscorr) {
-    const int numfst = ch.onefst ? 1 : K;
-    const int j = ch.onefst ? 0 : k;
-    double dsum = 0.0;
-    if (kvalid) {
-      const double oldf = ch.F[j];
-      const double nf = oldf + ch.fpriorsd * normal_draw((uint32_t)j, (uint32_t)rep, kSFst, key);
-      if (nf > 0.0 && nf < 1.0) {
-        const double nfr = (1.0 - nf) / nf, ofr = (1.0 - oldf) / oldf;
+  if (fstage) {
+    // per-warp sums of each proposal's locus terms, then CTA sums in warp order
+    const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto fterm = [&](int k, double nf) {
+      double v = 0.0;
+      if (lvalid && nf > 0.0 && nf < 1.0) {
+        const double nfr = (1.0 - nf) / nf, ofr = sFrac[k];
+        const size_t base = ((size_t)l * K + k) * A;
         for (int a = 0; a < na; a++) {
           const double e = ch.eps[(size_t)l * A + a];
           const double lp = (double)ch.logP[base + a];
-          dsum += (nfr - ofr) * e * lp - (lanczos_lgamma_fast(nfr * e) - lanczos_lgamma_fast(ofr * e));
+          v += (nfr - ofr) * e * lp - (lanczos_lgamma_fast(nfr * e) - lanczos_lgamma_fast(ofr * e));
         }
       }
+      return v;
+    };
+    for (int j = 0; j < numfst; j++) {
+      double v = 0.0;
+      if (ch.onefst) {
+        for (int k = 0; k < K; k++) v += fterm(k, sNF[0]);
+      } else {
+        v = fterm(j, sNF[j]);
+      }
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) sF[warp * numfst + j] = v;
     }
-    // per-warp slot sums (slot = proposal j), then CTA sums in warp order
-    const int nwarps = blockDim.x >> 5;
-    for (int idx = threadIdx.x; idx < nwarps * numfst; idx += blockDim.x) sF[idx] = 0.0;
     __syncthreads();
-    if (ch.onefst) {
-      for (int off = 1; off < 32; off <<= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
-      if ((threadIdx.x & 31) == 0) sF[threadIdx.x >> 5] = dsum;
-    } else {
-      warp_slot_sums(dsum, G, sF, numfst, k < K ? k : -1);
-    }
-    __syncthreads();
-    const int nblocks = (L + gpb - 1) / gpb;
+    const int nblocks = (L + blockDim.x - 1) / blockDim.x;
     if (threadIdx.x < numfst) {
       double s = 0.0;
       for (int w = 0; w < nwarps; w++) s += sF[w * numfst + threadIdx.x];
@@ -200,7 +204,7 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         const double m = ch.fpriormean, sd = ch.fpriorsd;
         for (int jj = 0; jj < numfst; jj++) {
           const double oldf = ch.F[jj];
-          const double nf = oldf + sd * normal_draw((uint32_t)jj, (uint32_t)rep, kSFst, key);
+          const double nf = sNF[jj];
           ch.stats[kStFstNew + jj] = nf;
           ch.stats[kStFstDiff + jj] = sTot[jj];
           if (!(nf > 0.0 && nf < 1.0)) { ch.stats[kStFstLpd + jj] = 0.0; continue; }
@@ -226,13 +230,10 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   if (errb) set_err(ch.err, errb);
 }
 
-int ctas_locus(const ChainDev& c, int block) {
-  const int gpb = block / c.G;
-  return (c.L + gpb - 1) / gpb;
-}
+int ctas_locus(const ChainDev& c, int block) { return (c.L + block - 1) / block; }
 
-cudaError_t launch_locus(const LaunchSet& ls, int G, int stages, int block) {
-  locus_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, G, stages);
+cudaError_t launch_locus(const LaunchSet& ls, int stages, int block) {
+  locus_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, stages);
   return cudaGetLastError();
 }
 
