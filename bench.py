@@ -223,6 +223,10 @@ def run_ours(args):
     chains = [api.Chain(ctx, data, api.model_defaults(**mk), 2000 + 1000 * rank + r)
               for r in range(B)]
     batch = api.Batch(ctx, chains)
+    # Z-pass tiles timed on these chains (st_batch_autotune); batches of the
+    # same shapes made later in the process (the e2e leg) start from them
+    batch.autotune()
+    tdims = chains[0].get(api.F_DIMS)
 
     # warm-up = burn-in
     batch.sweep(W)
@@ -324,7 +328,9 @@ def run_ours(args):
                    "model": "admixture + F model, alpha and F inferred, METROFREQ=10",
                    "genotypes": "2 bits/genotype, locus-major", "store_z": False,
                    "l2": f"no flush: per-sweep working set {(G + B * (per_chain + L * K * 2 * 12)) / 1e9:.2f} GB > 126 MB L2",
-                   "parallelism": f"{world} GPU x {B} chains (replicas)"},
+                   "parallelism": f"{world} GPU x {B} chains (replicas)",
+                   "z_tile": {"chunks_of_individuals": int(tdims[6]),
+                              "locus_groups": int(tdims[7]), "chosen_by": "st_batch_autotune"}},
         "z_updates_per_s": round(value * copies, 1),
         "plain": {"value": round(plain, 3), "unit": METRIC,
                   "path": "one chain per launch, same kernels"},

@@ -252,6 +252,15 @@ int st_batch_destroy(st_batch *b);
  * No reference counterpart (the reference enqueues every kernel per sweep,
  * src/structure.c:497-685).                                                  */
 int st_batch_graphs(st_batch *b, int enable);
+/* Z-pass tile autotuner (biallelic 2-bit path): for each K class of the
+ * batch, times candidate tiles (individuals per chunk x locus blocks per CTA)
+ * with `reps` Z passes each on the batch's own chains, keeps the fastest and
+ * remembers it for batches of the same chain shapes created later in this
+ * process (chains created with st_model.tile_t / tile_r set are left alone
+ * then).  Draws and counts do not depend on the tile; the chain state is left
+ * as it was.  Takes about a second on 20 chains of 2000 x 50,000.  No
+ * reference counterpart.                                                     */
+int st_batch_autotune(st_batch *b, int reps);
 
 /* ---- gradient of ln P(D|Q,P) -----------------------------------------------
  * No reference counterpart (the reference evaluates the likelihood only,

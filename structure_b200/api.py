@@ -97,6 +97,7 @@ def lib():
         "st_update_q_mala": ([vp], C.c_int),
         "st_update_lambda": ([vp], C.c_int),
         "st_update_locprior": ([vp], C.c_int),
+        "st_batch_autotune": ([vp, C.c_int], C.c_int),
         "st_chain_save": ([vp, C.c_char_p], C.c_int),
         "st_chain_load": ([vp, C.c_char_p], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
@@ -337,6 +338,10 @@ class Batch:
     def graphs(self, enable=True):
         """Replay captured CUDA graphs of the sweep (default on)."""
         self.ctx.check(lib().st_batch_graphs(self.h, int(enable)))
+
+    def autotune(self, reps=3):
+        """Time candidate Z-pass tiles on these chains and keep the fastest."""
+        self.ctx.check(lib().st_batch_autotune(self.h, int(reps)))
 
     def close(self):
         if self.h:

@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "stgpu.h"
 #include "st_kernels.h"
@@ -59,6 +61,8 @@ struct st_chain {
   size_t zsmem = 0;
   double* d_injected = nullptr;
   size_t injected_n = 0;
+  int tile_min_t = 0;      // Z-pass tiles the scratch was sized for: T >= tile_min_t,
+  int tile_min_r = 1;      // R >= tile_min_r (fast path; the autotuner stays inside)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   bool timed = false;
@@ -89,6 +93,8 @@ struct st_batch {
   cudaGraphExec_t gx[2] = {nullptr, nullptr};  // [Gibbs sweep, Metropolis sweep]
   int glaunches[2] = {0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<ChainDev> table;             // host copies of the device tables
+  std::vector<int> pz, pl, pi;
 };
 
 namespace {
@@ -753,7 +759,16 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   h.cnt_groups = 1;
 
   const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A, LA = (size_t)L * A;
-  const int zctas = c->fast ? ctas_zpass_b2g(h) : ctas_zpass_u8(h, 256);
+  int zctas = c->fast ? ctas_zpass_b2g(h) : ctas_zpass_u8(h, 256);
+  if (c->fast) {
+    // room for the autotuner's smaller tiles (st_batch_autotune): T down to
+    // half the chosen one at the chosen R
+    c->tile_min_t = std::max(16, (h.tileT / 2 + 15) & ~15);
+    c->tile_min_r = h.tileR;
+    ChainDev hs = h;
+    hs.nchunks = (N + c->tile_min_t - 1) / c->tile_min_t;
+    zctas = std::max(zctas, ctas_zpass_b2g(hs));
+  }
   ChainDev hw = h;
   hw.G = 32;  // scratch sized for the widest group a batch may impose
   const int nred = std::max(ctas_locus(hw, kBlockLoc) * K, ctas_ind(hw, kBlockInd) * (K + 1));
@@ -1372,6 +1387,122 @@ extern "C" int st_set_state(st_chain* c, int f, const void* host, size_t bytes) 
 // ===========================================================================
 // batches
 // ===========================================================================
+
+// ---------------------------------------------------------------------------
+// Batch launch layout: per-chain CTA prefixes of the three kernels and, on
+// the fast path, one Z launch per K class (ZGroup).  The host copies are kept
+// in the batch so the autotuner can rebuild them after changing tiles.
+// ---------------------------------------------------------------------------
+static int batch_layout(st_batch* b, bool keep_groups) {
+  const int n = (int)b->chains.size();
+  b->table.assign(n, ChainDev{});
+  b->pz.assign(n, 0);
+  b->pl.assign(n, 0);
+  b->pi.assign(n, 0);
+  b->tz = b->tl = b->ti = 0;
+  if (!keep_groups) b->zg.clear();
+  for (ZGroup& g : b->zg) { g.tz = 0; g.zsmem = 0; g.n = 0; }
+  size_t gi = 0;
+  for (int j = 0; j < n; j++) {
+    st_chain* c = b->chains[j];
+    b->table[j] = c->h;
+    b->table[j].G = b->G;   // every chain's kernels index their groups by the batch-wide G
+    if (b->fast) {
+      if (!keep_groups && (b->zg.empty() || b->zg.back().KT != c->KT)) {
+        ZGroup g;
+        g.first = j;
+        g.KT = c->KT;
+        g.W = c->h.tileW;
+        b->zg.push_back(g);
+      }
+      while (gi + 1 < b->zg.size() && j >= b->zg[gi + 1].first) gi++;
+      ZGroup& g = keep_groups ? b->zg[gi] : b->zg.back();
+      if (c->h.tileW != g.W)
+        return seterr(b->ctx, ST_ERR_ARG, "chains of one K class must share the Z-pass width");
+      b->pz[j] = g.tz;
+      g.tz += ctas_zpass_b2g(b->table[j]);
+      g.zsmem = std::max(g.zsmem, c->zsmem);
+      g.n++;
+    } else {
+      b->pz[j] = b->tz;
+      b->tz += ctas_zpass_u8(b->table[j], 256);
+    }
+    b->pl[j] = b->tl;
+    b->pi[j] = b->ti;
+    b->tl += ctas_locus(b->table[j], kBlockLoc);
+    b->ti += ctas_ind(b->table[j], kBlockInd);
+  }
+  return ST_OK;
+}
+
+static void batch_upload(st_batch* b) {
+  const int n = (int)b->chains.size();
+  cudaMemcpy(b->d_table, b->table.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pz, b->pz.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pl, b->pl.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pi, b->pi.data(), 4 * n, cudaMemcpyHostToDevice);
+}
+
+// Z-pass tile (T individuals per chunk, R locus blocks per CTA) of one chain;
+// false when the chain's scratch was not sized for it.
+static bool set_tile(st_chain* c, int T, int R) {
+  ChainDev& h = c->h;
+  if (!c->fast || T < c->tile_min_t || R < c->tile_min_r || (T & 15)) return false;
+  const size_t smem = zpass_smem_all(c->KT, h.K, T, h.tileW);
+  if (smem > 200 * 1024) return false;
+  h.tileT = T;
+  h.tileR = R;
+  h.nchunks = (h.N + T - 1) / T;
+  const int lblocks = (h.L + 32 * h.tileW - 1) / (32 * h.tileW);
+  h.ngroups = (lblocks + R - 1) / R;
+  c->zsmem = smem;
+  return true;
+}
+
+static bool apply_group_tile(st_batch* b, const ZGroup& g, int T, int R) {
+  for (int j = g.first; j < g.first + g.n; j++) {
+    st_chain* c = b->chains[j];
+    const int t0 = c->h.tileT, r0 = c->h.tileR;
+    if (!set_tile(c, std::min(T, (c->h.N + 15) & ~15), R)) {
+      set_tile(c, t0, r0);
+      for (int q = g.first; q < j; q++) set_tile(b->chains[q], b->table[q].tileT, b->table[q].tileR);
+      return false;
+    }
+  }
+  for (int j = g.first; j < g.first + g.n; j++) upload_chain(b->chains[j]);
+  return true;
+}
+
+// In-process cache of tuned tiles, keyed by the K class and the shapes of the
+// group's chains.
+struct TileKey {
+  int KT;
+  std::vector<int64_t> shapes;
+  bool operator<(const TileKey& o) const {
+    return KT != o.KT ? KT < o.KT : shapes < o.shapes;
+  }
+};
+static std::mutex g_tile_mu;
+static std::map<TileKey, std::pair<int, int>> g_tile_cache;
+
+static TileKey tile_key(st_batch* b, const ZGroup& g) {
+  TileKey k{g.KT, {}};
+  for (int j = g.first; j < g.first + g.n; j++)
+    k.shapes.push_back(((int64_t)b->chains[j]->h.N << 32) | (uint32_t)b->chains[j]->h.L);
+  return k;
+}
+
+static bool tile_cache_get(st_batch* b, const ZGroup& g, int* T, int* R) {
+  for (int j = g.first; j < g.first + g.n; j++)
+    if (b->chains[j]->model.tile_t > 0 || b->chains[j]->model.tile_r > 0) return false;
+  std::lock_guard<std::mutex> lk(g_tile_mu);
+  auto it = g_tile_cache.find(tile_key(b, g));
+  if (it == g_tile_cache.end()) return false;
+  *T = it->second.first;
+  *R = it->second.second;
+  return true;
+}
+
 extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch** out) {
   if (!ctx || !chains || n < 1 || !out) return ST_ERR_ARG;
   *out = nullptr;
@@ -1402,39 +1533,10 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
     G = std::max(G, c->h.G);
   }
   b->G = G;
-  std::vector<ChainDev> table(n);
-  std::vector<int> pz(n), pl(n), pi(n);
-  for (int j = 0; j < n; j++) {
-    st_chain* c = b->chains[j];
-    table[j] = c->h;
-    table[j].G = G;   // every chain's kernels index their groups by the batch-wide G
-    if (b->fast && (b->zg.empty() || b->zg.back().KT != c->KT)) {
-      ZGroup g;
-      g.first = j;
-      g.KT = c->KT;
-      g.W = c->h.tileW;
-      b->zg.push_back(g);
-    }
-    if (b->fast) {
-      ZGroup& g = b->zg.back();
-      if (c->h.tileW != g.W) {
-        delete b;
-        return seterr(ctx, ST_ERR_ARG, "chains of one K class must share the Z-pass width");
-      }
-      pz[j] = g.tz;
-      g.tz += ctas_zpass_b2g(table[j]);
-      g.zsmem = std::max(g.zsmem, c->zsmem);
-      g.n++;
-    } else {
-      pz[j] = b->tz;
-      b->tz += ctas_zpass_u8(table[j], 256);
-    }
-    pl[j] = b->tl;
-    pi[j] = b->ti;
-    b->tl += ctas_locus(table[j], kBlockLoc);
-    b->ti += ctas_ind(table[j], kBlockInd);
+  if (int rc = batch_layout(b, false)) {
+    delete b;
+    return rc;
   }
-  // per-chain reduction scratch is sized for G = 32 (st_chain_create).
   auto alloc = [&](void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     return e == cudaSuccess ? ST_OK : seterr(ctx, ST_ERR_NOMEM, "batch table");
@@ -1444,14 +1546,117 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
     st_batch_destroy(b);
     return ST_ERR_NOMEM;
   }
-  cudaMemcpy(b->d_table, table.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_pz, pz.data(), 4 * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_pl, pl.data(), 4 * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_pi, pi.data(), 4 * n, cudaMemcpyHostToDevice);
+  // tiles the autotuner found for the same shapes earlier in this process
+  if (b->fast) {
+    bool changed = false;
+    for (ZGroup& g : b->zg) {
+      int T, R;
+      if (tile_cache_get(b, g, &T, &R)) changed = apply_group_tile(b, g, T, R) || changed;
+    }
+    if (changed) batch_layout(b, false);
+  }
+  batch_upload(b);
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
   *out = b;
   return ST_OK;
+}
+
+// Z-pass tile autotuner: for each K class of the batch, times candidate
+// tiles (T individuals per chunk x R locus blocks per CTA) on the batch's own
+// chains and data with the sweep's Z pass (counts on, no ln P(D), no
+// advance), keeps the fastest, and remembers it for batches of the same
+// shapes created later in the process.  Draws and counts do not depend on
+// the tile (Philox counters are per genotype, counts are exact), so a tuned
+// batch samples the same chain; only the order of the FP64 ln P(D) partial
+// sums changes.  The counts of the last Z pass are saved and restored around
+// the trials.
+extern "C" int st_batch_autotune(st_batch* b, int reps) {
+  if (!b) return ST_ERR_ARG;
+  if (!b->fast) return ST_OK;   // the generic path has one tile shape
+  st_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if (reps < 1) reps = 3;
+  ST_CUDA(ctx, cudaStreamSynchronize(s));
+  size_t total = 0;
+  for (st_chain* c : b->chains)
+    total += ((size_t)c->h.K * c->h.A * c->h.L + (size_t)c->h.N * c->h.K) * 4;
+  char* scratch = nullptr;
+  ST_CUDA(ctx, cudaMalloc((void**)&scratch, total));
+  auto copy_counts = [&](bool save) {
+    char* at = scratch;
+    for (st_chain* c : b->chains) {
+      const size_t nb = (size_t)c->h.K * c->h.A * c->h.L * 4, mb = (size_t)c->h.N * c->h.K * 4;
+      cudaMemcpyAsync(save ? at : (void*)c->h.npart, save ? (void*)c->h.npart : at, nb,
+                      cudaMemcpyDeviceToDevice, s);
+      at += nb;
+      cudaMemcpyAsync(save ? at : (void*)c->h.mpart, save ? (void*)c->h.mpart : at, mb,
+                      cudaMemcpyDeviceToDevice, s);
+      at += mb;
+    }
+  };
+  copy_counts(true);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = ST_OK;
+  for (size_t gi = 0; gi < b->zg.size() && rc == ST_OK; gi++) {
+    ZGroup& g = b->zg[gi];
+    st_chain* c0 = b->chains[g.first];
+    const int T0 = c0->h.tileT, R0 = c0->h.tileR;
+    std::vector<std::pair<int, int>> cand;
+    for (int tm : {2, 3, 4, 5, 6, 8})
+      for (int rm : {1, 2, 4, 8}) {
+        const std::pair<int, int> tr{((T0 * tm / 4) + 15) & ~15, R0 * rm};
+        if (std::find(cand.begin(), cand.end(), tr) == cand.end()) cand.push_back(tr);
+      }
+    double best = 1e300;
+    int bT = T0, bR = R0;
+    for (const auto& tr : cand) {
+      if (!apply_group_tile(b, g, tr.first, tr.second)) continue;
+      batch_layout(b, true);
+      batch_upload(b);
+      LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, s};
+      double ms_sum = 0.0;
+      for (int r = 0; r <= reps && rc == ST_OK; r++) {
+        for (int j = g.first; j < g.first + g.n; j++) {
+          const ChainDev& h = b->chains[j]->h;
+          cudaMemsetAsync(h.npart, 0, (size_t)h.K * h.A * h.L * 4, s);
+          cudaMemsetAsync(h.mpart, 0, (size_t)h.N * h.K * 4, s);
+        }
+        cudaEventRecord(e0, s);
+        cudaError_t e = launch_zpass_b2g(lg, g.KT, g.W, kZNormal, 0, g.zsmem);
+        cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) rc = cuda_check(ctx, e, "autotune");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0) ms_sum += ms;
+      }
+      if (rc == ST_OK && ms_sum < best) {
+        best = ms_sum;
+        bT = tr.first;
+        bR = tr.second;
+      }
+    }
+    apply_group_tile(b, g, bT, bR);
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    g_tile_cache[tile_key(b, g)] = {bT, bR};
+  }
+  batch_layout(b, true);
+  batch_upload(b);
+  copy_counts(false);
+  cudaStreamSynchronize(s);
+  cudaFree(scratch);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int j = 0; j < 2; j++)   // launch shapes changed: capture the sweeps again
+    if (b->gx[j]) {
+      cudaGraphExecDestroy(b->gx[j]);
+      b->gx[j] = nullptr;
+    }
+  return rc;
 }
 
 extern "C" int st_batch_destroy(st_batch* b) {

@@ -73,3 +73,43 @@ def test_batched_uneven_chains_equal_plain_chains(ctx, graphs):
         c.close()
     for d in data:
         d.close()
+
+
+def test_autotuned_batch_samples_the_same_chains(ctx):
+    """st_batch_autotune changes the Z-pass tiles only: the tuned batch and an
+    untuned twin (same seeds) end in the same state after sweeps that include
+    Metropolis steps; a batch of the same shapes created afterwards starts
+    from the remembered tiles."""
+    data = _datasets(ctx)
+    specs = [(K, s, d) for (K, s, d) in _specs() if K in (2, 5, 10)]
+    mk = lambda: [api.Chain(ctx, data[d], _model(K, s), 500 + 10 * K + s) for (K, s, d) in specs]
+    tuned, plain = mk(), mk()
+    bt, bp = api.Batch(ctx, tuned), api.Batch(ctx, plain)
+    bt.sweep(2)
+    bp.sweep(2)
+    before = [c.get(api.F_DIMS)[6:8].copy() for c in tuned]
+    bt.autotune(2)
+    after = [c.get(api.F_DIMS)[6:8].copy() for c in tuned]
+    bt.sweep(9)
+    bp.sweep(9)
+    for ct, cp in zip(tuned, plain):
+        assert ct.sync() == 0 and cp.sync() == 0
+        for f in EXACT:
+            a, b = ct.get(f), cp.get(f)
+            if f == api.F_REP or f == api.F_ERR:
+                assert a == b
+            else:
+                np.testing.assert_array_equal(a, b, err_msg=str(f))
+        sa, sp = ct.get(api.F_STATS), cp.get(api.F_STATS)
+        assert sa[api.ST_SUMLIKES] == pytest.approx(sp[api.ST_SUMLIKES], rel=1e-12)
+    # the remembered tiles apply to a new batch of the same shapes
+    again = mk()
+    ba = api.Batch(ctx, again)
+    np.testing.assert_array_equal([c.get(api.F_DIMS)[6:8] for c in again], after)
+    print("tiles (nchunks, ngroups) before", before[:3], "after", after[:3])
+    for b in (bt, bp, ba):
+        b.close()
+    for c in tuned + plain + again:
+        c.close()
+    for d in data:
+        d.close()
