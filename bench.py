@@ -569,6 +569,70 @@ def run_scale(args):
     print(json.dumps(out), flush=True)
 
 
+def run_uneven(args):
+    """Config 3: 40 chains = K in 1..10 x 4 seeds, seed s on data set s of
+    (N, L) = (300, 5000), (1000, 10000), (2500, 20000), (4000, 8000) (true K=4,
+    F_k ~ U[0.02, 0.2]), batched (one launch per update step and K class, CUDA
+    graphs, autotuned tiles) against the same chains one at a time."""
+    import torch
+    from structure_b200 import api, synth
+    sets = synth.config3_datasets(want_int32=False)
+    ctx = api.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    datas = [api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=d["N"], num_loci=d["L"],
+                      layout=api.LAYOUT_B2G) for d in sets]
+    mk = lambda K: api.model_defaults(maxpops=K, burnin=args.warmup, numreps=args.steps + 10,
+                                      freqscorr=1, inferalpha=1, alpha=1.0, metrofreq=10,
+                                      fpriormean=0.01, fpriorsd=0.05, computeprob=1)
+    chains = [api.Chain(ctx, datas[s], mk(K), 3000 + 10 * K + s) for K in range(1, 11)
+              for s in range(4)]
+    b = api.Batch(ctx, chains)
+    b.autotune()
+    b.sweep(args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.sweep(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    n = len(chains)
+    plain_sweeps = max(2, min(args.steps, 20))
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for c in chains:
+        c.sweep(plain_sweeps)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    for c in chains:
+        assert c.sync() == 0
+    value = n * args.steps / (ms / 1e3)
+    plain = n * plain_sweeps / (p0.elapsed_time(p1) / 1e3)
+    copies = sum(2 * d["N"] * d["L"] * 10 for d in sets) * 0.97
+    out = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
+           "data": "synthetic, seeded (config 3 generator)",
+           "config": {"workload": "uneven batch: 40 chains, K=1..10 x 4 seeds over 4 SNP data sets "
+                                  "(300x5000, 1000x10000, 2500x20000, 4000x8000), F model",
+                      "chains": n, "k_classes": 10},
+           "plain": {"value": round(plain, 3), "unit": METRIC,
+                     "path": "one chain per launch, same kernels"},
+           "batched_over_plain": round(value / plain, 3),
+           "z_updates_per_s": round(args.steps * copies / (ms / 1e3), 1),
+           "clocks": clk}
+    b.close()
+    for c in chains:
+        c.close()
+    for d in datas:
+        d.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,14 +640,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="snp", choices=["snp", "grad", "mala", "scale"],
+    ap.add_argument("--workload", default="snp",
+                    choices=["snp", "grad", "mala", "scale", "uneven"],
                     help="snp: the headline (default); grad: config 4 forward+backward; "
-                         "mala: config 4 ESS/s, Gibbs vs Gibbs+Langevin; scale: config 5")
+                         "mala: config 4 ESS/s, Gibbs vs Gibbs+Langevin; scale: config 5; "
+                         "uneven: config 3 batched vs one chain at a time")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload != "snp" and args.impl == "ours":
-        {"grad": run_grad, "mala": run_mala, "scale": run_scale}[args.workload](args)
+        {"grad": run_grad, "mala": run_mala, "scale": run_scale,
+         "uneven": run_uneven}[args.workload](args)
         return
     if args.impl == "reference":
         run_reference(args)

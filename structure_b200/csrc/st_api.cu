@@ -95,6 +95,9 @@ struct st_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<ChainDev> table;             // host copies of the device tables
   std::vector<int> pz, pl, pi;
+  std::vector<cudaStream_t> aux;           // one per K class (several classes only)
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
 };
 
 namespace {
@@ -1558,6 +1561,20 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
   batch_upload(b);
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
+  if (b->fast && b->zg.size() > 1) {
+    cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    for (size_t gi = 0; gi < b->zg.size(); gi++) {
+      cudaStream_t as = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithFlags(&as, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        st_batch_destroy(b);
+        return seterr(ctx, ST_ERR_CUDA, "batch streams");
+      }
+      b->aux.push_back(as);
+      b->ev_join.push_back(ev);
+    }
+  }
   *out = b;
   return ST_OK;
 }
@@ -1668,6 +1685,9 @@ extern "C" int st_batch_destroy(st_batch* b) {
   if (b->ev1) cudaEventDestroy(b->ev1);
   for (cudaGraphExec_t x : b->gx)
     if (x) cudaGraphExecDestroy(x);
+  for (cudaStream_t as : b->aux) cudaStreamDestroy(as);
+  for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   delete b;
   return ST_OK;
 }
@@ -1684,11 +1704,22 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
   cudaStream_t s = ctx->stream;
   LaunchSet lz{b->d_table, b->d_pz, n, b->tz, s};
   // one fast Z launch per K class over its slice of the table
+  // one fast Z launch per K class; with several classes they run side by side
+  // on forked streams (independent chains), so one class's tail overlaps the next
   auto zfast = [&](int mode, int flags) -> int {
-    for (const ZGroup& g : b->zg) {
-      LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, s};
+    const bool fork = b->zg.size() > 1 && !b->aux.empty();
+    if (fork) ST_CUDA(ctx, cudaEventRecord(b->ev_fork, s));
+    for (size_t gi = 0; gi < b->zg.size(); gi++) {
+      const ZGroup& g = b->zg[gi];
+      cudaStream_t gs = fork ? b->aux[gi] : s;
+      if (fork) ST_CUDA(ctx, cudaStreamWaitEvent(gs, b->ev_fork, 0));
+      LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, gs};
       ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags, g.zsmem));
+      if (fork) ST_CUDA(ctx, cudaEventRecord(b->ev_join[gi], gs));
     }
+    if (fork)
+      for (size_t gi = 0; gi < b->zg.size(); gi++)
+        ST_CUDA(ctx, cudaStreamWaitEvent(s, b->ev_join[gi], 0));
     ctx->launches += (int64_t)b->zg.size() - 1;   // the bracket counted one
     return ST_OK;
   };
@@ -1756,9 +1787,9 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
   for (st_chain* c : b->chains)
     if (c->h.mala && c->h.K > 1)
       if (int rc = mala_step(c)) return rc;
-  for (st_chain* c : b->chains) {   // the Z pass adds into cleared histograms
-    ST_CUDA(ctx, cudaMemsetAsync(c->h.npart, 0, sizeof(int32_t) * (size_t)c->h.K * c->h.A * c->h.L, s));
-    ST_CUDA(ctx, cudaMemsetAsync(c->h.mpart, 0, sizeof(int32_t) * (size_t)c->h.N * c->h.K, s));
+  {   // the Z pass adds into cleared histograms: one kernel for every chain
+    Bracket br(ctx, ST_K_OTHER);
+    ST_CUDA(ctx, launch_clear_counts(b->d_table, n, s));
   }
   {
     Bracket br(ctx, ST_K_ZPASS);

@@ -56,6 +56,7 @@ cudaError_t launch_popinfo(const ChainDev& h, const ChainDev* d_chain, cudaStrea
 cudaError_t launch_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
 cudaError_t launch_alpha_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
+cudaError_t launch_clear_counts(const ChainDev* d_table, int nchains, cudaStream_t s);
 
 // CTA counts per chain for each launch kind (host-side mirror of the tiling).
 int ctas_zpass_b2g(const ChainDev& c);

@@ -252,4 +252,21 @@ cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStrea
   return cudaGetLastError();
 }
 
+// Clears the allele and ancestry histograms (n [K][A][L], m [N][K]) of every
+// chain of a batch before the counting Z pass: one launch, blockIdx.y = chain.
+__global__ void clear_counts_kernel(const ChainDev* __restrict__ chains) {
+  const ChainDev& ch = chains[blockIdx.y];
+  const size_t nn = (size_t)ch.K * ch.A * ch.L, nm = (size_t)ch.N * ch.K;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < nn + nm; j += stride) {
+    if (j < nn) ch.npart[j] = 0;
+    else ch.mpart[j - nn] = 0;
+  }
+}
+
+cudaError_t launch_clear_counts(const ChainDev* d_table, int nchains, cudaStream_t s) {
+  clear_counts_kernel<<<dim3(64, nchains), 256, 0, s>>>(d_table);
+  return cudaGetLastError();
+}
+
 }  // namespace st

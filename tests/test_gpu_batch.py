@@ -50,9 +50,10 @@ def test_batched_uneven_chains_equal_plain_chains(ctx, graphs):
     b.graphs(graphs)
     l0 = ctx.launches()
     b.sweep(4)
-    # one locus, one or two individual and one Z launch per K class per sweep
+    # one locus, one or two individual, one count-clearing and one Z launch per
+    # K class per sweep
     nclass = len({api.fast_class(K) for K, _, _ in _specs()})
-    assert ctx.launches() - l0 == 4 * (2 + nclass) + 2 * (1 + nclass)
+    assert ctx.launches() - l0 == 4 * (3 + nclass) + 2 * (1 + nclass)
     for c in plain:
         c.sweep(4)
     for cb, cp in zip(batched, plain):
