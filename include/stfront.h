@@ -88,6 +88,11 @@ int stf_set_usepopprobs(stf_run *r, const double *usepop);
 int stf_num_locations(const stf_run *r);
 int stf_set_locprior_sums(stf_run *r, const double *sums, size_t n);
 
+/* INTERMEDSAVE: with savenum > 0 the next stf_write_results writes the
+ * intermediate file OUTFILE_<savenum> (src/output.c:1381-1385) and no
+ * OUTFILE_q; 0 (the default) writes OUTFILE_f.                             */
+int stf_set_save_number(stf_run *r, int savenum);
+
 /* Writes OUTFILE_f (and OUTFILE_q when PRINTQHAT=1) from the run's sums, in
  * the reference layouts: QSum [N][K], PSum [L][K][MAXALLELES], SumEpsilon
  * [L][MAXALLELES] (may be NULL without FREQSCORR), FstSum [K], sumAlpha [K],

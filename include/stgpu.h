@@ -159,7 +159,10 @@ typedef struct st_model {
     int32_t popflag_given;     /* 1: popflags in the data are POPFLAG values; 0: every
                                 * individual with a population is flagged (POPFLAG=0) */
     int32_t updatelocprior;    /* UPDATELOCPRIOR (LOCPRIOR): 0 keeps r, nu, gamma fixed */
-    int32_t reserved;
+    int32_t startatpopinfo;    /* STARTATPOPINFO: initial Z at each individual's given
+                                * population where it is in 1..K (needs population
+                                * data; without it the start is random, as in
+                                * src/Init.c:89-93) */
     double migrprior;          /* MIGRPRIOR (USEPOPINFO) */
     double locpriorinit;       /* LOCPRIORINIT: initial r */
     double maxlocprior;        /* MAXLOCPRIOR: upper bound of r */
@@ -188,6 +191,9 @@ int st_update_alpha(st_chain *c);  /* UpdateAlphaCL  src/Updates/UpdateAlpha.c:3
 int st_update_eps(st_chain *c);    /* UpdateEpsilonCL src/Updates/UpdateEpsilon.c:270-292 */
 int st_update_fst(st_chain *c);    /* UpdateFstCL    src/Updates/UpdateFst.c:100-140 */
 int st_collect(st_chain *c);       /* DataCollectionCL src/output.c:104-183         */
+int st_calc_like(st_chain *c, double *like); /* CalcLike src/CalcLike.c:387-426:
+                                      ln P(D|Q,P) of the current state (synchronous;
+                                      no sums are touched)                          */
 int st_update_lambda(st_chain *c); /* UpdateLambda / UpdatePopLambda (CPU only in the
                                       reference) src/Updates/UpdateLambda.c:8-102   */
 int st_update_locprior(st_chain *c);/* UpdateLocPrior (CPU only in the reference)

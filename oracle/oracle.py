@@ -380,7 +380,8 @@ class RefModel(C.Structure):
               [("inferlambda", _ci), ("popspecificlambda", _ci), ("noadmix", _ci),
                ("admburnin", _ci), ("usepopinfo", _ci), ("gensback", _ci), ("popflag", _ci),
                ("migrprior", _cd), ("locprior", _ci), ("updatelocprior", _ci),
-               ("locpriorinit", _cd), ("maxlocprior", _cd), ("locpriorstep", _cd)]
+               ("locpriorinit", _cd), ("maxlocprior", _cd), ("locpriorstep", _cd),
+               ("startatpopinfo", _ci)]
 
 
 class RefView(C.Structure):
@@ -401,7 +402,8 @@ def ref_model(**kw):
              alphapropsd=0.025, alphapriora=0.05, alphapriorb=0.001, lambda_=1.0,
              fpriormean=0.01, fpriorsd=0.05, inferlambda=0, popspecificlambda=0, noadmix=0,
              admburnin=0, usepopinfo=0, gensback=2, popflag=0, migrprior=0.05, locprior=0,
-             updatelocprior=1, locpriorinit=1.0, maxlocprior=20.0, locpriorstep=0.1)
+             updatelocprior=1, locpriorinit=1.0, maxlocprior=20.0, locpriorstep=0.1,
+             startatpopinfo=0)
     d.update(kw)
     return RefModel(**d)
 

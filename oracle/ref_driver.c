@@ -145,6 +145,7 @@ typedef struct stref_model {
     double migrprior;
     int locprior, updatelocprior;
     double locpriorinit, maxlocprior, locpriorstep;
+    int startatpopinfo;
 } stref_model;
 
 void stref_set_globals(const stref_model *m)
@@ -164,7 +165,8 @@ void stref_set_globals(const stref_model *m)
     MAXLOCPRIOR = m->maxlocprior; LOCPRIORSTEP = m->locpriorstep;
     RECESSIVEALLELES = 0;
     INFERLAMBDA = m->inferlambda; POPSPECIFICLAMBDA = m->popspecificlambda;
-    STARTATPOPINFO = 0; POPDATA = m->usepopinfo ? 1 : 0; POPFLAG = m->popflag;
+    STARTATPOPINFO = m->startatpopinfo;
+    POPDATA = (m->usepopinfo || m->startatpopinfo) ? 1 : 0; POPFLAG = m->popflag;
     MIGRPRIOR = m->migrprior;
     INTERMEDSAVE = 0; REPORTHITRATE = 0; UPDATEFREQ = 1 << 30; ADMBURNIN = m->admburnin;
     NOALPHA = 0; PHASED = 0; PHASEINFO = 0; MARKOVPHASE = 0; NOQS = 0;

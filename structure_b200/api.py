@@ -54,7 +54,7 @@ class Model(C.Structure):
                                    "alphapriorb", "lambda_", "fpriormean", "fpriorsd")] + \
         [(n, C.c_int32) for n in ("store_z", "precision", "tile_t", "tile_w", "tile_r", "mala",
                                   "mala_target", "admburnin", "gensback", "popflag_given")] + \
-        [("updatelocprior", C.c_int32), ("reserved", C.c_int32), ("migrprior", C.c_double),
+        [("updatelocprior", C.c_int32), ("startatpopinfo", C.c_int32), ("migrprior", C.c_double),
          ("locpriorinit", C.c_double), ("maxlocprior", C.c_double),
          ("locpriorstep", C.c_double)]
 
@@ -97,6 +97,7 @@ def lib():
         "st_update_q_mala": ([vp], C.c_int),
         "st_update_lambda": ([vp], C.c_int),
         "st_update_locprior": ([vp], C.c_int),
+        "st_calc_like": ([vp, C.POINTER(C.c_double)], C.c_int),
         "st_batch_autotune": ([vp, C.c_int], C.c_int),
         "st_chain_save": ([vp, C.c_char_p], C.c_int),
         "st_chain_load": ([vp, C.c_char_p], C.c_int),
@@ -290,6 +291,12 @@ class Chain:
     def UpdateQMala(self): self.ctx.check(lib().st_update_q_mala(self.h))
     def UpdateLambda(self): self.ctx.check(lib().st_update_lambda(self.h))
     def UpdateLocPrior(self): self.ctx.check(lib().st_update_locprior(self.h))
+
+    def CalcLike(self):
+        """ln P(D|Q,P) of the current state (st_calc_like)."""
+        v = C.c_double()
+        self.ctx.check(lib().st_calc_like(self.h, C.byref(v)))
+        return v.value
 
     def save(self, path):
         """Checkpoint the whole chain state to `path` (st_chain_save)."""

@@ -798,6 +798,15 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
                                   {&pi_init, (size_t)N * 4}, {&pi_use, (size_t)N * KG * 8},
                                   {&pi_part, (size_t)h.pi_lchunks * N * KG * 8}})
       bufs.push_back(b);
+  } else if (model->startatpopinfo && !data->population_h.empty()) {
+    // STARTATPOPINFO (src/Init.c:412-413,74-117 InitFromGeogPop): copies of
+    // individuals with a population in 1..K start there, the others at random
+    initpop.resize(N);
+    for (int i = 0; i < N; i++) {
+      const int p = data->population_h[i];
+      initpop[i] = (p >= 1 && p <= K) ? p - 1 : -1;
+    }
+    bufs.push_back({&pi_init, (size_t)N * 4});
   }
   void *lp_myloc = nullptr, *lp_start = nullptr, *lp_inds = nullptr, *lp_p = nullptr,
        *lp_sum = nullptr;
@@ -862,10 +871,10 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     h.locp = (double*)lp_p;
     h.sumlocp = (double*)lp_sum;
   }
+  if (!initpop.empty()) h.initpop = (const int32_t*)pi_init;
   if (model->usepopinfo) {
     h.popflags = (int32_t*)pi_flag;
     h.population = (const int32_t*)pi_pop;
-    h.initpop = (const int32_t*)pi_init;
     h.usepop = (double*)pi_use;
     h.pipart = (double*)pi_part;
   }
@@ -938,10 +947,11 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     cudaMemcpyAsync(lp_p, lpv.data(), (size_t)h.lp_len * 8, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(lp_sum, 0, (size_t)h.lp_len * 8, s);
   }
+  if (!initpop.empty())
+    cudaMemcpyAsync(pi_init, initpop.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
   if (h.usepopinfo) {
     cudaMemcpyAsync(pi_flag, pflag.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(pi_pop, pop1.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(pi_init, initpop.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(pi_use, 0, (size_t)N * K * (h.gensback + 1) * 8, s);
   }
   int zero = 0;
@@ -1066,6 +1076,18 @@ extern "C" int st_collect(st_chain* c) {
   Bracket br(c->ctx, ST_K_OTHER);
   LaunchSet ls = single(c, ctas_collect(c->h, kBlockCol));
   return cuda_check(c->ctx, launch_collect(ls, kBlockCol), "collect");
+}
+
+// CalcLike (src/CalcLike.c:387-426): ln P(D|Q,P) of the chain's current
+// state, sums untouched.
+extern "C" int st_calc_like(st_chain* c, double* like) {
+  if (!c || !like) return ST_ERR_ARG;
+  cudaSetDevice(c->ctx->device);
+  if (int rc = zpass(c, kZLike, kZfLikeAlways)) return rc;
+  ST_CUDA(c->ctx, cudaMemcpyAsync(like, c->h.stats + kStLike, sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->ctx->stream));
+  ST_CUDA(c->ctx, cudaStreamSynchronize(c->ctx->stream));
+  return ST_OK;
 }
 
 extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int precision) {

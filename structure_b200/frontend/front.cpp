@@ -193,6 +193,7 @@ struct stf_run {
   std::vector<double> usepop;   // [N][MAXPOPS][GENSBACK+1]
   // LOCPRIOR (stf_set_locprior_sums): sumLocPrior, the reference's layout
   std::vector<double> sumlocp;
+  int savenum = 0;              // > 0: the next results go to OUTFILE_<savenum>
 };
 
 namespace {
@@ -661,6 +662,12 @@ extern "C" int stf_set_locprior_sums(stf_run* r, const double* sums, size_t n) {
   const size_t need = I(r, "NOADMIX") ? 1 + (size_t)I(r, "MAXPOPS") * (location_ids(r).size() + 1) : 1;
   if (n != need) return fail(r, STF_ERR_ARG, "sumLocPrior: %zu values given, %zu expected", n, need);
   r->sumlocp.assign(sums, sums + n);
+  return STF_OK;
+}
+
+extern "C" int stf_set_save_number(stf_run* r, int savenum) {
+  if (!r || savenum < 0) return STF_ERR_ARG;
+  r->savenum = savenum;
   return STF_OK;
 }
 
@@ -1137,9 +1144,12 @@ extern "C" int stf_write_results(stf_run* r, int rep, const double* QSum, const 
   ancestry(r, o, s);
   allele_freqs(r, o, s);
   all_params(r, o);
-  const std::string name = S(r, "OUTFILE") + "_f";
+  // src/output.c:1381-1385: OUTFILE_f at the end, OUTFILE_<n> for the n-th
+  // intermediate save (INTERMEDSAVE); OUTFILE_q only at the end
+  const std::string name =
+      S(r, "OUTFILE") + (r->savenum > 0 ? "_" + std::to_string(r->savenum) : std::string("_f"));
   if (!write_text(name, o.s)) return fail(r, STF_ERR_IO, "Unable to open output file %s.", name.c_str());
-  if (I(r, "PRINTQHAT")) {
+  if (I(r, "PRINTQHAT") && r->savenum == 0) {
     // src/output.c:914-953 PrintQFile
     Out q;
     const int K = I(r, "MAXPOPS"), reps = rep - I(r, "BURNIN");

@@ -12,6 +12,7 @@
 // Options the GPU path does not implement (LINKAGE, RECESSIVEALLELES, PLOIDY
 // other than 2) stop the program with a message instead of running a
 // different model.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -142,6 +143,7 @@ int main(int argc, char** argv) {
   m.popflag_given = 1;   // the flags above already hold CheckPopPriors' result
   m.gensback = pi(r, "GENSBACK");
   m.migrprior = pd(r, "MIGRPRIOR");
+  m.startatpopinfo = pi(r, "STARTATPOPINFO");
   m.locprior = pi(r, "LOCPRIOR");
   m.updatelocprior = pi(r, "UPDATELOCPRIOR");
   m.locpriorinit = pd(r, "LOCPRIORINIT");
@@ -155,59 +157,91 @@ int main(int argc, char** argv) {
   printf("%d iterations + %d burnin\n\n", m.numreps, m.burnin);
   const int total = m.burnin + m.numreps, every = pi(r, "UPDATEFREQ") > 0 ? pi(r, "UPDATEFREQ") : 100;
   std::vector<double> alpha(K), F(K), stats(256);
+  // results from the run's sums: OUTFILE_f at the end, OUTFILE_<n> for the
+  // n-th intermediate save (src/structure.c:640-660)
+  const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A;
+  auto write_results = [&](int rep, int savenum) -> int {
+    std::vector<double> QSum(NK), PSum(LKA), SumEps((size_t)L * A), FstSum(K),
+        sumAlpha(st_field_bytes(c, ST_F_SUMALPHA) / 8), sumlambda(K);
+    std::vector<int32_t> AD;
+    st_get_state(c, ST_F_QSUM, QSum.data(), NK * 8);
+    st_get_state(c, ST_F_PSUM, PSum.data(), LKA * 8);
+    st_get_state(c, ST_F_SUMEPS, SumEps.data(), SumEps.size() * 8);
+    st_get_state(c, ST_F_FSTSUM, FstSum.data(), K * 8);
+    st_get_state(c, ST_F_SUMALPHA, sumAlpha.data(), sumAlpha.size() * 8);
+    st_get_state(c, ST_F_SUMLAMBDA, sumlambda.data(), K * 8);
+    st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
+    if (m.ancestdist) {
+      AD.resize(NK * (size_t)m.numboxes);
+      st_get_state(c, ST_F_ANCESTDIST, AD.data(), AD.size() * 4);
+    }
+    if (m.locprior) {
+      std::vector<double> lp(st_field_bytes(c, ST_F_SUMLOCPRIOR) / 8);
+      st_get_state(c, ST_F_SUMLOCPRIOR, lp.data(), lp.size() * 8);
+      if (stf_set_locprior_sums(r, lp.data(), lp.size()) != STF_OK) return STF_ERR_ARG;
+    }
+    if (m.usepopinfo) {
+      std::vector<double> up(NK * (size_t)(m.gensback + 1));
+      st_get_state(c, ST_F_USEPOPPROBS, up.data(), up.size() * 8);
+      stf_set_usepopprobs(r, up.data());
+    }
+    stf_set_save_number(r, savenum);
+    const int wrc = stf_write_results(r, rep, QSum.data(), PSum.data(), SumEps.data(),
+                                      FstSum.data(), sumAlpha.data(), sumlambda.data(),
+                                      AD.empty() ? nullptr : AD.data(), stats[1], stats[2]);
+    stf_set_save_number(r, 0);
+    return wrc;
+  };
+  // INTERMEDSAVE: results every savefreq collected sweeps (src/Init.c:376-385)
+  int savefreq = 0;
+  if (pi(r, "INTERMEDSAVE") > 0) {
+    savefreq = m.numreps / (pi(r, "INTERMEDSAVE") + 1);
+    if (savefreq * (pi(r, "INTERMEDSAVE") + 1) < m.numreps) savefreq++;
+  }
+  const bool printlikes = pi(r, "PRINTLIKES") != 0;
   printf(" Rep#:   Alpha   %s Ln Like    Est Ln P(D)\n", m.freqscorr ? " F(mean)" : "");
   for (int done = 0; done < total;) {
-    const int n = total - done < every ? total - done : every;
-    rc = st_sweep(c, n);
+    int next = std::min(total, (done / every + 1) * every);
+    if (savefreq > 0 && savefreq <= m.numreps) {
+      const int after = std::max(done + 1, m.burnin + 1);
+      const int save = m.burnin + ((after - m.burnin + savefreq - 1) / savefreq) * savefreq;
+      if (save < total) next = std::min(next, save);
+    }
+    if (printlikes) next = done + 1;
+    rc = st_sweep(c, next - done);
     if (rc == ST_OK) rc = st_sync(c);
     if (rc != ST_OK) return die("GPU", st_last_error(ctx));
-    done += n;
-    st_get_state(c, ST_F_ALPHA, alpha.data(), alpha.size() * 8);
-    st_get_state(c, ST_F_F, F.data(), F.size() * 8);
+    done = next;
     st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
-    double fm = 0.0;
-    for (double v : F) fm += v / K;
-    printf("%5d:    %1.3f  ", done, alpha[0]);
-    if (m.freqscorr) printf("  %1.3f  ", fm);
-    if (done > m.burnin && m.computeprob) {
-      const double reps = done - m.burnin, mean = stats[1] / reps;
-      const double var = reps > 1 ? (stats[2] - stats[1] * stats[1] / reps) / (reps - 1) : 0.0;
-      printf("%9.0f  %9.0f", stats[0], mean - var / 2.0);
-    } else if (done == m.burnin) {
-      printf("\nBURNIN completed");
+    if (printlikes) {
+      // src/output.c:187-200 PrintLike: the sweep's ln P(D) once collecting,
+      // else CalcLike of the current state
+      double like = stats[0];
+      if (done <= m.burnin && st_calc_like(c, &like) != ST_OK) return die("GPU", st_last_error(ctx));
+      printf("%6.0f\n", like);
     }
-    printf("\n");
-  }
-  const size_t NK = (size_t)N * K, LKA = (size_t)L * K * A;
-  std::vector<double> QSum(NK), PSum(LKA), SumEps((size_t)L * A), FstSum(K),
-      sumAlpha(st_field_bytes(c, ST_F_SUMALPHA) / 8), sumlambda(K);
-  std::vector<int32_t> AD;
-  st_get_state(c, ST_F_QSUM, QSum.data(), NK * 8);
-  st_get_state(c, ST_F_PSUM, PSum.data(), LKA * 8);
-  st_get_state(c, ST_F_SUMEPS, SumEps.data(), SumEps.size() * 8);
-  st_get_state(c, ST_F_FSTSUM, FstSum.data(), K * 8);
-  st_get_state(c, ST_F_SUMALPHA, sumAlpha.data(), sumAlpha.size() * 8);
-  st_get_state(c, ST_F_SUMLAMBDA, sumlambda.data(), K * 8);
-  st_get_state(c, ST_F_STATS, stats.data(), stats.size() * 8);
-  if (m.ancestdist) {
-    AD.resize(NK * (size_t)m.numboxes);
-    st_get_state(c, ST_F_ANCESTDIST, AD.data(), AD.size() * 4);
-  }
-  if (m.locprior) {
-    std::vector<double> lp(st_field_bytes(c, ST_F_SUMLOCPRIOR) / 8);
-    st_get_state(c, ST_F_SUMLOCPRIOR, lp.data(), lp.size() * 8);
-    if (stf_set_locprior_sums(r, lp.data(), lp.size()) != STF_OK)
-      return die("output", stf_last_error(r));
-  }
-  if (m.usepopinfo) {
-    std::vector<double> up(NK * (size_t)(m.gensback + 1));
-    st_get_state(c, ST_F_USEPOPPROBS, up.data(), up.size() * 8);
-    stf_set_usepopprobs(r, up.data());
+    if (done % every == 0 || done == total) {
+      st_get_state(c, ST_F_ALPHA, alpha.data(), alpha.size() * 8);
+      st_get_state(c, ST_F_F, F.data(), F.size() * 8);
+      double fm = 0.0;
+      for (double v : F) fm += v / K;
+      printf("%5d:    %1.3f  ", done, alpha[0]);
+      if (m.freqscorr) printf("  %1.3f  ", fm);
+      if (done > m.burnin && m.computeprob) {
+        const double reps = done - m.burnin, mean = stats[1] / reps;
+        const double var = reps > 1 ? (stats[2] - stats[1] * stats[1] / reps) / (reps - 1) : 0.0;
+        printf("%9.0f  %9.0f", stats[0], mean - var / 2.0);
+      } else if (done == m.burnin) {
+        printf("\nBURNIN completed");
+      }
+      printf("\n");
+    }
+    if (savefreq > 0 && done > m.burnin && (done - m.burnin) % savefreq == 0 && done != total)
+      if (write_results(done, (done - m.burnin) / savefreq) != STF_OK)
+        return die("output", stf_last_error(r));
   }
   printf("\nMCMC completed\n");
-  rc = stf_write_results(r, total, QSum.data(), PSum.data(), SumEps.data(), FstSum.data(),
-                         sumAlpha.data(), sumlambda.data(), AD.empty() ? nullptr : AD.data(),
-                         stats[1], stats[2]);
+  rc = write_results(total, 0);
   if (rc != STF_OK) return die("output", stf_last_error(r));
   char outfile[256];
   stf_param_str(r, "OUTFILE", outfile, sizeof outfile);

@@ -195,6 +195,8 @@ EXTRA_TMPL = """EXTRA PARAMS (written by the test)
 #define ALPHAMAX     10.0 // (d)
 #define ALPHAPROPSD 0.025 // (d)
 #define UPDATEFREQ   {updatefreq}  // (int)
+#define INTERMEDSAVE {intermedsave}  // (int)
+#define PRINTLIKES   {printlikes}  // (B)
 #define PRINTQHAT  {printqhat}  // (B)
 #define ANCESTDIST   {ancestdist}  // (B)
 #define NUMBOXES   {numboxes} // (int)
@@ -213,7 +215,8 @@ def _scenario(d, **kw):
              missing=-9, onerow=0, label=1, popdata=1, popflag=0, extracols=0, markernames=1,
              mapdist=0, freqscorr=1, onefst=0, popalphas=0, updatefreq=0, printqhat=0,
              ancestdist=0, numboxes=100, seed=4242, noadmix=0, usepopinfo=0, migrprior=0.05,
-             gensback=2, locdata=0, locprior=0, locispop=0, admburnin=50)
+             gensback=2, locdata=0, locprior=0, locispop=0, admburnin=50, intermedsave=0,
+             printlikes=0)
     p.update(kw)
     with open(os.path.join(d, "mainparams"), "w") as f:
         f.write(MAIN_TMPL.format(**p))

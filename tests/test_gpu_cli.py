@@ -29,13 +29,16 @@ def _snp_data(d, p):
         f.write("\n".join(rows) + "\n")
 
 
-@pytest.mark.parametrize("kind", ["microsat", "snp", "usepopinfo", "locprior", "locprior-noadmix"])
+@pytest.mark.parametrize("kind", ["microsat", "snp", "usepopinfo", "locprior", "locprior-noadmix",
+                                  "intermedsave"])
 def test_cli_run_writes_results(tmp_path, kind):
     d = str(tmp_path)
     if kind == "usepopinfo":
         return _usepopinfo_run(d)
     if kind.startswith("locprior"):
         return _locprior_run(d, kind.endswith("noadmix"))
+    if kind == "intermedsave":
+        return _intermedsave_run(d)
     if kind == "microsat":
         p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200)
     else:
@@ -116,3 +119,22 @@ def _locprior_run(d, noadmix):
         assert "Mean value of alpha_local for each location:" in text
         rows = re.findall(r"^\tlocation\s+(\d+):((?:\s+[0-9.]+){3})$", text, re.M)
         assert [int(x) for x, _ in rows] == [5, 8, 11]
+
+
+def _intermedsave_run(d):
+    """INTERMEDSAVE=2 writes results_1 and results_2 after 200 and 400 of the
+    600 collected sweeps (src/structure.c:640-660); PRINTLIKES=1 prints one ln
+    likelihood per sweep (src/output.c:187-200)."""
+    p = _scenario(d, N=40, L=20, burnin=100, numreps=600, updatefreq=100, intermedsave=2,
+                  printlikes=1)
+    r = subprocess.run([CLI, "-D", "5"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for k, reps in ((1, 200), (2, 400)):
+        text = open(os.path.join(d, f"results_{k}")).read()
+        assert f"   {reps} Reps" in text
+        assert "Estimated Ln Prob of Data" in text
+    assert not os.path.exists(os.path.join(d, "results_3"))
+    assert "   600 Reps" in open(os.path.join(d, "results_f")).read()
+    likes = re.findall(r"^\s*(-\d+)$", r.stdout, re.M)
+    assert len(likes) == p["burnin"] + p["numreps"]
+    assert all(float(x) < 0 for x in likes)

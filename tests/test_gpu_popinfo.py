@@ -86,3 +86,26 @@ def test_popinfo_q_matches_oracle(ctx, orc, layout):
                                       Q1, lQ1)
     np.testing.assert_array_equal(Qm[f], Qo8[f])
     c.close(); data.close()
+
+
+@pytest.mark.parametrize("layout", [api.LAYOUT_U8, api.LAYOUT_B2G])
+def test_startatpopinfo_initial_z(ctx, layout):
+    """STARTATPOPINFO without USEPOPINFO (src/Init.c:412-413 InitFromGeogPop):
+    every copy of an individual whose population is in 1..K starts there,
+    the others at random; without it the start is random for everyone."""
+    geno, na, pop, eff, data, _ = _setup(ctx, layout)
+    K = 3
+    ok = (pop >= 1) & (pop <= K)
+    home = np.clip(pop - 1, 0, K - 1)
+    for start in (1, 0):
+        m = api.model_defaults(maxpops=K, burnin=5, numreps=20, startatpopinfo=start)
+        c = api.Chain(ctx, data, m, SEED)
+        M = c.get(api.F_M)
+        at_home = M[ok, home[ok]] == M[ok].sum(1)
+        if start:
+            assert at_home.all()
+            assert not (M[~ok].max(1) == M[~ok].sum(1)).all()   # out of range: random
+        else:
+            assert not at_home.any()
+        c.close()
+    data.close()
