@@ -78,7 +78,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
   z.q2 = o; if (useP) o = zalign16(o + (size_t)T * KT2 * 8);            // (q,q) pairs
   z.t2 = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * KT2 * 8);  // (t,t) pairs
   z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT2 * nw32 * 8);      // allele table
-  z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * 8);
+  z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * (nw32 / 32) * 4);   // per warp
   z.inc = o; if (counts && KT <= 8) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * 8);
   z.m = o;  if (counts) o = zalign16(o + (size_t)T * KT * 4);
   z.n = o;  if (counts) o = zalign16(o + (size_t)(2 * K + 1) * nw32 * 4);
@@ -106,7 +106,7 @@ struct ZArgs {
   const float2* Xlane;
   const float2* sQ2;
   const float2* sT2;
-  double* sLD;
+  float* sLD;     // this warp's Metropolis log-ratio partials, one per row
   const uint2* sInc;
   int* sM;
   int* mycol;
@@ -157,7 +157,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   const float2* Xlane = za.Xlane;
   const float2* sQ2 = za.sQ2;
   const float2* sT2 = za.sT2;
-  double* sLD = za.sLD;
+  float* sLD = za.sLD;
   const uint2* sInc = za.sInc;
   int* sM = za.sM;
   int* mycol = za.mycol;
@@ -238,7 +238,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               }
 #pragma unroll
               for (int off = 16; off > 0; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
-              if (lane == 0) atomicAdd(&sLD[row], (double)term);
+              if (lane == 0) sLD[row] += term;   // this warp's row: no other writer
             }
             if (LIKE) {
               // j + h is a compile-time constant after unrolling
@@ -348,7 +348,7 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   float2* sQ2 = reinterpret_cast<float2*>(smem + lay.q2);
   float2* sT2 = reinterpret_cast<float2*>(smem + lay.t2);
   float2* sX = reinterpret_cast<float2*>(smem + lay.x);
-  double* sLD = reinterpret_cast<double*>(smem + lay.ld);
+  float* sLD = reinterpret_cast<float*>(smem + lay.ld);   // [W][nT16]
   uint2* sInc = reinterpret_cast<uint2*>(smem + lay.inc);
   int* sM = reinterpret_cast<int*>(smem + lay.m);
   int* sN = reinterpret_cast<int*>(smem + lay.n);
@@ -379,7 +379,7 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     }
   }
   if (MODE == kZMetro)
-    for (int idx = threadIdx.x; idx < nT16; idx += NW32) sLD[idx] = 0.0;
+    for (int idx = threadIdx.x; idx < nT16 * W; idx += NW32) sLD[idx] = 0.0f;
   __syncthreads();
 
   // lane k < K extracts population k's field from the reduced words
@@ -420,7 +420,8 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     const uint32_t* grow = ch.g2 + (size_t)(valid ? l : 0) * ch.wpr;
     const float2* Xlane = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
     {
-      ZArgs za{&ch, grow, Xlane, sQ2, sT2, sLD, sInc, sM, mycol, i0, i1, nT16, l, K, L, lane,
+      ZArgs za{&ch, grow, Xlane, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
+               K, L, lane,
                my_word, my_shift, prep, key, stream, valid, pfonly};
       if (want_like) {
         if (store_z) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb);
@@ -453,8 +454,13 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     }
   }
   if (MODE == kZMetro) {
+    // the warps' partials in warp order: a fixed summation order
     double* dst = ch.ldpart + (size_t)grp * N + i0;
-    for (int idx = threadIdx.x; idx < nT; idx += NW32) dst[idx] = sLD[idx];
+    for (int idx = threadIdx.x; idx < nT; idx += NW32) {
+      double v = 0.0;
+      for (int w = 0; w < W; w++) v += (double)sLD[w * nT16 + idx];
+      dst[idx] = v;
+    }
   }
   if (errb) set_err(ch.err, errb);
 

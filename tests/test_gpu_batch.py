@@ -5,8 +5,9 @@ state as each chain advanced alone by st_sweep.
 
 Random draws are keyed by (chain seed, sweep, update, element), never by the
 launch, so batching changes no draw: Z counts, P, Q, eps, F, alpha and every
-sum must agree exactly.  The one exception is the Metropolis log ratio, whose
-per-row shared-memory sums are not order-fixed (compared to 1e-12).
+sum must agree exactly.  The Metropolis log ratio is a sum over locus groups
+whose partition follows the Z-pass tile, which a tuned batch may change; it is
+compared to 1e-12.
 """
 import numpy as np
 import pytest
