@@ -485,7 +485,7 @@ cudaError_t launch_b2g_kw(const LaunchSet& ls, int mode, int flags, size_t smem)
 #define ST_ZCASE(M)                                                                        \
   case M: {                                                                                \
     auto fn = zpass_b2g_kernel<KT, M, W>;                                                   \
-    if (smem > 48 * 1024)                                                                  \
+    if (smem > 40 * 1024) /* above the default 48 KB with the static smem */            \
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
     fn<<<grid, block, smem, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, flags);         \
     return cudaGetLastError();                                                             \
