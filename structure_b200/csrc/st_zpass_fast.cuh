@@ -144,14 +144,26 @@ __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, cons
   return s;
 }
 
+// The Metropolis pass (no draws, no counts) is bound by the shared-memory
+// data pipe, mostly the per-lane allele-table loads; it takes the lane's
+// frequencies from registers instead (K classes up to 6, where they fit
+// without spilling).
+// The counting pass is bound by the ALU pipe, where the selects would cost
+// more than the loads.
+__host__ __device__ constexpr bool zregx(int mode, int kt) { return mode == kZMetro && kt <= 6; }
+__host__ __device__ constexpr int zregn(int mode, int kt) { return zregx(mode, kt) ? kt : 1; }
+
 template <int KT, int MODE, int W, bool LIKE, bool SZ>
-__device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, int& errb) {
+__device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, int& errb,
+                                           const float (&p0r)[zregn(MODE, KT)],
+                                           const float (&p1r)[zregn(MODE, KT)]) {
   constexpr int NW32 = 32 * W;
   constexpr int KT2 = (KT + 1) & ~1;
   constexpr int NWM = (KT + 3) / 4;
   constexpr bool kUseP = (MODE == kZNormal || MODE == kZMetro || MODE == kZLike);
   constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
   constexpr bool kLut = kCounts && KT <= 8;
+  constexpr bool kRegX = zregx(MODE, KT);
   ChainDev& ch = *za.chp;
   const uint32_t* grow = za.grow;
   const float2* Xlane = za.Xlane;
@@ -192,9 +204,20 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               const float4 v = q4[k >> 1];
               Q2[k] = make_float2(v.x, v.y);
               Q2[k + 1] = make_float2(v.z, v.w);
-              const float4 xv = X4[(k >> 1) * NW32];
-              X[k] = make_float2(xv.x, xv.y);
-              X[k + 1] = make_float2(xv.z, xv.w);
+              if (!kRegX) {
+                const float4 xv = X4[(k >> 1) * NW32];
+                X[k] = make_float2(xv.x, xv.y);
+                X[k + 1] = make_float2(xv.z, xv.w);
+              }
+            }
+            if (kRegX) {
+              // (P[a0][k], P[a1][k]); a missing genotype reads class 1/1, and
+              // its terms are discarded below
+#pragma unroll
+              for (int k = 0; k < KT2; k++) {
+                const int kk = k < zregn(MODE, KT) ? k : 0;
+                X[k] = make_float2(a0 ? p1r[kk] : p0r[kk], a1 ? p1r[kk] : p0r[kk]);
+              }
             }
             Cs[0] = mul2_rn(Q2[0], X[0]);
 #pragma unroll
@@ -396,6 +419,10 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     if (lbase >= L) break;  // warp-uniform
     const int l = lbase + lane;
     const bool valid = l < L;
+    constexpr int NP = zregn(MODE, KT);
+    float p0r[NP], p1r[NP];   // Metropolis pass: this lane's P[l][k][0], P[l][k][1]
+#pragma unroll
+    for (int k = 0; k < NP; k++) p0r[k] = p1r[k] = 0.0f;
     if (kUseP) {
       // allele table of this lane's locus, per class g in {0/0, 0/1, 1/1}:
       // float4 (P[a0][k], P[a1][k], P[a0][k+1], P[a1][k+1]) per pair of k
@@ -408,6 +435,10 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
           const int kk = k + e;
           p0[e] = (valid && kk < K) ? ch.P[((size_t)l * K + kk) * A] : 0.0f;
           p1[e] = (valid && kk < K && A > 1) ? ch.P[((size_t)l * K + kk) * A + 1] : 0.0f;
+          if (zregx(MODE, KT) && kk < NP) {
+            p0r[kk < NP ? kk : 0] = p0[e];
+            p1r[kk < NP ? kk : 0] = p1[e];
+          }
         }
         X4w[(0 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
         X4w[(1 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
@@ -424,11 +455,11 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
                K, L, lane,
                my_word, my_shift, prep, key, stream, valid, pfonly};
       if (want_like) {
-        if (store_z) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb);
-        else zword_loop<KT, MODE, W, true, false>(za, like_acc, errb);
+        if (store_z) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb, p0r, p1r);
+        else zword_loop<KT, MODE, W, true, false>(za, like_acc, errb, p0r, p1r);
       } else {
-        if (store_z) zword_loop<KT, MODE, W, false, true>(za, like_acc, errb);
-        else zword_loop<KT, MODE, W, false, false>(za, like_acc, errb);
+        if (store_z) zword_loop<KT, MODE, W, false, true>(za, like_acc, errb, p0r, p1r);
+        else zword_loop<KT, MODE, W, false, false>(za, like_acc, errb, p0r, p1r);
       }
     }
     if (kCounts) {
