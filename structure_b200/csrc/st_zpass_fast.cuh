@@ -77,7 +77,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
   size_t o = 0;
   z.q2 = o; if (useP) o = zalign16(o + (size_t)T * KT2 * 8);            // (q,q) pairs
   z.t2 = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * KT2 * 8);  // (t,t) pairs
-  z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT2 * nw32 * 8);      // allele table
+  z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT * nw32 * 8);       // allele table
   z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * (nw32 / 32) * 4);   // per warp
   z.inc = o; if (counts && KT <= 8) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * 8);
   z.m = o;  if (counts) o = zalign16(o + (size_t)T * KT * 4);
@@ -103,7 +103,8 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
 struct ZArgs {
   ChainDev* chp;
   const uint32_t* grow;
-  const float2* Xlane;
+  const float2* Xlane;   // this lane's allele-table column (pairs of pairs)
+  const float2* Xtail;   // odd K classes: this lane's last pair
   const float2* sQ2;
   const float2* sT2;
   float* sLD;     // this warp's Metropolis log-ratio partials, one per row
@@ -121,20 +122,27 @@ struct ZArgs {
 // a term below kLikeFastMin.
 template <int KT, int W>
 __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, const float2* Xlane,
-                                               const float2* sQ2) {
+                                               const float2* Xtail, const float2* sQ2) {
   constexpr int NW32 = 32 * W;
   constexpr int KT2 = (KT + 1) & ~1;
+  constexpr int XP = KT / 2;
   double s = 0.0;
   for (int gi = 0; gi < 16; gi++) {
     const uint32_t g = (word >> (2 * gi)) & 3u;
     if (g == 3u) continue;
     const float4* q4 = reinterpret_cast<const float4*>(sQ2 + (row_base + gi) * KT2);
-    const float4* X4 = reinterpret_cast<const float4*>(Xlane) + g * ((KT2 / 2) * NW32);
+    const float4* X4 = reinterpret_cast<const float4*>(Xlane) + g * (XP * NW32);
     float2 C = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < KT2; k += 2) {
       const float4 v = q4[k >> 1];
-      const float4 xv = X4[(k >> 1) * NW32];
+      float4 xv;
+      if (k + 1 < KT) {
+        xv = X4[(k >> 1) * NW32];
+      } else {
+        const float2 t = Xtail[g * NW32];
+        xv = make_float4(t.x, t.y, 0.0f, 0.0f);
+      }
       if (k == 0) C = mul2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y));
       else C = fma2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y), C);
       if (k + 1 < KT) C = fma2_rn(make_float2(v.z, v.w), make_float2(xv.z, xv.w), C);
@@ -167,6 +175,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   ChainDev& ch = *za.chp;
   const uint32_t* grow = za.grow;
   const float2* Xlane = za.Xlane;
+  const float2* Xtail = za.Xtail;
   const float2* sQ2 = za.sQ2;
   const float2* sT2 = za.sT2;
   float* sLD = za.sLD;
@@ -196,7 +205,8 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
           int z0 = 0, z1 = 0;
           if (kUseP) {
             const float4* q4 = reinterpret_cast<const float4*>(sQ2 + row * KT2);
-            const float4* X4 = reinterpret_cast<const float4*>(Xlane) + (miss ? 0u : g) * ((KT2 / 2) * NW32);
+            const uint32_t cls = miss ? 0u : g;
+            const float4* X4 = reinterpret_cast<const float4*>(Xlane) + cls * ((KT / 2) * NW32);
             float2 Cs[KT];
             float2 Q2[KT2], X[KT2];
 #pragma unroll
@@ -205,9 +215,14 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               Q2[k] = make_float2(v.x, v.y);
               Q2[k + 1] = make_float2(v.z, v.w);
               if (!kRegX) {
-                const float4 xv = X4[(k >> 1) * NW32];
-                X[k] = make_float2(xv.x, xv.y);
-                X[k + 1] = make_float2(xv.z, xv.w);
+                if (k + 1 < KT) {
+                  const float4 xv = X4[(k >> 1) * NW32];
+                  X[k] = make_float2(xv.x, xv.y);
+                  X[k + 1] = make_float2(xv.z, xv.w);
+                } else {   // odd K class: the last pair from its own 8-byte table
+                  X[k] = Xtail[cls * NW32];
+                  X[k + 1] = make_float2(0.0f, 0.0f);
+                }
               }
             }
             if (kRegX) {
@@ -328,7 +343,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
         double wl = (double)wlike;
         if (__any_sync(0xffffffffu, !(wmin > kLikeFastMin))) {   // once per word, rare
           if (!(wmin > kLikeFastMin))
-            wl = word_like_exact<KT, W>(word, wi << 4, Xlane, sQ2);
+            wl = word_like_exact<KT, W>(word, wi << 4, Xlane, Xtail, sQ2);
         }
         like_acc += wl;
       }
@@ -425,8 +440,13 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     for (int k = 0; k < NP; k++) p0r[k] = p1r[k] = 0.0f;
     if (kUseP) {
       // allele table of this lane's locus, per class g in {0/0, 0/1, 1/1}:
-      // float4 (P[a0][k], P[a1][k], P[a0][k+1], P[a1][k+1]) per pair of k
+      // float4 (P[a0][k], P[a1][k], P[a0][k+1], P[a1][k+1]) per pair of k; for
+      // odd K classes the last (P[a0][k], P[a1][k]) goes to a float2 table, so
+      // the warp reads it in two shared-memory wavefronts instead of four
+      constexpr int XP = KT / 2;
       float4* X4w = reinterpret_cast<float4*>(sX) + threadIdx.x;
+      float2* XTw = reinterpret_cast<float2*>(reinterpret_cast<float4*>(sX) + 3 * XP * NW32) +
+                    threadIdx.x;
 #pragma unroll
       for (int k = 0; k < KT2; k += 2) {
         float p0[2], p1[2];
@@ -440,9 +460,15 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
             p1r[kk < NP ? kk : 0] = p1[e];
           }
         }
-        X4w[(0 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
-        X4w[(1 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
-        X4w[(2 * (KT2 / 2) + (k >> 1)) * NW32] = make_float4(p1[0], p1[0], p1[1], p1[1]);
+        if (k + 1 < KT) {
+          X4w[(0 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
+          X4w[(1 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
+          X4w[(2 * XP + (k >> 1)) * NW32] = make_float4(p1[0], p1[0], p1[1], p1[1]);
+        } else {
+          XTw[0 * NW32] = make_float2(p0[0], p0[0]);
+          XTw[1 * NW32] = make_float2(p0[0], p1[0]);
+          XTw[2 * NW32] = make_float2(p1[0], p1[0]);
+        }
       }
     }
     if (kCounts)
@@ -450,8 +476,10 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     __syncwarp();
     const uint32_t* grow = ch.g2 + (size_t)(valid ? l : 0) * ch.wpr;
     const float2* Xlane = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
+    const float2* Xtail = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) +
+                                                          3 * (KT / 2) * NW32) + threadIdx.x;
     {
-      ZArgs za{&ch, grow, Xlane, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
+      ZArgs za{&ch, grow, Xlane, Xtail, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
                K, L, lane,
                my_word, my_shift, prep, key, stream, valid, pfonly};
       if (want_like) {
