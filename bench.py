@@ -279,15 +279,22 @@ def run_ours(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     data2 = api.Data(ctx, na, packed=ppk, num_inds=N, num_loci=L, layout=api.LAYOUT_B2G)
+    t1 = time.perf_counter()
     mk2 = model_kwargs(burnin=0, numreps=S)
     ch2 = [api.Chain(ctx, data2, api.model_defaults(**mk2), 9000 + r) for r in range(B)]
     b2 = api.Batch(ctx, ch2)
+    t2 = time.perf_counter()
     b2.sweep(S)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
     d2h = 0
     for c in ch2:
         for f in (api.F_QSUM, api.F_PSUM, api.F_STATS, api.F_ALPHA, api.F_F):
             d2h += c.get(f).nbytes
     t_e2e = time.perf_counter() - t0
+    e2e_parts = {"upload_ms": round((t1 - t0) * 1e3, 2), "create_ms": round((t2 - t1) * 1e3, 2),
+                 "sweeps_ms": round((t3 - t2) * 1e3, 2),
+                 "d2h_ms": round((t0 + t_e2e - t3) * 1e3, 2)}
     e2e = B * S / t_e2e
     b2.close()
     for c in ch2:
@@ -338,7 +345,7 @@ def run_ours(args):
         "mean_lnpd_over_chains": round(float(np.mean(like)), 2),
         "e2e": {"value": round(e2e, 3), "unit": METRIC,
                 "h2d_bytes_per_step": int(math.ceil(packed.nbytes / S)),
-                "d2h_bytes_per_step": int(math.ceil(d2h / S)),
+                "d2h_bytes_per_step": int(math.ceil(d2h / S)), "parts": e2e_parts,
                 "includes": "st_data_upload from pinned host words, 20 x st_chain_create "
                             "(initial Z pass), st_batch_sweep, st_get_state of QSum/PSum/"
                             "stats/alpha/F"},

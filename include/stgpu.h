@@ -330,8 +330,10 @@ size_t st_field_bytes(st_chain *c, int field);
  * st_chain_save writes every array of the chain, its sweep counter and its
  * random-stream key to a file; st_chain_load restores them into a chain
  * created on the same data with the same K, layout and options (seed
- * irrelevant).  Draws are keyed by (seed, sweep, update, element), so the
- * loaded chain continues exactly as the saved one would have.             */
+ * irrelevant; its Z-pass tile may differ).  Draws are keyed by (seed,
+ * sweep, update, element), so the loaded chain continues exactly as the
+ * saved one would have.  Load before putting the chain in a batch: a batch
+ * keeps its own copy of each chain's descriptor from st_batch_create.      */
 int st_chain_save(st_chain *c, const char *path);
 int st_chain_load(st_chain *c, const char *path);
 

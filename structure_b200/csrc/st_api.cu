@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <unordered_map>
 #include <cuda_runtime.h>
 #include "stgpu.h"
 #include "st_kernels.h"
@@ -28,6 +29,12 @@ struct st_ctx {
   std::vector<Ev> evs;
   double prof_ms[ST_K_COUNT] = {0};
   int64_t prof_n[ST_K_COUNT] = {0};
+  // device blocks of destroyed chains / data sets kept for reuse: creating
+  // chains of a shape seen before then needs no cudaMalloc (whose cost swings
+  // by tens of ms when the driver must map fresh memory)
+  std::multimap<size_t, void*> cache;   // size -> block
+  size_t cached = 0;
+  std::unordered_map<void*, size_t> live;   // block -> size, for ctx_free
 };
 
 struct st_data {
@@ -129,6 +136,17 @@ int cuda_check(st_ctx* ctx, cudaError_t e, const char* what) {
     if (_r != ST_OK) return _r;                                       \
   } while (0)
 
+constexpr size_t kCacheMax = (size_t)8 << 30;   // bytes kept for reuse per context
+
+void ctx_release_cache(st_ctx* ctx) {
+  for (auto& kv : ctx->cache) cudaFree(kv.second);
+  ctx->cache.clear();
+  ctx->cached = 0;
+}
+
+// Device memory for a chain, data set or gradient workspace, under the
+// context's admission budget; a cached block of a fitting size (at most a
+// quarter larger) is reused before cudaMalloc is called.
 int ctx_alloc(st_ctx* ctx, size_t bytes, void** p, std::vector<void*>* track, size_t* acc) {
   *p = nullptr;
   if (bytes == 0) return ST_OK;
@@ -136,15 +154,49 @@ int ctx_alloc(st_ctx* ctx, size_t bytes, void** p, std::vector<void*>* track, si
     return seterr(ctx, ST_ERR_ADMISSION,
                   "admission: %zu bytes requested, %zu of %zu in use", bytes, ctx->in_use,
                   ctx->budget);
-  cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return seterr(ctx, ST_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  size_t got = bytes;
+  auto it = ctx->cache.lower_bound(bytes);
+  if (it != ctx->cache.end() && it->first <= bytes + bytes / 4) {
+    got = it->first;
+    *p = it->second;
+    ctx->cached -= got;
+    ctx->cache.erase(it);
+  } else {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess && ctx->cached) {   // give the cache back and try again
+      cudaGetLastError();
+      ctx_release_cache(ctx);
+      e = cudaMalloc(p, bytes);
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      return seterr(ctx, ST_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
   }
-  ctx->in_use += bytes;
+  ctx->live[*p] = got;
+  ctx->in_use += got;
   if (track) track->push_back(*p);
-  if (acc) *acc += bytes;
+  if (acc) *acc += got;
   return ST_OK;
+}
+
+// Returns a block from ctx_alloc.  The caller has synchronised whatever may
+// still use it; the block goes to the cache (or back to the driver when the
+// cache is full).
+void ctx_free(st_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = ctx->live.find(p);
+  if (it == ctx->live.end()) return;
+  const size_t n = it->second;
+  ctx->live.erase(it);
+  ctx->in_use -= n;
+  if (ctx->cached + n <= kCacheMax) {
+    ctx->cache.emplace(n, p);
+    ctx->cached += n;
+  } else {
+    cudaFree(p);
+  }
 }
 
 int pow2_at_least(int k) {
@@ -350,6 +402,7 @@ extern "C" int st_ctx_destroy(st_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  ctx_release_cache(ctx);
   cudaStreamDestroy(ctx->own);
   delete ctx;
   return ST_OK;
@@ -521,7 +574,7 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
   if (rc) { delete s; return rc; }
   s->numalleles = (int32_t*)p;
   rc = ctx_alloc(ctx, sizeof(int32_t) * N, &p, nullptr, &s->bytes);
-  if (rc) { cudaFree(s->numalleles); delete s; return rc; }
+  if (rc) { ctx_free(ctx, s->numalleles); delete s; return rc; }
   s->popflags = (int32_t*)p;
   cudaMemcpy(s->numalleles, s->na_h.data(), sizeof(int32_t) * L, cudaMemcpyHostToDevice);
   std::vector<int32_t> pf(N, 0);
@@ -532,8 +585,8 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
   if (d->location) {
     for (int i = 0; i < N; i++)
       if (d->location[i] < 0) {
-        cudaFree(s->numalleles);
-        cudaFree(s->popflags);
+        ctx_free(ctx, s->numalleles);
+        ctx_free(ctx, s->popflags);
         delete s;
         // src/Util.c:241-246
         return seterr(ctx, ST_ERR_ARG, "individual %d has negative location %d", i, d->location[i]);
@@ -592,9 +645,9 @@ extern "C" int st_data_destroy(st_data* s) {
   if (!s) return ST_ERR_ARG;
   if (s->chains > 0) return seterr(s->ctx, ST_ERR_STATE, "data still used by %d chains", s->chains);
   cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
   for (void* p : {(void*)s->g2, (void*)s->g8, (void*)s->numalleles, (void*)s->popflags})
-    if (p) cudaFree(p);
-  s->ctx->in_use -= s->bytes;
+    ctx_free(s->ctx, p);
   delete s;
   return ST_OK;
 }
@@ -970,9 +1023,8 @@ extern "C" int st_chain_destroy(st_chain* c) {
   if (!c) return ST_ERR_ARG;
   cudaSetDevice(c->ctx->device);
   cudaStreamSynchronize(c->ctx->stream);
-  for (void* p : c->allocs) cudaFree(p);
-  if (c->d_injected) { cudaFree(c->d_injected); c->ctx->in_use -= c->injected_n * 8; }
-  c->ctx->in_use -= c->bytes;
+  for (void* p : c->allocs) ctx_free(c->ctx, p);
+  if (c->d_injected) ctx_free(c->ctx, c->d_injected);
   if (c->h.N) c->data->chains--;
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1099,7 +1151,10 @@ extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int 
   if (precision != 32 && precision != 64) return seterr(c->ctx, ST_ERR_ARG, "precision 32 or 64");
   cudaSetDevice(c->ctx->device);
   if (c->injected_n != n) {
-    if (c->d_injected) { cudaFree(c->d_injected); c->ctx->in_use -= c->injected_n * 8; }
+    if (c->d_injected) {
+      cudaStreamSynchronize(c->ctx->stream);
+      ctx_free(c->ctx, c->d_injected);
+    }
     c->d_injected = nullptr;
     c->injected_n = 0;
     void* p;
@@ -1939,8 +1994,7 @@ extern "C" int st_grad_create(st_ctx* ctx, st_data* data, int maxpops, int preci
   for (auto& r : req) {
     int rc = ctx_alloc(ctx, r.b, r.p, &g->allocs, &g->bytes);
     if (rc) {
-      for (void* p : g->allocs) cudaFree(p);
-      ctx->in_use -= g->bytes;
+      for (void* p : g->allocs) ctx_free(ctx, p);
       delete g;
       return rc;
     }
@@ -1953,8 +2007,7 @@ extern "C" int st_grad_destroy(st_grad* g) {
   if (!g) return ST_ERR_ARG;
   cudaSetDevice(g->ctx->device);
   cudaStreamSynchronize(g->ctx->stream);
-  for (void* p : g->allocs) cudaFree(p);
-  g->ctx->in_use -= g->bytes;
+  for (void* p : g->allocs) ctx_free(g->ctx, p);
   delete g;
   return ST_OK;
 }
@@ -1988,7 +2041,7 @@ extern "C" int st_loglik_grad(st_grad* g, const void* q_logits, const void* p_lo
 namespace {
 
 constexpr char kCkptMagic[8] = {'S', 'T', 'G', 'P', 'U', 'C', 'K', '1'};
-constexpr int32_t kCkptVersion = 1;
+constexpr int32_t kCkptVersion = 2;   // 1 also held the Metropolis scratch (ldpart)
 
 struct CkField { void* p; size_t bytes; };
 
@@ -2002,7 +2055,7 @@ std::vector<CkField> ckpt_fields(st_chain* c) {
       {h.Q, NK * 4}, {h.logQ, NK * 4}, {h.TestQ, NK * 4}, {h.logTestQ, NK * 4},
       {h.P, LKA * 4}, {h.logP, LKA * 4}, {h.eps, LA * 8}, {h.F, (size_t)h.K * 8},
       {h.alpha, arow_n(h) * 8}, {h.lambda, (size_t)h.K * 8}, {h.npart, LKA * 4},
-      {h.mpart, NK * 4}, {h.ldpart, (size_t)h.ngroups * h.N * 8}, {h.QSum, NK * 8},
+      {h.mpart, NK * 4}, {h.QSum, NK * 8},
       {h.PSum, LKA * 8}, {h.SumEps, LA * 8}, {h.FstSum, (size_t)h.K * 8},
       {h.sumAlpha, arow_n(h) * 8}, {h.sumlambda, (size_t)h.K * 8},
       {h.stats, (size_t)kStSize * 8}, {h.err, 4}};
@@ -2066,10 +2119,17 @@ extern "C" int st_chain_load(st_chain* c, const char* path) {
             fread(hdr, 4, 12, f) == 12 && fread(&key, 4, 1, f) == 1 &&
             fread(&model, sizeof(st_model), 1, f) == 1;
   ckpt_header(c, mine);
+  if (ok && hdr[0] != kCkptVersion) {
+    fclose(f);
+    return seterr(ctx, ST_ERR_STATE, "%s has checkpoint format %d; this library reads %d", path,
+                  hdr[0], kCkptVersion);
+  }
   // the chain must have been created on the same data with the same shape;
-  // the sweep counter (slot 7) is what the file restores
+  // the sweep counter (slot 7) is what the file restores, and the Z-pass
+  // locus grouping (slot 6) may differ (tiles are chosen per chain or batch
+  // and nothing saved depends on them)
   for (int j = 0; ok && j < 12; j++)
-    if (j != 7 && hdr[j] != mine[j]) ok = false;
+    if (j != 7 && j != 6 && hdr[j] != mine[j]) ok = false;
   if (!ok) {
     fclose(f);
     return seterr(ctx, ST_ERR_STATE, "%s is not a checkpoint of a chain of this shape", path);

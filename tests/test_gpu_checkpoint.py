@@ -45,3 +45,35 @@ def test_resume_continues_exactly(ctx, tmp_path, kind):
     for x in (a, b, c):
         x.close()
     data.close()
+
+
+def test_resume_into_a_chain_with_another_tile(ctx, tmp_path):
+    """A chain saved after st_batch_autotune changed its Z-pass tile loads into
+    a fresh chain with the starting tile and continues exactly: nothing saved
+    depends on the tile."""
+    d = synth.snp_fmodel(300, 3000, 3, np.linspace(0.05, 0.2, 3), 0.4, 0.03, 12)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], layout=api.LAYOUT_B2G,
+                    num_inds=300, num_loci=3000)
+    m = api.model_defaults(maxpops=3, burnin=2, numreps=20, freqscorr=1, metrofreq=3)
+    a = api.Chain(ctx, data, m, 77)
+    b = api.Batch(ctx, [a])
+    b.sweep(2)
+    b.autotune(1)
+    b.sweep(2)
+    path = str(tmp_path / "tuned.ckpt")
+    a.save(path)
+    b.sweep(4)
+    fresh = api.Chain(ctx, data, m, 1)
+    fresh.load(path)
+    fresh.sweep(4)
+    assert a.sync() == 0 and fresh.sync() == 0
+    for f in FIELDS:
+        if f == api.F_STATS:
+            # ln P(D) partial sums follow the tile's locus grouping
+            np.testing.assert_allclose(a.get(f), fresh.get(f), rtol=1e-12)
+        else:
+            np.testing.assert_array_equal(a.get(f), fresh.get(f), err_msg=f"field {f}")
+    b.close()
+    for x in (a, fresh):
+        x.close()
+    data.close()
