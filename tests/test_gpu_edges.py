@@ -165,3 +165,26 @@ def test_invalid_inputs_are_refused(ctx):
         m = api.model_defaults(**kw)
         assert code(lambda: api.Chain(ctx, d, m, 1)) == want, kw
     d.close()
+
+
+def test_reused_device_blocks_give_identical_chains(ctx):
+    """A chain created in the device blocks a destroyed chain left in the
+    context's cache starts from the same state as one in fresh memory: same
+    seed, same sweeps, same result; the cached blocks are not counted as in use."""
+    geno, na = _snp(120, 400, seed=21)
+    base, _ = ctx.memory()
+    d = api.Data(ctx, na, geno=geno, layout=api.LAYOUT_B2G)
+    m = api.model_defaults(maxpops=3, burnin=3, numreps=6, freqscorr=1, metrofreq=2)
+    runs = []
+    for _ in range(2):
+        c = api.Chain(ctx, d, m, 4242)
+        c.sweep(6)
+        assert c.sync() == 0
+        runs.append([c.get(f) for f in (api.F_Q, api.F_P, api.F_QSUM, api.F_STATS)])
+        used, _ = ctx.memory()
+        c.close()
+    for a, b in zip(*runs):
+        np.testing.assert_array_equal(a, b)
+    d.close()
+    assert ctx.memory()[0] == base
+    assert used > base
