@@ -189,6 +189,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
     for (int wi = 0; wi < (nT16 >> 4); wi++) {
       const uint32_t word = valid ? __ldg(grow + (i0 >> 4) + wi) : 0xFFFFFFFFu;
       float wlike = 0.0f, wprod = 1.0f, wmin = 1.0f;
+      float tr[MODE == kZMetro ? 16 : 1];   // Metropolis pass: this lane's term per row
 #pragma unroll
       for (int j = 0; j < 16; j += 2) {
         const int row0 = (wi << 4) + j;              // chunk-relative individual
@@ -274,9 +275,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
                   term = (float)(log((double)S.x) + log((double)S.y) - log((double)Tp.x) -
                                  log((double)Tp.y));
               }
-#pragma unroll
-              for (int off = 16; off > 0; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
-              if (lane == 0) sLD[row] += term;   // this warp's row: no other writer
+              tr[MODE == kZMetro ? j + h : 0] = term;
             }
             if (LIKE) {
               // j + h is a compile-time constant after unrolling
@@ -338,6 +337,33 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
             ch.Z[zi + L] = miss ? kZMissing : (uint8_t)z1;
           }
         }
+      }
+      if constexpr (MODE == kZMetro) {
+        // the word's 16 row sums over the warp's 32 loci by a transposed
+        // butterfly: at the exchange across lane bit b a lane keeps the half
+        // of its rows picked by its own bit b and adds its partner's partial
+        // for the same rows; after lane bits 4..1 lanes 2r, 2r+1 hold row r.
+        // 31 exchanges per word instead of 5 per row.
+        float v8[8], v4[4], v2[2];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const bool hi = lane & 16;
+          v8[i] = (hi ? tr[i + 8] : tr[i]) + __shfl_xor_sync(0xffffffffu, hi ? tr[i] : tr[i + 8], 16);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const bool hi = lane & 8;
+          v4[i] = (hi ? v8[i + 4] : v8[i]) + __shfl_xor_sync(0xffffffffu, hi ? v8[i] : v8[i + 4], 8);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const bool hi = lane & 4;
+          v2[i] = (hi ? v4[i + 2] : v4[i]) + __shfl_xor_sync(0xffffffffu, hi ? v4[i] : v4[i + 2], 4);
+        }
+        const bool hi = lane & 2;
+        float v = (hi ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, hi ? v2[0] : v2[1], 2);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        if (!(lane & 1)) sLD[(wi << 4) + (lane >> 1)] += v;   // this warp's rows only
       }
       if (LIKE) {
         double wl = (double)wlike;
