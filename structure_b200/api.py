@@ -265,9 +265,17 @@ class Chain:
                 F_QSUM: (N, K), F_PSUM: (L, K, A), F_STATS: (256,), F_DIMS: (8,),
                 F_MALA_EPS: (N,), F_USEPOPPROBS: (N, K, -1)}.get(f, None)
 
-    def get(self, f):
+    def get(self, f, out=None):
+        """Copy field f to the host.  `out`, if given, is a C-contiguous array of
+        the field's type and size (page-locked memory makes the copy a direct DMA)
+        and is filled and returned in the field's shape."""
         n = lib().st_field_bytes(self.h, f)
-        out = np.zeros(n // np.dtype(_DT[f]).itemsize, _DT[f])
+        if out is None:
+            out = np.zeros(n // np.dtype(_DT[f]).itemsize, _DT[f])
+        elif (out.dtype != np.dtype(_DT[f]) or out.nbytes != n
+              or not out.flags["C_CONTIGUOUS"]):
+            raise StError(ST_ERR_ARG, "field %d: output array must be C-contiguous %s of %d bytes"
+                          % (f, np.dtype(_DT[f]).name, n))
         self.ctx.check(lib().st_get_state(self.h, f, out.ctypes.data, n))
         shp = self._shape(f) if f != F_DIMS else (8,)
         if f == F_ANCESTDIST:

@@ -188,3 +188,26 @@ def test_reused_device_blocks_give_identical_chains(ctx):
     d.close()
     assert ctx.memory()[0] == base
     assert used > base
+
+
+def test_get_into_caller_array(ctx):
+    """Chain.get(f, out=...) fills a caller-owned (here page-locked) array with
+    the same bytes as a fresh copy, and refuses an array of the wrong size or type."""
+    import torch
+    geno, na = _snp(60, 300, seed=23)
+    d = api.Data(ctx, na, geno=geno, layout=api.LAYOUT_B2G)
+    c = api.Chain(ctx, d, api.model_defaults(maxpops=4, burnin=1, numreps=4, freqscorr=1), 99)
+    c.sweep(4)
+    for f in (api.F_QSUM, api.F_PSUM, api.F_STATS, api.F_ALPHA, api.F_F):
+        ref = c.get(f)
+        buf = torch.empty(ref.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(ref.dtype)
+        got = c.get(f, out=buf)
+        np.testing.assert_array_equal(got, ref)
+        assert np.shares_memory(got, buf)
+    q = c.get(api.F_QSUM)
+    with pytest.raises(api.StError):
+        c.get(api.F_QSUM, out=np.zeros(q.size + 1, q.dtype))
+    with pytest.raises(api.StError):
+        c.get(api.F_QSUM, out=np.zeros(q.size, np.float32))
+    c.close()
+    d.close()
