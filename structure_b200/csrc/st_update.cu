@@ -75,7 +75,8 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         int n = 0;
         for (int cc = 0; cc < ch.cnt_chunks; cc++)
           n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
-        if (ch.freqscorr) return ch.eps[(size_t)l * A + a] * (1.0 - ch.F[k]) / ch.F[k] + (double)n;
+        // eps (1-F)/F + n (Updates/UpdateP.c:161-164), with (1-F)/F formed once per CTA
+        if (ch.freqscorr) return ch.eps[(size_t)l * A + a] * sFrac[k] + (double)n;
         return ch.lambda[k] + (double)n;
       };
       auto emit = [&](int a, double lg, double ls, int nac) {

@@ -258,6 +258,35 @@ def test_updateq_metro_matches_oracle(ctx, orc, layout):
     c.close(); d.close()
 
 
+@pytest.mark.parametrize("K,layout", [(5, api.LAYOUT_B2G), (7, api.LAYOUT_B2G),
+                                      (10, api.LAYOUT_B2G), (13, api.LAYOUT_B2G),
+                                      (16, api.LAYOUT_B2G), (24, api.LAYOUT_B2G),
+                                      (32, api.LAYOUT_B2G), (10, api.LAYOUT_U8)])
+def test_metro_logdiff_across_k_classes(ctx, orc, K, layout):
+    """The Metropolis data pass of each K-class family (allele frequencies in
+    registers up to class 6, shared allele tables above it, two-warp CTAs from
+    class 16; the one-byte layout's own pass) against the oracle's FP64 sums,
+    with rows not a multiple of 16 and loci not a multiple of 32; then the
+    accept step on the device's ratios, exactly."""
+    geno, na, _ = _snp(N=137, L=333, K=4, seed=40 + K)
+    N, _, L = geno.shape
+    d, c = _chain(ctx, geno, na, K, layout=layout, metrofreq=10, alpha=0.5)
+    Q, P = _rand_state(np.random.default_rng(K), N, L, K, na)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    lQ = c.get(api.F_LOGQ)
+    c.set(api.F_REP, np.array([20], np.int32))
+    c.UpdateQ()
+    assert c.sync() == 0
+    ld_dev = c.get(api.F_LOGDIFF)
+    ld_o = orc.metro_logdiff(geno, Q, c.get(api.F_TESTQ), P)
+    np.testing.assert_allclose(ld_dev, ld_o, rtol=1e-5, atol=2e-3)
+    Qo, _, _ = orc.metro_accept(ld_dev, SEED, 20, Q, lQ, c.get(api.F_TESTQ),
+                                c.get(api.F_LOGTESTQ))
+    np.testing.assert_array_equal(c.get(api.F_Q), Qo)
+    c.close(); d.close()
+
+
 # ---------------------------------------------------------------------------
 # alpha, eps, F
 # ---------------------------------------------------------------------------
