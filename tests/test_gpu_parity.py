@@ -137,8 +137,10 @@ def test_updatez_fast_path_many_draws_bitexact(ctx, orc):
     c.close(); d.close()
 
 
-@pytest.mark.parametrize("K", [1, 2, 5, 7, 13])
+@pytest.mark.parametrize("K", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13])
 def test_fast_path_padded_k_bitexact(ctx, orc, K):
+    """Every K class up to 12 and a padded one (13 in class 16): Z and counts
+    bit-exact, ln P(D) of the same state within 1e-5."""
     geno, na, _ = _snp(N=130, L=300, K=3, seed=K)
     N, _, L = geno.shape
     rng = np.random.default_rng(K)
@@ -152,6 +154,8 @@ def test_fast_path_padded_k_bitexact(ctx, orc, K):
     assert (_zdev(c) == zo).all()
     n_o, m_o = orc.counts(geno, zo, K, c.A)
     assert (c.get(api.F_N) == n_o).all() and (c.get(api.F_M) == m_o).all()
+    like, lo = c.CalcLike(), orc.calc_like(geno, Q, P)
+    assert abs(like - lo) <= 1e-5 * abs(lo)
     c.close(); d.close()
 
 
