@@ -95,3 +95,37 @@ def test_reference_chain_driver_runs(ref):
     assert v["rep"] == 9 and np.isfinite(v["sumlikes"]) and v["sumlikes"] < 0
     np.testing.assert_allclose(v["QSum"].sum(1), 6.0, rtol=1e-9)
     assert (v["Geno"] == d["geno"]).all()      # the reference's recoding == synth.recode
+
+
+def test_get_into_caller_array_checks_type_and_size(monkeypatch):
+    """Chain.get(f, out=...) hands the caller's array to st_get_state and
+    refuses, before any library call, one of the wrong type, size or layout."""
+    from structure_b200 import api
+
+    calls = []
+
+    class FakeLib:
+        def st_field_bytes(self, h, f):
+            return 6 * 8
+
+        def st_get_state(self, h, f, ptr, n):
+            calls.append((ptr, n))
+            return 0
+
+    class FakeCtx:
+        def check(self, rc):
+            assert rc == 0
+
+    monkeypatch.setattr(api, "lib", lambda: FakeLib())
+    c = api.Chain.__new__(api.Chain)
+    c.h, c.ctx = 1, FakeCtx()
+    monkeypatch.setattr(c, "_shape", lambda f: (2, 3), raising=False)
+    buf = np.empty(6, np.float64)
+    got = c.get(api.F_QSUM, out=buf)
+    assert got.shape == (2, 3) and np.shares_memory(got, buf)
+    assert calls == [(buf.ctypes.data, 48)]
+    for bad in (np.empty(7), np.empty(6, np.float32), np.empty(12)[::2]):
+        with pytest.raises(api.StError) as e:
+            c.get(api.F_QSUM, out=bad)
+        assert e.value.code == api.ST_ERR_ARG
+    assert len(calls) == 1
