@@ -459,37 +459,61 @@ extern "C" int st_ctx_memory(const st_ctx* ctx, size_t* in_use, size_t* budget) 
 
 // ===========================================================================
 // data
-// Allele counts of each locus of 2-bit packed data, 16 genotypes per word:
-// with lo / hi the low / high bit of every code, popcounts give the number
-// of codes 1 (lo & ~hi), 2 (hi & ~lo) and 3 = missing (lo & hi).  Built
-// twice: with the popcnt instruction where the host has it, else generic.
+// Allele counts of each locus of 2-bit packed data, 16 genotypes per word,
+// on the device after the upload: one warp per locus row.  With lo / hi the
+// low / high bit of every code, popcounts give the number of codes 1
+// (lo & ~hi), 2 (hi & ~lo) and 3 = missing (lo & hi); padding genotypes of
+// the last word are masked off.  Feeds the initial eps (Init.c:173-240).
 namespace {
-template <int kTag>
-__attribute__((always_inline)) inline void count_b2g(const uint32_t* packed, int N, int L, int A, int64_t* cnt, int64_t* tot) {
-  const int wpr = (N + 15) / 16;
+__global__ void count_b2g_kernel(const uint32_t* __restrict__ g2, int N, int L, int wpr, int A,
+                                 long long* __restrict__ cnt, long long* __restrict__ tot) {
+  const int l = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (l >= L) return;   // warp-uniform
   const uint32_t tail = (N & 15) ? (0x55555555u >> (2 * (16 - (N & 15)))) : 0x55555555u;
-  for (int l = 0; l < L; l++) {
-    const uint32_t* row = packed + (size_t)l * wpr;
-    int64_t n1 = 0, n2 = 0, n3 = 0;
-    for (int w = 0; w < wpr; w++) {
-      const uint32_t valid = w == wpr - 1 ? tail : 0x55555555u;
-      const uint32_t lo = row[w] & valid, hi = (row[w] >> 1) & valid;
-      n1 += __builtin_popcount(lo & ~hi);
-      n2 += __builtin_popcount(hi & ~lo);
-      n3 += __builtin_popcount(lo & hi);
-    }
-    const int64_t n0 = (int64_t)N - n1 - n2 - n3;
+  const uint32_t* row = g2 + (size_t)l * wpr;
+  unsigned n1 = 0, n2 = 0, n3 = 0;
+  for (int w = lane; w < wpr; w += 32) {
+    const uint32_t valid = w == wpr - 1 ? tail : 0x55555555u;
+    const uint32_t x = row[w];
+    const uint32_t lo = x & valid, hi = (x >> 1) & valid;
+    n1 += __popc(lo & ~hi);
+    n2 += __popc(hi & ~lo);
+    n3 += __popc(lo & hi);
+  }
+  n1 = __reduce_add_sync(0xffffffffu, n1);
+  n2 = __reduce_add_sync(0xffffffffu, n2);
+  n3 = __reduce_add_sync(0xffffffffu, n3);
+  if (lane == 0) {
+    const long long n0 = (long long)N - n1 - n2 - n3;
     tot[l] = 2 * (n0 + n1 + n2);
-    cnt[(size_t)l * A + 0] = 2 * n0 + n1;
-    if (A > 1) cnt[(size_t)l * A + 1] = 2 * n2 + n1;
+    cnt[(size_t)l * A] = 2 * n0 + n1;
+    if (A > 1) cnt[(size_t)l * A + 1] = 2 * (long long)n2 + n1;
   }
 }
-__attribute__((target("popcnt"))) void count_b2g_popcnt(const uint32_t* p, int N, int L, int A,
-                                                        int64_t* cnt, int64_t* tot) {
-  count_b2g<1>(p, N, L, A, cnt, tot);
-}
-void count_b2g_generic(const uint32_t* p, int N, int L, int A, int64_t* cnt, int64_t* tot) {
-  count_b2g<0>(p, N, L, A, cnt, tot);
+
+// Runs count_b2g_kernel on the uploaded words and reads the counts back.
+int count_b2g_device(st_ctx* ctx, const uint32_t* g2, int N, int L, int wpr, int A,
+                     int64_t* cnt_h, int64_t* tot_h) {
+  void* p = nullptr;
+  size_t scratch = 0;
+  const size_t ncnt = (size_t)L * A;
+  int rc = ctx_alloc(ctx, sizeof(long long) * (ncnt + L), &p, nullptr, &scratch);
+  if (rc) return rc;
+  long long* cnt = (long long*)p;
+  long long* tot = cnt + ncnt;
+  cudaStream_t s = ctx->stream;
+  const int block = 256;
+  const unsigned grid = (unsigned)(((size_t)L * 32 + block - 1) / block);
+  count_b2g_kernel<<<grid, block, 0, s>>>(g2, N, L, wpr, A, cnt, tot);
+  rc = cuda_check(ctx, cudaGetLastError(), "count alleles");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(cnt_h, cnt, sizeof(long long) * ncnt,
+                                                cudaMemcpyDeviceToHost, s), "read counts");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(tot_h, tot, sizeof(long long) * L,
+                                                cudaMemcpyDeviceToHost, s), "read totals");
+  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "count alleles");
+  ctx_free(ctx, p);
+  return rc;
 }
 }  // namespace
 
@@ -552,8 +576,7 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
       delete s;
       return seterr(ctx, ST_ERR_ARG, "packed genotypes need <= 2 alleles per locus");
     }
-    if (__builtin_cpu_supports("popcnt")) count_b2g_popcnt(d->packed, N, L, A, s->cnt_h.data(), s->tot_h.data());
-    else count_b2g_generic(d->packed, N, L, A, s->cnt_h.data(), s->tot_h.data());
+    // allele counts: on the device once the words are there (below)
   }
   int layout = d->layout;
   if (layout == ST_LAYOUT_AUTO) layout = b2g_ok ? ST_LAYOUT_B2G : ST_LAYOUT_U8;
@@ -616,6 +639,8 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
     s->g2 = (uint32_t*)p;
     rc = cuda_check(ctx, cudaMemcpy(s->g2, src, sizeof(uint32_t) * (size_t)L * wpr,
                                     cudaMemcpyHostToDevice), "upload packed");
+    if (!rc && d->packed)
+      rc = count_b2g_device(ctx, s->g2, N, L, wpr, A, s->cnt_h.data(), s->tot_h.data());
     if (rc) { st_data_destroy(s); return rc; }
   } else {
     const size_t n = (size_t)N * 2 * L;

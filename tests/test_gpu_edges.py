@@ -211,3 +211,24 @@ def test_get_into_caller_array(ctx):
         c.get(api.F_QSUM, out=np.zeros(q.size, np.float32))
     c.close()
     d.close()
+
+
+@pytest.mark.parametrize("N", [1, 17, 130])
+def test_packed_upload_counts_match_int32_upload(ctx, N):
+    """Allele counts of 2-bit words (counted on the device, padding genotypes of
+    the last word masked) equal those of the int32 upload of the same data: the
+    initial eps (lambda + n_a) / (A lambda + n) agree exactly."""
+    L = 257
+    d = synth.snp_fmodel(N, L, 3, np.linspace(0.05, 0.25, 3), 0.4, 0.05, 31 + N)
+    m = api.model_defaults(maxpops=3, freqscorr=1, burnin=1, numreps=2)
+    a = api.Data(ctx, d["numalleles"], geno=d["geno"], layout=api.LAYOUT_B2G)
+    b = api.Data(ctx, d["numalleles"], packed=d["packed"], layout=api.LAYOUT_B2G,
+                 num_inds=N, num_loci=L)
+    ca, cb = api.Chain(ctx, a, m, 5), api.Chain(ctx, b, m, 5)
+    ea = ca.get(api.F_EPS)
+    np.testing.assert_array_equal(ea, cb.get(api.F_EPS))
+    two = np.asarray(d["numalleles"]) == 2
+    assert ((ea[two] > 0) & (ea[two] < 1)).all()
+    np.testing.assert_allclose(ea[two].sum(1), 1.0, rtol=1e-12)
+    for x in (ca, cb, a, b):
+        x.close()
