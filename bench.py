@@ -325,6 +325,13 @@ def run_ours(args):
     alu_achieved = B * copies * ops_per_copy / (zavg / 1e3) / 1e12
     sm_mhz = clk["sm_mhz"] or 1965.0
     alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+    # issue roofline of the same kernel, the limit it actually meets: warp
+    # instructions per 32 genotypes from the ncu capture of a burn-in launch
+    # (profiles/zpass_b2g_snp2000x50000_k5_batch20.txt); the timed launches also
+    # add the ln P(D) terms, so the fraction below is a lower bound
+    inst_per_32 = 115.6
+    issue_achieved = B * N * L / 32 * inst_per_32 / (zavg / 1e3) / 1e12
+    issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e12
     traffic = read_traffic()
     total_ms = sum(v[0] for v in prof.values())
 
@@ -367,6 +374,13 @@ def run_ours(args):
                          "ops_per_copy": ops_per_copy,
                          "note": "2K+2 FP32 + ~10 int (Philox/4) + 0.5 log per allele copy; "
                                  "peak = 148 SM x 128 lanes x median SM clock"},
+        "roofline_issue": {"bound": "issue", "achieved": round(issue_achieved, 4),
+                           "peak": round(issue_peak, 4), "unit": "T warp-inst/s",
+                           "frac": round(issue_achieved / issue_peak, 4),
+                           "inst_per_32_genotypes": inst_per_32,
+                           "note": "instructions from an ncu capture of a burn-in launch "
+                                   "(no ln P(D) terms; lower bound); peak = 148 SM x 4 "
+                                   "schedulers x median SM clock"},
         "kernels_ms": {k: round(v[0], 3) for k, v in prof.items()},
         "kernel_share": {k: round(v[0] / total_ms, 4) for k, v in prof.items()} if total_ms else {},
         "gpu_launches": int(launches),
