@@ -505,7 +505,10 @@ int count_b2g_device(st_ctx* ctx, const uint32_t* g2, int N, int L, int wpr, int
   cudaStream_t s = ctx->stream;
   const int block = 256;
   const unsigned grid = (unsigned)(((size_t)L * 32 + block - 1) / block);
-  count_b2g_kernel<<<grid, block, 0, s>>>(g2, N, L, wpr, A, cnt, tot);
+  {
+    Bracket br(ctx, ST_K_OTHER);
+    count_b2g_kernel<<<grid, block, 0, s>>>(g2, N, L, wpr, A, cnt, tot);
+  }
   rc = cuda_check(ctx, cudaGetLastError(), "count alleles");
   if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(cnt_h, cnt, sizeof(long long) * ncnt,
                                                 cudaMemcpyDeviceToHost, s), "read counts");
@@ -656,6 +659,7 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
       size_t m = std::min(slice, n - off);
       cudaMemcpy(tmp, d->geno + off, sizeof(int32_t) * m, cudaMemcpyHostToDevice);
       launch_pack_u8(tmp, s->g8 + off, m, 0);
+      ctx->launches++;
     }
     cudaDeviceSynchronize();
     cudaFree(tmp);
