@@ -49,10 +49,11 @@ def make_data():
 
 # ---------------------------------------------------------------------------
 # CPU legs: the reference's own CPU update functions (oracle/_ref) in
-# structure.c order, timed over one METROFREQ cycle (9 Gibbs + 1 Metropolis
-# sweep) of a 10,000-locus slice; time scales linearly in L.
+# structure.c order, timed over consecutive sweeps of a locus slice (one
+# METROFREQ cycle = 9 Gibbs + 1 Metropolis sweep per ten); time scales
+# linearly in L.
 # ---------------------------------------------------------------------------
-def _ref_worker(q, path, N, L_slice, seed, core):
+def _ref_worker(q, path, N, L_slice, seed, core, warmup, steps):
     try:
         # the reference prints progress on stdout; keep the bench's stdout to one line
         devnull = os.open(os.devnull, os.O_WRONLY)
@@ -67,9 +68,9 @@ def _ref_worker(q, path, N, L_slice, seed, core):
                       metrofreq=WL["metrofreq"], burnin=0, numreps=100,
                       alphapropsd=WL["alphapropsd"])
         ch = r.chain_new(m, geno, seed=seed)
-        r.lib.stref_chain_sweeps(ch, 1)                   # rep 0 (untimed warm-up)
+        r.lib.stref_chain_sweeps(ch, warmup)              # reps 0..warmup-1, untimed
         t0 = time.perf_counter()
-        r.lib.stref_chain_sweeps(ch, 10)                  # reps 1..10: 9 Gibbs + 1 Metropolis
+        r.lib.stref_chain_sweeps(ch, steps)               # the timed sweeps
         dt = time.perf_counter() - t0
         r.lib.stref_chain_free(ch)
         q.put(dt)
@@ -77,16 +78,18 @@ def _ref_worker(q, path, N, L_slice, seed, core):
         q.put(repr(e))
 
 
-def cpu_reference(packed, workers, pin=False):
-    """chain-sweeps/s of `workers` concurrent reference chains at full L."""
+def cpu_reference(packed, workers, pin=False, warmup=1, steps=10, slice_l=SLICE_L):
+    """chain-sweeps/s of `workers` concurrent reference chains at full L, from
+    `steps` timed sweeps (after `warmup` untimed ones) of a `slice_l`-locus slice."""
     from structure_b200 import synth
-    geno = synth.unpack_int32(packed, WL["N"], 0, SLICE_L)
+    geno = synth.unpack_int32(packed, WL["N"], 0, slice_l)
     tmp = tempfile.NamedTemporaryFile(suffix=".npy", delete=False)
     np.save(tmp.name, geno)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_ref_worker,
-                         args=(q, tmp.name, WL["N"], SLICE_L, 1000 + w, (w if pin else None)))
+                         args=(q, tmp.name, WL["N"], slice_l, 1000 + w, (w if pin else None),
+                               warmup, steps))
              for w in range(workers)]
     for p in procs:
         p.start()
@@ -106,12 +109,12 @@ def cpu_reference(packed, workers, pin=False):
     bad = [x for x in res if not isinstance(x, float)]
     if bad:
         raise RuntimeError(f"reference worker failed: {bad[0]}")
-    scale = SLICE_L / WL["L"]
-    rate = sum(10.0 / dt for dt in res) * scale
-    sample = (f"{workers} concurrent reference chain(s), each timed over sweeps 1-10 "
-              f"(9 Gibbs + 1 Metropolis) of a {SLICE_L}-locus slice (N={WL['N']}, K={WL['K']}, "
-              f"F model), scaled by {SLICE_L}/{WL['L']} loci; uniforms for the array-fed "
-              f"updates from xorshift128+")
+    scale = slice_l / WL["L"]
+    rate = sum(steps / dt for dt in res) * scale
+    sample = (f"{workers} concurrent reference chain(s), each timed over sweeps "
+              f"{warmup}-{warmup + steps - 1} (one Metropolis sweep in {WL['metrofreq']}) of a "
+              f"{slice_l}-locus slice (N={WL['N']}, K={WL['K']}, F model), scaled by "
+              f"{slice_l}/{WL['L']} loci; uniforms for the array-fed updates from xorshift128+")
     return rate, sample, max(res)
 
 
@@ -402,13 +405,18 @@ def run_reference(args):
         return
     d = make_data()
     workers = usable_workers()
-    rate, sample, tmax = cpu_reference(d["packed"], workers, pin=False)
+    # each step is one sweep of a locus slice sized so that warm-up + steps take
+    # about two minutes (~0.26 ms per locus and sweep for one reference chain)
+    steps, warmup = max(1, args.steps), max(1, args.warmup)
+    slice_l = int(min(SLICE_L, max(1000, 120.0 / ((steps + warmup) * 0.26e-3) // 1000 * 1000)))
+    rate, sample, tmax = cpu_reference(d["packed"], workers, pin=False, warmup=warmup,
+                                       steps=steps, slice_l=slice_l)
     out = {"metric": METRIC, "value": round(rate, 5), "unit": METRIC, "n_gpus": world,
-           "steps": 10, "warmup": 10, "ms_per_step": round(tmax * 1e3 / 10, 1),
+           "steps": steps, "warmup": warmup, "ms_per_step": round(tmax * 1e3 / steps, 1),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic, seeded (same generator and seed as the GPU arm)",
            "config": {"workload": WORKLOAD_NAME, "N": WL["N"], "L": WL["L"], "K": WL["K"],
-                      "slice_loci": SLICE_L, "workers": workers},
+                      "slice_loci": slice_l, "workers": workers},
            "impl": "reference",
            "cpu_baseline": {"value": round(rate, 5), "unit": METRIC, "cores": workers,
                             "kind": "reference", "sample": sample},
