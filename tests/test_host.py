@@ -129,3 +129,27 @@ def test_get_into_caller_array_checks_type_and_size(monkeypatch):
             c.get(api.F_QSUM, out=bad)
         assert e.value.code == api.ST_ERR_ARG
     assert len(calls) == 1
+
+
+def test_bench_reference_arm_line(ref):
+    """`bench.py --impl reference` runs the reference's CPU functions for the
+    requested warm-up and timed sweeps and prints one JSON line in the bench
+    contract (same metric and workload as the GPU arm, no host-device bytes)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0")
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2",
+                        "--warmup", "3"], cwd=root, env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "chain-sweeps/s"
+    assert d["steps"] == 2 and d["warmup"] == 3 and d["value"] > 0
+    assert d["higher_is_better"] is True
+    assert d["config"]["workload"].startswith("snp-fmodel N=2000 L=50000 K=5")
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
