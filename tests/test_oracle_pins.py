@@ -54,7 +54,7 @@ def test_lgamma_matches_reference_mylgamma(orc, ref):
         assert orc.lgamma(z) == ref.lib.mylgamma(z)
 
 
-@pytest.mark.parametrize("K,seed", [(1, 1), (2, 2), (3, 3), (6, 4)])
+@pytest.mark.parametrize("K,seed", [(1, 1), (2, 2), (3, 3), (6, 4), (10, 5), (17, 6), (32, 7)])
 def test_updatez_f64_matches_reference(orc, ref, K, seed):
     geno, na = _microsat(40, 30, 3, seed)
     N, _, L = geno.shape
@@ -124,11 +124,11 @@ def test_initfreqpriors_matches_reference(orc, ref, freqscorr):
     np.testing.assert_array_equal(fo, fr)
 
 
-def test_calclike_and_metro_logdiff_match_reference(orc, ref):
+@pytest.mark.parametrize("K", [1, 4, 9, 20])
+def test_calclike_and_metro_logdiff_match_reference(orc, ref, K):
     geno, na = _snp(60, 200, 3, 6)
     N, _, L = geno.shape
-    K = 4
-    rng = np.random.default_rng(6)
+    rng = np.random.default_rng(6 + K)
     Q, P = _state(rng, N, L, K, na)
     T, _ = _state(rng, N, L, K, na)
     ref.set_globals(N=N, L=L, K=K, maxalleles=P.shape[2])
