@@ -15,7 +15,8 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+# the reference's src/ directory; STRUCTURE_REF_SRC overrides the default
+REF_SRC = os.environ.get("STRUCTURE_REF_SRC", "/root/reference/src")
 
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -45,7 +46,7 @@ def build(ref=True):
     targets = ["oracle"]
     if ref and os.path.isdir(REF_SRC):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "REF=" + REF_SRC] + targets, check=True)
 
 
 def _load(path):

@@ -25,7 +25,7 @@ from structure_b200 import synth
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 FRONT_LIB = os.path.join(ROOT, "structure_b200", "libstfront.so")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libstref.so")
-REF_SRC = "/root/reference/src"
+from oracle.oracle import REF_SRC  # noqa: E402  (STRUCTURE_REF_SRC overrides it)
 
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference library not built")
 
