@@ -118,6 +118,18 @@ def cpu_reference(packed, workers, pin=False, warmup=1, steps=10, slice_l=SLICE_
     return rate, sample, max(res)
 
 
+def cpu_model():
+    """The host CPU's model name (as lscpu reports it, from /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def usable_workers():
     n = os.cpu_count() or 1
     try:
@@ -236,8 +248,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ctx.profile(True)
-    ctx.profile_read()
+    # the timed sweeps replay the batch's CUDA graphs (one per sweep kind)
     clocks = ClockSampler(local)
     l0 = ctx.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -248,9 +259,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = ctx.launches() - l0
-    prof = ctx.profile_read()
     clk = clocks.stop()
-    ctx.profile(False)
     for c in chains:
         assert c.sync() == 0, "device error word set"
     if world > 1:
@@ -259,16 +268,37 @@ def run_ours(args):
         ms = float(t.item())
     value = world * B * S / (ms / 1e3)
 
-    # plain path: the same chains one at a time (one chain per launch)
-    plain_sweeps = max(2, min(S, 10))
+    # per-kernel times: graph replay cannot bracket single launches, so the
+    # same batch runs PS more sweeps (one Metropolis sweep in METROFREQ, as in
+    # the timed ones) launch by launch with CUDA events around every launch
+    PS = max(WL["metrofreq"], min(S, 2 * WL["metrofreq"]))
+    ctx.profile(True)
+    ctx.profile_read()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    batch.sweep(PS)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = q0.elapsed_time(q1) / PS
+    prof = ctx.profile_read()
+    ctx.profile(False)
+
+    # plain path: the same chains one at a time (one chain per launch), each
+    # replaying its own CUDA graphs, captured by untimed sweeps first
+    plain_sweeps = WL["metrofreq"]
+    singles = [api.Batch(ctx, [c]) for c in chains]
+    for sb in singles:
+        sb.sweep(WL["metrofreq"])
     torch.cuda.synchronize()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record(stream)
-    for c in chains:
-        c.sweep(plain_sweeps)
+    for sb in singles:
+        sb.sweep(plain_sweeps)
     p1.record(stream)
     torch.cuda.synchronize()
     plain = B * plain_sweeps / (p0.elapsed_time(p1) / 1e3)
+    for sb in singles:
+        sb.close()
     like = [c.get(api.F_STATS)[api.ST_SUMLIKES] / max(1, c.get(api.F_STATS)[api.ST_NLIKE])
             for c in chains]
     # page-locked result arrays for the end-to-end leg's reads (fields of the same shapes)
@@ -356,7 +386,8 @@ def run_ours(args):
                               "locus_groups": int(tdims[7]), "chosen_by": "st_batch_autotune"}},
         "z_updates_per_s": round(value * copies, 1),
         "plain": {"value": round(plain, 3), "unit": METRIC,
-                  "path": "one chain per launch, same kernels"},
+                  "path": "one chain per launch, same kernels, each chain's sweep replayed "
+                          "from its own CUDA graphs"},
         "batched_over_plain": round(value / world / plain, 3),
         "mean_lnpd_over_chains": round(float(np.mean(like)), 2),
         "e2e": {"value": round(e2e, 3), "unit": METRIC,
@@ -384,14 +415,23 @@ def run_ours(args):
                            "note": "instructions from an ncu capture of a burn-in launch "
                                    "(no ln P(D) terms; lower bound); peak = 148 SM x 4 "
                                    "schedulers x median SM clock"},
-        "kernels_ms": {k: round(v[0], 3) for k, v in prof.items()},
+        "timed_path": "CUDA-graph replay of the batched sweep (st_batch_sweep, graphs on)",
+        "profiled_pass": {"sweeps": PS, "ms_per_step": round(eager_ms, 4),
+                          "note": "kernels_ms_per_step, kernel_share and the Z-pass launch "
+                                  "time come from these sweeps, run launch by launch with "
+                                  "CUDA events around every launch right after the timed ones"},
+        "kernels_ms_per_step": {k: round(v[0] / PS, 4) for k, v in prof.items()},
         "kernel_share": {k: round(v[0] / total_ms, 4) for k, v in prof.items()} if total_ms else {},
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if world == 1 and not args.headline_only:
+        ctx.close()
+        out["other_configs"] = other_configs(not args.no_cpu_baseline)
     if cpu_rate is not None:
         out["cpu_baseline"] = {"value": round(cpu_rate, 5), "unit": METRIC, "cores": 1,
-                               "kind": "reference", "sample": cpu_sample}
+                               "kind": "reference", "sample": cpu_sample,
+                               "cpu_model": cpu_model(), "host_cpus": os.cpu_count()}
     print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
@@ -419,7 +459,8 @@ def run_reference(args):
                       "slice_loci": slice_l, "workers": workers},
            "impl": "reference",
            "cpu_baseline": {"value": round(rate, 5), "unit": METRIC, "cores": workers,
-                            "kind": "reference", "sample": sample},
+                            "kind": "reference", "sample": sample, "cpu_model": cpu_model(),
+                            "host_cpus": os.cpu_count()},
            "e2e": {"value": round(rate, 5), "unit": METRIC, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -449,69 +490,433 @@ def _ess(x):
     return n / max(-1.0 + 2.0 * s, 1e-12)
 
 
-def run_grad(args):
+def _ref_jobs_worker(q, jobs, core):
+    """Runs reference chains one after another on one pinned core; each job is
+    (npy path, ref_model kwargs, seed, untimed sweeps, timed sweeps)."""
+    try:
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        if core is not None:
+            os.sched_setaffinity(0, {core})
+        from oracle.oracle import RefLib, ref_model
+        r = RefLib()
+        out = []
+        for path, mkw, seed, warm, steps in jobs:
+            geno = np.load(path)
+            ch = r.chain_new(ref_model(**mkw), geno, seed=seed)
+            if warm:
+                r.lib.stref_chain_sweeps(ch, warm)
+            t0 = time.perf_counter()
+            r.lib.stref_chain_sweeps(ch, steps)
+            out.append(time.perf_counter() - t0)
+            r.lib.stref_chain_free(ch)
+        q.put(out)
+    except Exception as e:  # pragma: no cover - reported to the parent
+        q.put(repr(e))
+
+
+def cpu_reference_jobs(jobs):
+    """Times reference chains (genotype arrays, model kwargs, seed, untimed and
+    timed sweeps) one after another in one process on one core; returns the
+    timed seconds of each job."""
+    tmp, spec = [], []
+    for geno, mkw, seed, warm, steps in jobs:
+        f = tempfile.NamedTemporaryFile(suffix=".npy", delete=False)
+        np.save(f.name, np.ascontiguousarray(geno, np.int32))
+        tmp.append(f.name)
+        spec.append((f.name, mkw, seed, warm, steps))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_ref_jobs_worker, args=(q, spec, 0))
+    p.start()
+    res = None
+    while res is None:
+        try:
+            res = q.get(timeout=5)
+        except Exception:
+            if not p.is_alive() and p.exitcode not in (0, None):
+                raise RuntimeError(f"reference worker exited with code {p.exitcode}")
+    p.join()
+    for f in tmp:
+        os.unlink(f)
+    if not isinstance(res, list):
+        raise RuntimeError(f"reference worker failed: {res}")
+    return res
+
+
+def _timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _observed_copies(packed, N):
+    L = packed.shape[0]
+    codes = (packed[:, :, None] >> (2 * np.arange(16, dtype=np.uint32))[None, None, :]) & 3
+    return int(2 * (codes.reshape(L, -1)[:, :N] != 3).sum())
+
+
+def _alu_roofline(copies_by_kclass, zpass_ms, sm_mhz):
+    """ALU roofline of the Z pass: (2K+2) FP32 + ~10 integer (Philox/4) + 1/2 log
+    per allele copy at each chain's K class, against 148 SM x 128 lanes."""
+    ops = sum(c * (2 * kc + 2 + 10 + 0.5) for kc, c in copies_by_kclass)
+    ach = ops / (zpass_ms / 1e3) / 1e12
+    peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+    return {"bound": "alu", "achieved": round(ach, 3), "peak": round(peak, 2), "unit": "Top/s",
+            "frac": round(ach / peak, 4), "kernel": "zpass_b2g_kernel (per K class)",
+            "avg_zpass_ms_per_sweep": round(zpass_ms, 4),
+            "note": "(2K+2) FP32 + ~10 int (Philox/4) + 0.5 log per allele copy at the K "
+                    "class; peak = 148 SM x 128 lanes x median SM clock; Z-pass time from "
+                    "a profiled pass of the same sweeps (CUDA events per launch)"}
+
+
+def _kernel_share(prof):
+    tot = max(1e-9, sum(v[0] for v in prof.values()))
+    return {k: round(v[0] / tot, 4) for k, v in prof.items()}
+
+
+def measure_config1(with_cpu=True):
+    """Config 1: N=200, L=100 microsatellite-like loci (2-10 alleles, 5% of
+    copies missing), K=3 admixture model, independent frequencies (lambda=1),
+    alpha inferred; the whole run of 1,000 burn-in + 10,000 sweeps of one
+    chain, on the device and on the reference's CPU code."""
+    import torch
+    from structure_b200 import api, synth
+    d = synth.microsat()
+    geno, na = d["geno"], d["numalleles"]
+    N, _, L = geno.shape
+    K, burn, reps = 3, 1000, 10000
+    mk = dict(maxpops=K, burnin=burn, numreps=reps, freqscorr=0, inferalpha=1, alpha=1.0,
+              unifprioralpha=1, alphamax=10.0, alphapropsd=0.025, metrofreq=10, computeprob=1)
+    ctx = api.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    data = api.Data(ctx, na, geno=geno)
+    c = api.Chain(ctx, data, api.model_defaults(**mk), 1001)
+    b = api.Batch(ctx, [c])
+    l0 = ctx.launches()
+    ms = _timed(stream, lambda: b.sweep(burn + reps))
+    launches = ctx.launches() - l0
+    c.get(api.F_QSUM)
+    st = c.get(api.F_STATS)
+    e2e_s = time.perf_counter() - t0
+    assert c.sync() == 0
+    copies = int((geno >= 0).sum())
+    sweeps = burn + reps
+    out = {"workload": "config 1: N=200 L=100 microsatellites (2-10 alleles), K=3, "
+                       "1,000 + 10,000 sweeps, one chain",
+           "value": round(sweeps / (ms / 1e3), 1), "unit": "sweeps/s",
+           "run_s": round(ms / 1e3, 4), "z_updates_per_s": round(sweeps * copies / (ms / 1e3), 1),
+           "e2e": {"value": round(sweeps / e2e_s, 1), "unit": "sweeps/s",
+                   "includes": "st_data_upload, st_chain_create, the whole run, QSum and "
+                               "stats read back"},
+           "gpu_launches": int(launches),
+           "mean_lnpd": round(st[api.ST_SUMLIKES] / max(1, st[api.ST_NLIKE]), 3),
+           "roofline": {"bound": "launch", "achieved_us_per_sweep": round(ms * 1e3 / sweeps, 2),
+                        "kernels_per_sweep": round(launches / sweeps, 2),
+                        "note": "4e4 allele copies per sweep: each sweep is a few "
+                                "microsecond-scale kernels replayed from a CUDA graph, so "
+                                "launch latency bounds it, not HBM or the ALUs"}}
+    b.close(); c.close(); data.close(); ctx.close()
+    if with_cpu:
+        A = int(na.max())
+        mkw = dict(N=N, L=L, K=K, maxalleles=A, freqscorr=0, inferalpha=1, alpha=1.0,
+                   unifprioralpha=1, alphamax=10.0, alphapropsd=0.025, metrofreq=10,
+                   burnin=burn, numreps=reps, lambda_=1.0)
+        (dt,) = cpu_reference_jobs([(geno, mkw, 1001, 0, sweeps)])
+        out["cpu_baseline"] = {"value": round(sweeps / dt, 2), "unit": "sweeps/s",
+                               "cores": 1, "kind": "reference",
+                               "sample": "the whole run (1,000 + 10,000 sweeps) of one "
+                                         "reference chain", "cpu_model": cpu_model()}
+    return out
+
+
+def measure_config3(steps, warmup, with_cpu=True):
+    """Config 3: 40 chains = K in 1..10 x 4 seeds, seed s on data set s of
+    (N, L) = (300, 5000), (1000, 10000), (2500, 20000), (4000, 8000) (true
+    K=4, F_k ~ U[0.02, 0.2]), batched (one launch per update step and K class,
+    CUDA graphs, autotuned tiles) against the same chains one at a time."""
+    import torch
+    from structure_b200 import api, synth
+    sets = synth.config3_datasets(want_int32=False)
+    ctx = api.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    datas = [api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=d["N"], num_loci=d["L"],
+                      layout=api.LAYOUT_B2G) for d in sets]
+    mk = lambda K: api.model_defaults(maxpops=K, burnin=warmup, numreps=steps + 40,
+                                      freqscorr=1, inferalpha=1, alpha=1.0, metrofreq=10,
+                                      fpriormean=0.01, fpriorsd=0.05, computeprob=1)
+    spec = [(K, s) for K in range(1, 11) for s in range(4)]
+    chains = [api.Chain(ctx, datas[s], mk(K), 3000 + 10 * K + s) for K, s in spec]
+    b = api.Batch(ctx, chains)
+    b.autotune()
+    b.sweep(warmup)
+    clocks = ClockSampler(0)
+    l0 = ctx.launches()
+    ms = _timed(stream, lambda: b.sweep(steps))
+    launches = ctx.launches() - l0
+    clk = clocks.stop()
+    n = len(chains)
+    # Z-pass time per sweep from a profiled pass (CUDA events around each launch)
+    ctx.profile(True)
+    ctx.profile_read()
+    ps = 10
+    b.sweep(ps)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    # plain: each chain alone, replaying its own graphs
+    singles = [api.Batch(ctx, [c]) for c in chains]
+    for sb in singles:
+        sb.sweep(10)
+    pms = _timed(stream, lambda: [sb.sweep(10) for sb in singles])
+    for c in chains:
+        assert c.sync() == 0
+    value = n * steps / (ms / 1e3)
+    plain = n * 10 / (pms / 1e3)
+    cp = [_observed_copies(d["packed"], d["N"]) for d in sets]
+    copies = sum(cp[s] for _, s in spec)
+    kcl = [(api.fast_class(K), cp[s]) for K, s in spec]
+    out = {"workload": "config 3: 40 chains, K=1..10 x 4 seeds over 4 SNP data sets "
+                       "(300x5000, 1000x10000, 2500x20000, 4000x8000), F model, batched",
+           "value": round(value, 3), "unit": METRIC, "steps": steps, "warmup": warmup,
+           "ms_per_step": round(ms / steps, 4),
+           "z_updates_per_s": round(value / n * copies, 1),
+           "plain": {"value": round(plain, 3), "unit": METRIC,
+                     "path": "each chain alone, replaying its own CUDA graphs"},
+           "batched_over_plain": round(value / plain, 3),
+           "gpu_launches": int(launches),
+           "kernel_share": _kernel_share(prof),
+           "roofline": _alu_roofline(kcl, prof["zpass"][0] / ps, clk["sm_mhz"] or 1965.0),
+           "clocks": clk}
+    for sb in singles:
+        sb.close()
+    b.close()
+    for c in chains:
+        c.close()
+    for d in datas:
+        d.close()
+    ctx.close()
+    if with_cpu:
+        # sweep 1 of each of the 40 reference chains (after one untimed sweep)
+        # on a slice of at most 1,000 loci, scaled to the chain's L
+        jobs, scale = [], []
+        for K, s in spec:
+            d = sets[s]
+            sl = min(d["L"], 1000)
+            g = synth.unpack_int32(d["packed"], d["N"], 0, sl)
+            jobs.append((g, dict(N=d["N"], L=sl, K=K, maxalleles=2, freqscorr=1,
+                                 fpriormean=0.01, fpriorsd=0.05, metrofreq=10, burnin=0,
+                                 numreps=100), 3000 + 10 * K + s, 1, 1))
+            scale.append(d["L"] / sl)
+        dts = cpu_reference_jobs(jobs)
+        total = sum(dt * sc for dt, sc in zip(dts, scale))
+        out["cpu_baseline"] = {"value": round(n / total, 5), "unit": METRIC, "cores": 1,
+                               "kind": "reference",
+                               "sample": "sweep 1 of each of the 40 reference chains on a slice "
+                                         "of min(L, 1000) loci, scaled to its L; the 40 chains "
+                                         "run one after another on one core",
+                               "cpu_model": cpu_model()}
+    return out
+
+
+def measure_config4(steps, warmup, with_cpu=True, data=None):
     """Config 4: forward + backward of ln P(D|Q,P) w.r.t. softmax logits,
     N=5000, L=100,000, K=8, FP32, one evaluation per step."""
     import torch
     from structure_b200 import api, synth
     from structure_b200.grad import LogLikGrad
-    d = synth.config4()
+    d = data or synth.snp_fmodel_device(5000, 100000, 8, np.full(8, 0.5), 0.2, 0.0,
+                                        synth.DATA_SEED_BASE + 4, indep_beta=(0.5, 0.5))
     N, L, K = d["N"], d["L"], 8
     ctx = api.Context(0)
-    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
-                    layout=api.LAYOUT_B2G)
-    ev = LogLikGrad(ctx, data, K, precision=32)
+    dd = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
+                  layout=api.LAYOUT_B2G)
+    ev = LogLikGrad(ctx, dd, K, precision=32)
     g = torch.Generator(device="cuda").manual_seed(4)
     ql = torch.randn(N, K, device="cuda", generator=g)
     pl = torch.randn(L, K, 2, device="cuda", generator=g)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         ev(ql, pl)
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        ev(ql, pl)
-    e1.record()
-    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ms = _timed(stream, lambda: [ev(ql, pl) for _ in range(steps)]) / steps
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    codes = (d["packed"][:, :, None] >> (2 * np.arange(16, dtype=np.uint32))[None, None, :]) & 3
-    geno_obs = int((codes.reshape(L, -1)[:, :N] != 3).sum())
+    geno_obs = _observed_copies(d["packed"], N) // 2
     flops = geno_obs * 2 * (4 * K) * 2         # two passes x (2K + 2K FMA) x 2 FLOP
     sm_mhz = clk["sm_mhz"] or 1965.0
     peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     ach = flops / (ms / 1e3) / 1e12
-    # end to end: logits from pinned host memory, loglik and gradients back
     qh, ph = ql.cpu().pin_memory(), pl.cpu().pin_memory()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         ll, dq, dp = ev(qh.to("cuda", non_blocking=True), ph.to("cuda", non_blocking=True))
         ll.cpu(); dq.cpu(); dp.cpu()
-    e2e = args.steps / (time.perf_counter() - t0)
-    out = {"metric": "loglik+gradient evaluations/s", "value": round(1e3 / ms, 3),
-           "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic, seeded (config 4 generator)",
-           "config": {"workload": "differentiation N=5000 L=100000 K=8 (fwd + bwd, softmax logits)",
-                      "N": N, "L": L, "K": K, "l2": "inputs 125 MB packed > L2 after logits"},
+    e2e = steps / (time.perf_counter() - t0)
+    out = {"workload": "config 4: differentiation N=5000 L=100000 K=8 (forward + backward, "
+                       "softmax logits, FP32)",
+           "metric": "loglik+gradient evaluations/s", "value": round(1e3 / ms, 3),
+           "unit": "evals/s", "steps": steps, "warmup": warmup, "ms_per_step": round(ms, 4),
            "genotypes_per_s": round(geno_obs * 1e3 / ms, 1),
            "roofline": {"bound": "fp32-fma", "achieved": round(ach, 3), "peak": round(peak, 2),
                         "unit": "TFLOP/s", "frac": round(ach / peak, 4),
-                        "note": "4K FMA per genotype per pass, two passes; peak = 148 SM x 128 "
-                                "lanes x 2 x median SM clock (no tensor cores: K=8 contraction)"},
+                        "note": "4K FMA per genotype per pass, two passes; peak = 148 SM x "
+                                "128 lanes x 2 x median SM clock (no tensor cores: the "
+                                "contraction is K=8 wide)"},
            "e2e": {"value": round(e2e, 3), "unit": "evals/s",
                    "h2d_bytes_per_step": int(qh.nbytes + ph.nbytes),
                    "d2h_bytes_per_step": int(8 + qh.nbytes + ph.nbytes)},
-           "gpu_launches": 6 * args.steps, "clocks": clk}
+           "gpu_launches": 6 * steps, "clocks": clk,
+           "data": "synthetic, seeded: config 4's generative model drawn on the GPU "
+                   "(synth.snp_fmodel_device)"}
+    del ev
+    dd.close()
+    ctx.close()
+    if with_cpu:
+        # the FP64 CPU restatement of the same forward + backward (the oracle;
+        # the reference has no gradient) on a 1,000-locus slice, scaled by L
+        from oracle.oracle import Oracle
+        sl = 1000
+        gs = synth.unpack_int32(d["packed"], N, 0, sl)
+        rng = np.random.default_rng(4)
+        qn, pn = rng.standard_normal((N, K)), rng.standard_normal((sl, K, 2))
+        orc = Oracle()
+        t0 = time.perf_counter()
+        orc.loglik_grad(gs, qn, pn)
+        dt = (time.perf_counter() - t0) * L / sl
+        out["cpu_baseline"] = {"value": round(1.0 / dt, 5), "unit": "evals/s", "cores": 1,
+                               "kind": "port",
+                               "sample": "one FP64 forward + backward of the oracle's "
+                                         "restatement on a 1,000-locus slice, scaled by L",
+                               "cpu_model": cpu_model()}
+    return out
+
+
+def measure_config5(steps, warmup, with_cpu=True):
+    """Config 5: N=10,000, L=500,000 (2-bit packed, 1.25 GB), 2% missing, K=10 F
+    model with F_k ~ U[0.01, 0.3], POPALPHAS=1, Q ~ Dir(0.1); 8 replicate chains
+    batched on one GPU under the context's HBM admission budget."""
+    import torch
+    from structure_b200 import api, synth
+    N, L, K, B = 10000, 500000, 10, 8
+    rng = np.random.default_rng(synth.DATA_SEED_BASE + 5)
+    F = rng.uniform(0.01, 0.3, K)
+    d = synth.snp_fmodel_device(N, L, K, F, 0.1, 0.02, synth.DATA_SEED_BASE + 5)
+    ctx = api.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
+                    layout=api.LAYOUT_B2G)
+    mk = dict(maxpops=K, burnin=warmup, numreps=steps + 20, freqscorr=1, inferalpha=1,
+              popalphas=1, alpha=1.0, metrofreq=10, fpriormean=0.01, fpriorsd=0.05,
+              computeprob=1)
+    chains = [api.Chain(ctx, data, api.model_defaults(**mk), 5000 + r) for r in range(B)]
+    used, budget = ctx.memory()
+    b = api.Batch(ctx, chains)
+    b.sweep(warmup)
+    clocks = ClockSampler(0)
+    l0 = ctx.launches()
+    ms = _timed(stream, lambda: b.sweep(steps))
+    launches = ctx.launches() - l0
+    clk = clocks.stop()
+    ctx.profile(True)
+    ctx.profile_read()
+    ps = 10
+    b.sweep(ps)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    for c in chains:
+        assert c.sync() == 0
+    copies = _observed_copies(d["packed"], N)
+    value = B * steps / (ms / 1e3)
+    out = {"workload": "config 5: N=10000 L=500000 K=10 F model, POPALPHAS=1, 8 chains batched",
+           "value": round(value, 3), "unit": METRIC, "steps": steps, "warmup": warmup,
+           "ms_per_step": round(ms / steps, 3), "z_updates_per_s": round(value * copies, 1),
+           "hbm_in_use_gb": round(used / 1e9, 2), "hbm_budget_gb": round(budget / 1e9, 2),
+           "gpu_launches": int(launches),
+           "kernel_share": _kernel_share(prof),
+           "roofline": _alu_roofline([(api.fast_class(K), B * copies)], prof["zpass"][0] / ps,
+                                     clk["sm_mhz"] or 1965.0),
+           "data": "synthetic, seeded: config 5's generative model drawn on the GPU "
+                   "(synth.snp_fmodel_device)",
+           "clocks": clk}
+    b.close()
+    for c in chains:
+        c.close()
+    data.close()
+    ctx.close()
+    if with_cpu:
+        sl = 1000
+        g = synth.unpack_int32(d["packed"], N, 0, sl)
+        mkw = dict(N=N, L=sl, K=K, maxalleles=2, freqscorr=1, popalphas=1, fpriormean=0.01,
+                   fpriorsd=0.05, metrofreq=10, burnin=0, numreps=100)
+        (dt,) = cpu_reference_jobs([(g, mkw, 5000, 1, 1)])
+        out["cpu_baseline"] = {"value": round(1.0 / (dt * L / sl), 6), "unit": METRIC,
+                               "cores": 1, "kind": "reference",
+                               "sample": "sweep 1 of one reference chain on a 1,000-locus slice "
+                                         "(N=10,000, K=10), scaled by 500,000/1,000 loci",
+                               "cpu_model": cpu_model()}
+    return out
+
+
+def _print_workload(name, res, steps, warmup):
+    out = {"metric": res.get("metric", METRIC), "value": res["value"], "unit": res["unit"],
+           "n_gpus": 1, "steps": steps, "warmup": warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32" if name == "grad" else "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
+           "data": res.get("data", "synthetic, seeded"), "config": {"workload": res["workload"]}}
+    out.update({k: v for k, v in res.items() if k not in out and k != "workload"})
     print(json.dumps(out), flush=True)
+
+
+def run_grad(args):
+    _print_workload("grad", measure_config4(args.steps, args.warmup, not args.no_cpu_baseline),
+                    args.steps, args.warmup)
+
+
+def run_scale(args):
+    _print_workload("scale", measure_config5(args.steps, args.warmup, not args.no_cpu_baseline),
+                    args.steps, args.warmup)
+
+
+def run_uneven(args):
+    _print_workload("uneven", measure_config3(args.steps, args.warmup, not args.no_cpu_baseline),
+                    args.steps, args.warmup)
+
+
+def run_small(args):
+    _print_workload("small", measure_config1(not args.no_cpu_baseline), 1, 0)
+
+
+def other_configs(with_cpu):
+    """The other configurations, measured briefly for the default bench line."""
+    out = {}
+    for key, fn in (("config1", lambda: measure_config1(with_cpu)),
+                    ("config3", lambda: measure_config3(20, 3, with_cpu)),
+                    ("config4", lambda: measure_config4(10, 3, with_cpu)),
+                    ("config5", lambda: measure_config5(5, 3, with_cpu))):
+        try:
+            out[key] = fn()
+        except Exception as e:  # reported in the line, never hides the headline
+            out[key] = {"error": repr(e)[:300]}
+    return out
 
 
 def run_mala(args):
     """Config 4 mixing: Gibbs chain vs Gibbs + Langevin-on-Q chain, ESS per
     second of device time for ln P(D) and for Q (median over entries)."""
     from structure_b200 import api, synth
-    d = synth.config4()
+    d = synth.snp_fmodel_device(5000, 100000, 8, np.full(8, 0.5), 0.2, 0.0,
+                                synth.DATA_SEED_BASE + 4, indep_beta=(0.5, 0.5))
     N, L, K = d["N"], d["L"], 8
     ctx = api.Context(0)
     data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
@@ -556,118 +961,6 @@ def run_mala(args):
     print(json.dumps(out), flush=True)
 
 
-def run_scale(args):
-    """Config 5: N=10,000, L=500,000, K=10 F model, POPALPHAS=1, 8 replicate
-    chains batched on one GPU under the context's HBM admission budget."""
-    import torch
-    from structure_b200 import api, synth
-    d = synth.config5()
-    N, L, K, B = d["N"], d["L"], 10, 8
-    ctx = api.Context(0)
-    stream = torch.cuda.Stream()
-    ctx.set_stream(stream.cuda_stream)
-    data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
-                    layout=api.LAYOUT_B2G)
-    mk = dict(maxpops=K, burnin=args.warmup, numreps=args.steps + 10, freqscorr=1,
-              inferalpha=1, popalphas=1, alpha=1.0, metrofreq=10, fpriormean=0.01,
-              fpriorsd=0.05, computeprob=1)
-    chains = [api.Chain(ctx, data, api.model_defaults(**mk), 5000 + r) for r in range(B)]
-    used, budget = ctx.memory()
-    b = api.Batch(ctx, chains)
-    b.sweep(args.warmup)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.sweep(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    for c in chains:
-        assert c.sync() == 0
-    ms = e0.elapsed_time(e1)
-    codes_missing = 0.02
-    out = {"metric": METRIC, "value": round(B * args.steps / (ms / 1e3), 3), "unit": METRIC,
-           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
-           "data": "synthetic, seeded (config 5 generator)",
-           "config": {"workload": "scale N=10000 L=500000 K=10 F model, POPALPHAS=1, 8 chains",
-                      "N": N, "L": L, "K": K, "chains": B, "hbm_in_use_gb": round(used / 1e9, 2),
-                      "hbm_budget_gb": round(budget / 1e9, 2)},
-           "z_updates_per_s": round(B * args.steps / (ms / 1e3) * 2 * N * L * (1 - codes_missing), 1),
-           "clocks": clk}
-    b.close()
-    for c in chains:
-        c.close()
-    data.close()
-    print(json.dumps(out), flush=True)
-
-
-def run_uneven(args):
-    """Config 3: 40 chains = K in 1..10 x 4 seeds, seed s on data set s of
-    (N, L) = (300, 5000), (1000, 10000), (2500, 20000), (4000, 8000) (true K=4,
-    F_k ~ U[0.02, 0.2]), batched (one launch per update step and K class, CUDA
-    graphs, autotuned tiles) against the same chains one at a time."""
-    import torch
-    from structure_b200 import api, synth
-    sets = synth.config3_datasets(want_int32=False)
-    ctx = api.Context(0)
-    stream = torch.cuda.Stream()
-    ctx.set_stream(stream.cuda_stream)
-    datas = [api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=d["N"], num_loci=d["L"],
-                      layout=api.LAYOUT_B2G) for d in sets]
-    mk = lambda K: api.model_defaults(maxpops=K, burnin=args.warmup, numreps=args.steps + 10,
-                                      freqscorr=1, inferalpha=1, alpha=1.0, metrofreq=10,
-                                      fpriormean=0.01, fpriorsd=0.05, computeprob=1)
-    chains = [api.Chain(ctx, datas[s], mk(K), 3000 + 10 * K + s) for K in range(1, 11)
-              for s in range(4)]
-    b = api.Batch(ctx, chains)
-    b.autotune()
-    b.sweep(args.warmup)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.sweep(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    n = len(chains)
-    plain_sweeps = max(2, min(args.steps, 20))
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    for c in chains:
-        c.sweep(plain_sweeps)
-    p1.record(stream)
-    torch.cuda.synchronize()
-    for c in chains:
-        assert c.sync() == 0
-    value = n * args.steps / (ms / 1e3)
-    plain = n * plain_sweeps / (p0.elapsed_time(p1) / 1e3)
-    copies = sum(2 * d["N"] * d["L"] * 10 for d in sets) * 0.97
-    out = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": 1,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32 (Z/P/Q) + f64 (MH ratios, lnP(D))",
-           "data": "synthetic, seeded (config 3 generator)",
-           "config": {"workload": "uneven batch: 40 chains, K=1..10 x 4 seeds over 4 SNP data sets "
-                                  "(300x5000, 1000x10000, 2500x20000, 4000x8000), F model",
-                      "chains": n, "k_classes": 10},
-           "plain": {"value": round(plain, 3), "unit": METRIC,
-                     "path": "one chain per launch, same kernels"},
-           "batched_over_plain": round(value / plain, 3),
-           "z_updates_per_s": round(args.steps * copies / (ms / 1e3), 1),
-           "clocks": clk}
-    b.close()
-    for c in chains:
-        c.close()
-    for d in datas:
-        d.close()
-    print(json.dumps(out), flush=True)
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -675,16 +968,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the brief measurements of configs 1, 3, 4 and 5 that the "
+                         "default line carries under other_configs")
     ap.add_argument("--workload", default="snp",
-                    choices=["snp", "grad", "mala", "scale", "uneven"],
-                    help="snp: the headline (default); grad: config 4 forward+backward; "
-                         "mala: config 4 ESS/s, Gibbs vs Gibbs+Langevin; scale: config 5; "
-                         "uneven: config 3 batched vs one chain at a time")
+                    choices=["snp", "small", "grad", "mala", "scale", "uneven"],
+                    help="snp: the headline (default); small: config 1 whole run; grad: "
+                         "config 4 forward+backward; mala: config 4 ESS/s, Gibbs vs "
+                         "Gibbs+Langevin; scale: config 5; uneven: config 3 batched vs one "
+                         "chain at a time")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload != "snp" and args.impl == "ours":
-        {"grad": run_grad, "mala": run_mala, "scale": run_scale,
+        {"grad": run_grad, "mala": run_mala, "scale": run_scale, "small": run_small,
          "uneven": run_uneven}[args.workload](args)
         return
     if args.impl == "reference":

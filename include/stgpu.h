@@ -209,6 +209,20 @@ int st_update_q_mala(st_chain *c);
  * that locus).  precision 64 reproduces the reference's FP64 arithmetic.
  * Needs U8 data.                                                             */
 int st_update_z_injected(st_chain *c, const double *uniforms, size_t n, int precision);
+/* UpdateP (src/Updates/UpdateP.c:106-199) fed an explicit uniform array laid
+ * out like the reference's randomArr for it: for locus l and population k the
+ * block of MAXALLELES*64 values at (l*K*MAXALLELES + k*MAXALLELES)*64, read in
+ * order by the reference's own sampler (LogRDirichletDisc over RGammaDisc,
+ * src/ran.c:1094-1188,1248-1272) in FP64; P from the chain's current counts
+ * (ST_F_N), eps, F and lambda.  n = L*K*MAXALLELES*64.  A draw that needs more
+ * than its block (the reference exits) sets ST_DERR_GAMMA_CAP.              */
+int st_update_p_injected(st_chain *c, const double *uniforms, size_t n);
+/* UpdateQMetro (src/Updates/UpdateQ.c:199-307) fed an explicit uniform array:
+ * for individual i the block of 64 values at i*64, from which the reference's
+ * RDirichletDisc (src/ran.c:1197-1210) draws TestQ from alpha and the next
+ * value is the accept uniform (accept iff u < exp(logdiff)); logdiff is the
+ * chain's Metropolis data pass (FP64 on ST_LAYOUT_U8 data).  n = N*64.       */
+int st_update_q_metro_injected(st_chain *c, const double *uniforms, size_t n);
 
 /* One Z update with its counts and ln P(D) that allocates no device memory.
  * No counterpart in the reference: it serves callers that own every device
@@ -231,7 +245,9 @@ int st_update_z_injected(st_chain *c, const double *uniforms, size_t n, int prec
  * returns ST_ERR_ADMISSION.  Calls are asynchronous on cuda_stream (NULL =
  * default stream) and share that array: calls that overlap on the GPU race.
  * The first call on a device looks the array up (and may load the library's
- * device code); make it before any stream capture.                           */
+ * device code); make it before any stream capture.  The address it caches
+ * belongs to the device's context: after a cudaDeviceReset the process must
+ * load the library again before calling this entry point.                   */
 #define ST_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int st_update_z_noalloc(int device, const uint32_t *g2, int32_t wpr, int32_t num_inds,
                         int32_t num_loci, int32_t maxpops, const float *Q, const float *P,
@@ -330,10 +346,14 @@ size_t st_field_bytes(st_chain *c, int field);
  * st_chain_save writes every array of the chain, its sweep counter and its
  * random-stream key to a file; st_chain_load restores them into a chain
  * created on the same data with the same K, layout and options (seed
- * irrelevant; its Z-pass tile may differ).  Draws are keyed by (seed,
- * sweep, update, element), so the loaded chain continues exactly as the
- * saved one would have.  Load before putting the chain in a batch: a batch
- * keeps its own copy of each chain's descriptor from st_batch_create.      */
+ * irrelevant; its Z-pass tile and NUMREPS may differ).  Draws are keyed by
+ * (seed, sweep, update, element), so the loaded chain continues exactly as
+ * the saved one would have.  A file of another shape, saved under other
+ * st_model options, truncated or with trailing bytes returns ST_ERR_STATE
+ * and leaves the chain unchanged (the file is read and checked whole before
+ * any device memory is written).  Load before putting the chain in a batch:
+ * a batch keeps its own copy of each chain's descriptor from
+ * st_batch_create.                                                          */
 int st_chain_save(st_chain *c, const char *path);
 int st_chain_load(st_chain *c, const char *path);
 

@@ -223,7 +223,8 @@ void orc_zupdate_f32(int N, int L, int K, int A, const int32_t *geno,
                 const float *p = P + (size_t)l * K * A + a;
                 C[0] = q[0] * p[0];
                 for (int k = 1; k < K; k++) C[k] = fmaf(q[k], p[(size_t)k * A], C[k - 1]);
-                float u = (float)(w[2 * (i & 1) + line] >> 8) * (1.0f / 16777216.0f);
+                /* u = the word's low 23 bits / 2^23; r = RN(u * T) */
+                float u = (float)(w[2 * (i & 1) + line] & 0x7FFFFFu) * (1.0f / 8388608.0f);
                 float r = u * C[K - 1];
                 int z = 0;
                 for (int k = 0; k < K - 1; k++) z += (C[k] < r);

@@ -102,6 +102,8 @@ def lib():
         "st_chain_save": ([vp, C.c_char_p], C.c_int),
         "st_chain_load": ([vp, C.c_char_p], C.c_int),
         "st_update_z_injected": ([vp, vp, sz, C.c_int], C.c_int),
+        "st_update_p_injected": ([vp, vp, sz], C.c_int),
+        "st_update_q_metro_injected": ([vp, vp, sz], C.c_int),
         "st_sweep": ([vp, C.c_int], C.c_int), "st_run": ([vp], C.c_int),
         "st_sync": ([vp], C.c_int),
         "st_batch_create": ([vp, C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
@@ -317,6 +319,18 @@ class Chain:
     def UpdateZInjected(self, uniforms, precision=64):
         u = np.ascontiguousarray(uniforms, np.float64)
         self.ctx.check(lib().st_update_z_injected(self.h, u.ctypes.data, u.size, precision))
+
+    def UpdatePInjected(self, uniforms):
+        """UpdateP with the reference's sampler on the reference's randomArr
+        slots (L*K*A*64 uniforms)."""
+        u = np.ascontiguousarray(uniforms, np.float64)
+        self.ctx.check(lib().st_update_p_injected(self.h, u.ctypes.data, u.size))
+
+    def UpdateQMetroInjected(self, uniforms):
+        """UpdateQMetro with the reference's sampler on its randomArr slots
+        (N*64 uniforms)."""
+        u = np.ascontiguousarray(uniforms, np.float64)
+        self.ctx.check(lib().st_update_q_metro_injected(self.h, u.ctypes.data, u.size))
 
     def sweep(self, n=1):
         self.ctx.check(lib().st_sweep(self.h, n))

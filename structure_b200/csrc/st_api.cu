@@ -1204,6 +1204,61 @@ extern "C" int st_update_z_injected(st_chain* c, const double* u, size_t n, int 
   return rc;
 }
 
+// Injected-array parity modes of UpdateP and UpdateQMetro (st_injected.cu).
+// The caller's array goes to the chain's injected buffer (grown on demand,
+// shared with st_update_z_injected), plus N ints of draw counts for the
+// Metropolis step.
+static int injected_buffer(st_chain* c, size_t doubles, size_t ints) {
+  const size_t n = doubles + (ints + 1) / 2;
+  if (c->injected_n >= n && c->d_injected) return ST_OK;
+  if (c->d_injected) {
+    cudaStreamSynchronize(c->ctx->stream);
+    ctx_free(c->ctx, c->d_injected);
+  }
+  c->d_injected = nullptr;
+  c->injected_n = 0;
+  void* p;
+  if (int rc = ctx_alloc(c->ctx, n * 8, &p, nullptr, nullptr)) return rc;
+  c->d_injected = (double*)p;
+  c->injected_n = n;
+  return ST_OK;
+}
+
+extern "C" int st_update_p_injected(st_chain* c, const double* u, size_t n) {
+  if (!c || !u) return ST_ERR_ARG;
+  const size_t need = (size_t)c->h.L * c->h.K * c->h.A * 64;
+  if (n != need)
+    return seterr(c->ctx, ST_ERR_ARG, "need L*K*MAXALLELES*64 = %zu uniforms", need);
+  cudaSetDevice(c->ctx->device);
+  if (int rc = injected_buffer(c, n, 0)) return rc;
+  ST_CUDA(c->ctx, cudaMemcpyAsync(c->d_injected, u, n * 8, cudaMemcpyHostToDevice, c->ctx->stream));
+  Bracket br(c->ctx, ST_K_OTHER);
+  return cuda_check(c->ctx, launch_inj_p(c->h, c->d_chain, c->d_injected, c->ctx->stream),
+                    "injected UpdateP");
+}
+
+extern "C" int st_update_q_metro_injected(st_chain* c, const double* u, size_t n) {
+  if (!c || !u) return ST_ERR_ARG;
+  const size_t need = (size_t)c->h.N * 64;
+  if (n != need) return seterr(c->ctx, ST_ERR_ARG, "need NUMINDS*64 = %zu uniforms", need);
+  if (c->h.noadmix)
+    return seterr(c->ctx, ST_ERR_STATE, "NOADMIX chains have no Metropolis Q update");
+  cudaSetDevice(c->ctx->device);
+  if (int rc = injected_buffer(c, n, (size_t)c->h.N)) return rc;
+  st_ctx* ctx = c->ctx;
+  int* taken = reinterpret_cast<int*>(c->d_injected + n);
+  ST_CUDA(ctx, cudaMemcpyAsync(c->d_injected, u, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  {
+    Bracket br(ctx, ST_K_IND);
+    ST_CUDA(ctx, launch_inj_metro_propose(c->h, c->d_chain, c->d_injected, taken, ctx->stream));
+  }
+  if (int rc = zpass(c, kZMetro, 0)) return rc;
+  Bracket br(ctx, ST_K_IND);
+  return cuda_check(ctx, launch_inj_metro_accept(c->h, c->d_chain, c->d_injected, taken,
+                                                 ctx->stream),
+                    "injected UpdateQMetro");
+}
+
 // ===========================================================================
 // sweeps
 // ===========================================================================
@@ -2134,6 +2189,27 @@ extern "C" int st_chain_save(st_chain* c, const char* path) {
   return ok ? ST_OK : seterr(ctx, ST_ERR_ARG, "writing %s failed", path);
 }
 
+// The options a checkpoint must share with the chain it is loaded into: every
+// st_model field except the Z-pass tile (draws do not depend on it) and
+// NUMREPS (only where st_run stops).  Field by field, so struct padding in the
+// file never matters.
+static bool same_model(const st_model& a, const st_model& b) {
+#define ST_SAME(f) (a.f == b.f)
+  return ST_SAME(maxpops) && ST_SAME(burnin) && ST_SAME(noadmix) && ST_SAME(linkage) &&
+         ST_SAME(usepopinfo) && ST_SAME(locprior) && ST_SAME(freqscorr) && ST_SAME(onefst) &&
+         ST_SAME(inferalpha) && ST_SAME(popalphas) && ST_SAME(inferlambda) &&
+         ST_SAME(popspecificlambda) && ST_SAME(unifprioralpha) && ST_SAME(computeprob) &&
+         ST_SAME(pfrompopflagonly) && ST_SAME(ancestdist) && ST_SAME(numboxes) &&
+         ST_SAME(metrofreq) && ST_SAME(recessivealleles) && ST_SAME(alpha) &&
+         ST_SAME(alphamax) && ST_SAME(alphapropsd) && ST_SAME(alphapriora) &&
+         ST_SAME(alphapriorb) && ST_SAME(lambda) && ST_SAME(fpriormean) && ST_SAME(fpriorsd) &&
+         ST_SAME(store_z) && ST_SAME(precision) && ST_SAME(mala) && ST_SAME(mala_target) &&
+         ST_SAME(admburnin) && ST_SAME(gensback) && ST_SAME(popflag_given) &&
+         ST_SAME(updatelocprior) && ST_SAME(startatpopinfo) && ST_SAME(migrprior) &&
+         ST_SAME(locpriorinit) && ST_SAME(maxlocprior) && ST_SAME(locpriorstep);
+#undef ST_SAME
+}
+
 extern "C" int st_chain_load(st_chain* c, const char* path) {
   if (!c || !path) return ST_ERR_ARG;
   st_ctx* ctx = c->ctx;
@@ -2163,20 +2239,30 @@ extern "C" int st_chain_load(st_chain* c, const char* path) {
     fclose(f);
     return seterr(ctx, ST_ERR_STATE, "%s is not a checkpoint of a chain of this shape", path);
   }
-  std::vector<char> buf;
-  ST_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (const CkField& fl : ckpt_fields(c)) {
-    uint64_t n = 0;
-    if (fread(&n, 8, 1, f) != 1 || n != fl.bytes) { ok = false; break; }
-    buf.resize(fl.bytes);
-    if (fread(buf.data(), 1, fl.bytes, f) != fl.bytes) { ok = false; break; }
-    if (cudaMemcpy(fl.p, buf.data(), fl.bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
-      fclose(f);
-      return seterr(ctx, ST_ERR_CUDA, "checkpoint upload failed");
-    }
+  if (!same_model(model, c->model)) {
+    fclose(f);
+    return seterr(ctx, ST_ERR_STATE,
+                  "%s was saved by a chain with other model options (st_model)", path);
   }
+  // every field is read and size-checked before any of the chain's device
+  // memory is written, so a truncated or mismatched file leaves it unchanged
+  const std::vector<CkField> fields = ckpt_fields(c);
+  std::vector<std::vector<char>> bufs(fields.size());
+  for (size_t j = 0; ok && j < fields.size(); j++) {
+    uint64_t n = 0;
+    if (fread(&n, 8, 1, f) != 1 || n != fields[j].bytes) { ok = false; break; }
+    bufs[j].resize(fields[j].bytes);
+    if (fread(bufs[j].data(), 1, fields[j].bytes, f) != fields[j].bytes) ok = false;
+  }
+  char extra;
+  if (ok && fread(&extra, 1, 1, f) != 0) ok = false;   // trailing bytes: another layout
   fclose(f);
   if (!ok) return seterr(ctx, ST_ERR_STATE, "%s is truncated or of another chain", path);
+  ST_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (size_t j = 0; j < fields.size(); j++)
+    if (cudaMemcpy(fields[j].p, bufs[j].data(), fields[j].bytes, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return seterr(ctx, ST_ERR_CUDA, "checkpoint upload failed");
   c->h.key = key;
   c->h.cnt_chunks = 1;
   c->h.cnt_groups = 1;

@@ -55,9 +55,16 @@ __device__ __forceinline__ double rnd31(U4 w) {
   return 1.0 / 4294967296.0;
 }
 
-// 24-bit uniform in [0,1) for the FP32 categorical draw.
-__device__ __forceinline__ float u24(uint32_t w) {
-  return (float)(w >> 8) * (1.0f / 16777216.0f);
+// Uniform u in [0,1) for the categorical draw of Z: a Philox word's low 23
+// bits over 2^23.  neg_one_plus_u23 builds -(1 + u) directly from those bits
+// (exponent of -1, the bits as mantissa: exact), so that
+// fma(-(1 + u), T, T) = RN(T - (1 + u) T) = RN(-u T) in one rounding, which is
+// -RN(u T): the same threshold r = RN(u T) that u23(w) * T gives.
+__device__ __forceinline__ float u23(uint32_t w) {
+  return (float)(w & 0x7FFFFFu) * (1.0f / 8388608.0f);
+}
+__device__ __forceinline__ float neg_one_plus_u23(uint32_t w) {
+  return __uint_as_float(0xBF800000u | (w & 0x7FFFFFu));
 }
 
 constexpr double kTwoPi = 6.283185307179586;

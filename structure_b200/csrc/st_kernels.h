@@ -55,6 +55,13 @@ cudaError_t launch_popinfo(const ChainDev& h, const ChainDev* d_chain, cudaStrea
 // UpdateAlphaLocPrior (global and location alphas, with their sums).
 cudaError_t launch_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
 cudaError_t launch_alpha_locprior(const ChainDev& h, const ChainDev* d_chain, cudaStream_t s);
+// Injected-array parity modes (st_injected.cu): UpdateP and the proposal and
+// accept steps of UpdateQMetro with the reference's own samplers.
+cudaError_t launch_inj_p(const ChainDev& h, ChainDev* d_chain, const double* uni, cudaStream_t s);
+cudaError_t launch_inj_metro_propose(const ChainDev& h, ChainDev* d_chain, const double* uni,
+                                     int* taken, cudaStream_t s);
+cudaError_t launch_inj_metro_accept(const ChainDev& h, ChainDev* d_chain, const double* uni,
+                                    const int* taken, cudaStream_t s);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
 cudaError_t launch_clear_counts(const ChainDev* d_table, int nchains, cudaStream_t s);
 

@@ -24,7 +24,8 @@
 //  * The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it; that may
 //    load this library's device code.  Make the first call before any stream
-//    capture.
+//    capture.  The cached address belongs to the device's context: after a
+//    cudaDeviceReset the library has to be loaded again.
 #include <cuda_runtime.h>
 
 #include <cstdint>

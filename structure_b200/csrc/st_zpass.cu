@@ -173,7 +173,7 @@ zpass_u8_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, i
         TF total;
         TF u;
         if (injected) u = (TF)ch.injected[(size_t)i * L * 2 + (size_t)l * 2 + taken];
-        else u = (TF)u24(wsel[line]);
+        else u = (TF)u23(wsel[line]);
         taken++;
         z = pick_generic<TF>(q, Pl, K, A, a, u, total, errb);
         if (want_like) like_acc += log(fmax((double)total, 1e-50));

@@ -22,10 +22,11 @@ namespace zfast {
 
 constexpr float kLikeTinyF = 1e-30f;
 // ln P(D) fast path: the genotype terms Q.P(copy 0) * Q.P(copy 1) of four
-// genotypes are multiplied in FP32 and logged once.  Each factor above this
-// bound keeps the product of four a normal float (>= 1e-36 > FLT_MIN); a word
-// holding a smaller term is recomputed exactly (word_like_exact).
-constexpr float kLikeFastMin = 1e-9f;
+// genotypes are multiplied in FP32 and logged once.  A product of four above
+// this bound has every factor above it too (factors are <= 1), so no partial
+// product is subnormal and no factor is near the reference's 1e-50 clamp; a
+// word holding a smaller product is recomputed exactly (word_like_exact).
+constexpr float kLikeFastMin = 1e-30f;
 
 // Deterministic block sum of one double per thread (fixed tree order).
 __device__ __forceinline__ double block_sum_d(double v, double* sred) {
@@ -93,7 +94,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
 //   X_k   = (P[l][k][a0], P[l][k][a1]) from a per-lane table indexed by the
 //           genotype class, so no per-copy select is executed;
 //   C_k   = fma(q_k, X_k, C_{k-1})  -- the cumulative mixture weights;
-//   r     = u * C_{K-1};  z = sum_k signbit(C_k - r) for k < K-1.
+//   r     = RN(u * C_{K-1});  z = sum_k signbit(C_k - r) for k < K-1.
 // sign(C_k - r) is exactly (C_k < r) in IEEE arithmetic without flush to zero,
 // so z is the reference's "first k with r <= cumsum_k" on FP32 weights.
 // The genotype loop of one lane (one locus) over the chunk's individuals,
@@ -240,20 +241,23 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
             for (int k = 1; k < KT; k++) Cs[k] = fma2_rn(Q2[k], X[k], Cs[k - 1]);
             const float2 Tp = Cs[KT - 1];
             if (MODE == kZNormal) {
-              const float2 U = make_float2(u24(h ? r4.z : r4.x), u24(h ? r4.w : r4.y));
-              // r = round(u*T), negated by flipping sign bits in the integer
-              // domain so the rounded product can never be fused into the add
-              const float2 NR =
-                  bits_f2(f2_bits(mul2_rn(U, Tp)) ^ 0x8000000080000000ull);
-              uint32_t s0 = 0, s1 = 0;
+              // NR = RN(-u T) for both copies: one fma of -(1 + u), built from
+              // the Philox words' low 23 bits, so the rounded threshold is
+              // never contracted into the compare below
+              const float2 NM = make_float2(neg_one_plus_u23(h ? r4.z : r4.x),
+                                            neg_one_plus_u23(h ? r4.w : r4.y));
+              const float2 NR = fma2_rn(NM, Tp, Tp);
+              // the sign bits of C_k - r (k < K-1) shifted into one word per
+              // copy; z = their count = #{k : C_k < r}
+              uint32_t t0 = 0u, t1 = 0u;
 #pragma unroll
               for (int k = 0; k < KT - 1; k++) {
                 const float2 D = add2_rn(Cs[k], NR);
-                s0 += __float_as_uint(D.x) >> 31;
-                s1 += __float_as_uint(D.y) >> 31;
+                t0 = __funnelshift_l(__float_as_uint(D.x), t0, 1);
+                t1 = __funnelshift_l(__float_as_uint(D.y), t1, 1);
               }
-              z0 = (int)s0;
-              z1 = (int)s1;
+              z0 = __popc(t0);
+              z1 = __popc(t1);
             }
             if (MODE == kZMetro) {
               const float4* t4 = reinterpret_cast<const float4*>(sT2 + row * KT2);
@@ -280,9 +284,11 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
             if (LIKE) {
               // j + h is a compile-time constant after unrolling
               const float pr = miss ? 1.0f : Tp.x * Tp.y;
-              wmin = fminf(wmin, pr);
               wprod = ((j + h) & 3) == 0 ? pr : wprod * pr;
-              if (((j + h) & 3) == 3) wlike += __logf(wprod);
+              if (((j + h) & 3) == 3) {
+                wmin = fminf(wmin, wprod);
+                wlike += __logf(wprod);
+              }
             }
           } else if (MODE == kZInit) {
             z0 = (int)(((uint64_t)((h ? r4.z : r4.x) >> 1) * (uint64_t)K) >> 31);

@@ -212,3 +212,66 @@ def config5(N=10000, L=500000, seed=None, want_int32=False):
     rng = np.random.default_rng(DATA_SEED_BASE + 5 if seed is None else seed)
     F = rng.uniform(0.01, 0.3, 10)
     return snp_fmodel(N, L, 10, F, 0.1, 0.02, int(rng.integers(1 << 31)), want_int32=want_int32)
+
+
+def snp_fmodel_device(N, L, K, F, qalpha, missing, seed, p_beta=(1.0, 1.0), indep_beta=None,
+                      chunk=2048, device="cuda"):
+    """snp_fmodel's generative model drawn on a CUDA device with torch's
+    generator (seeded), for the large shapes where the NumPy version takes
+    minutes (N=10,000 x L=500,000 is 5e9 genotypes).  Same model and the same
+    canonical coding (first non-missing copy of a locus is allele 0,
+    heterozygotes 0/1, whole genotypes missing); different random numbers.
+    Returns dict(packed [L][ceil(N/16)] uint32, numalleles, N, L, K)."""
+    import torch
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    torch.manual_seed(int(seed))       # torch._standard_gamma draws from the default generator
+    F = torch.as_tensor(np.asarray(F, np.float64), device=dev)
+    fr = (1.0 - F) / F
+    gq = torch._standard_gamma(torch.full((N, K), float(qalpha), dtype=torch.float64, device=dev))
+    Q = gq / gq.sum(1, keepdim=True).clamp_min(1e-300)
+    cq = torch.cumsum(Q, 1)[:, :K - 1].float().contiguous()           # [N, K-1]
+    wpr = (N + 15) // 16
+    packed = np.zeros((L, wpr), np.uint32)
+    numalleles = np.zeros(L, np.int32)
+    shifts = (2 * torch.arange(16, device=dev, dtype=torch.int64)).view(1, 16, 1)
+    for l0 in range(0, L, chunk):
+        l1 = min(L, l0 + chunk)
+        n = l1 - l0
+        if tuple(p_beta) == (1.0, 1.0):
+            p = torch.rand(n, generator=gen, device=dev, dtype=torch.float64)
+        else:
+            a = torch._standard_gamma(torch.full((n,), p_beta[0], dtype=torch.float64, device=dev))
+            b = torch._standard_gamma(torch.full((n,), p_beta[1], dtype=torch.float64, device=dev))
+            p = a / (a + b)
+        p = p.clamp(1e-4, 1 - 1e-4)
+        if indep_beta is None:
+            ca = (p[None, :] * fr[:, None]).clamp_min(1e-300)
+            cb = ((1 - p)[None, :] * fr[:, None]).clamp_min(1e-300)
+        else:
+            ca = torch.full((K, n), float(indep_beta[0]), dtype=torch.float64, device=dev)
+            cb = torch.full((K, n), float(indep_beta[1]), dtype=torch.float64, device=dev)
+        ga, gb = torch._standard_gamma(ca), torch._standard_gamma(cb)
+        P1 = (ga / (ga + gb).clamp_min(1e-300)).float().t().contiguous()  # [n, K]
+        u = torch.rand((N, 2 * n), generator=gen, device=dev)
+        z = torch.searchsorted(cq, u, right=False).view(N, 2, n)          # #(cq_k < u)
+        v = torch.rand((N, 2, n), generator=gen, device=dev)
+        lidx = torch.arange(n, device=dev).view(1, 1, n)
+        a1 = v < P1[lidx, z]
+        g = a1.sum(1, dtype=torch.uint8)                                   # [N, n]
+        g[torch.rand((N, n), generator=gen, device=dev) < missing] = 3
+        ok = g != 3
+        anyok = ok.any(0)
+        first = ok.to(torch.uint8).argmax(0)
+        flip = anyok & (g[first, torch.arange(n, device=dev)] == 2)
+        g = torch.where(flip[None, :] & ok, 2 - g, g)
+        has0 = ((g == 0) | (g == 1)).any(0)
+        has1 = ((g == 1) | (g == 2)).any(0)
+        numalleles[l0:l1] = (has0.int() + has1.int()).cpu().numpy()
+        gp = torch.full((wpr * 16, n), 3, dtype=torch.int64, device=dev)
+        gp[:N] = g.to(torch.int64)
+        w = (gp.view(wpr, 16, n) << shifts).sum(1)                         # [wpr, n]
+        packed[l0:l1] = w.t().contiguous().cpu().numpy().astype(np.uint32)
+        del u, z, v, a1, g, gp, w
+    return dict(packed=packed, numalleles=numalleles, N=N, L=L, K=K)

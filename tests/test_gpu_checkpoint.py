@@ -77,3 +77,47 @@ def test_resume_into_a_chain_with_another_tile(ctx, tmp_path):
     for x in (a, fresh):
         x.close()
     data.close()
+
+
+def test_bad_checkpoints_leave_the_chain_unchanged(ctx, tmp_path):
+    """A truncated file, a file with trailing bytes and a file saved under other
+    model options are refused with ST_ERR_STATE before any device memory of
+    the chain is written: its state afterwards equals its state before."""
+    d = synth.snp_fmodel(120, 500, 3, np.linspace(0.05, 0.2, 3), 0.4, 0.03, 19)
+    data = api.Data(ctx, d["numalleles"], packed=d["packed"], layout=api.LAYOUT_B2G,
+                    num_inds=120, num_loci=500)
+    mk = lambda burnin, numreps: api.model_defaults(maxpops=3, burnin=burnin, numreps=numreps,
+                                                    freqscorr=1, metrofreq=3)
+    src = api.Chain(ctx, data, mk(2, 20), 31)
+    src.sweep(5)
+    path = str(tmp_path / "good.ckpt")
+    src.save(path)
+    raw = open(path, "rb").read()
+    dst = api.Chain(ctx, data, mk(2, 20), 32)
+    dst.sweep(2)
+    before = {f: dst.get(f) for f in FIELDS}
+    for name, blob in (("truncated", raw[:len(raw) - 100]), ("trailing", raw + b"\0\0\0\0")):
+        p = str(tmp_path / f"{name}.ckpt")
+        with open(p, "wb") as fh:
+            fh.write(blob)
+        with pytest.raises(api.StError) as e:
+            dst.load(p)
+        assert e.value.code == api.ST_ERR_STATE, name
+    # the same shape but another BURNIN: refused as well
+    other = api.Chain(ctx, data, mk(7, 20), 33)
+    with pytest.raises(api.StError) as e:
+        other.load(path)
+    assert e.value.code == api.ST_ERR_STATE
+    for f in FIELDS:
+        a, b = dst.get(f), before[f]
+        if isinstance(a, int):
+            assert a == b, f
+        else:
+            np.testing.assert_array_equal(a, b, err_msg=f"field {f}")
+    # NUMREPS alone may differ (it only says where st_run stops)
+    more = api.Chain(ctx, data, mk(2, 50), 34)
+    more.load(path)
+    assert more.get(api.F_REP) == 5
+    for x in (src, dst, other, more):
+        x.close()
+    data.close()

@@ -4,8 +4,10 @@ streams.
 
 Tolerances: Z draws and counts are bit-exact; Dirichlet/gamma draws within
 1e-5 relative (FP32 storage of an FP64 draw); ln P(D) within 1e-5 relative;
-Metropolis decisions identical except inside a tie band of 1e-6 around the
-acceptance threshold.
+Metropolis log ratios within the FP32 error bound derived per individual from
+the fast log's documented error and the number of genotypes
+(conftest.metro_terms_and_bound), and Metropolis decisions identical to those
+on the oracle's FP64 ratios outside that band.
 """
 import numpy as np
 import pytest
@@ -255,11 +257,29 @@ def test_updateq_metro_matches_oracle(ctx, orc, layout):
     np.testing.assert_allclose(c.get(api.F_TESTQ), T, rtol=1e-5, atol=1e-35)
     ld_dev = c.get(api.F_LOGDIFF)
     ld_o = orc.metro_logdiff(geno, Q, c.get(api.F_TESTQ), P)
-    np.testing.assert_allclose(ld_dev, ld_o, rtol=1e-5, atol=2e-3)
+    _check_logdiff(orc, geno, Q, c.get(api.F_TESTQ), P, ld_dev, ld_o, 20)
     Qo, lQo, acc = orc.metro_accept(ld_dev, SEED, 20, Q, lQ, c.get(api.F_TESTQ), c.get(api.F_LOGTESTQ))
     np.testing.assert_array_equal(c.get(api.F_Q), Qo)
-    assert 0 < acc.sum() < N or True
+    # a proposal from the prior is sometimes accepted at this size (57 of 150
+    # on the oracle): the accept path is exercised, not only the reject path
+    assert 0 < acc.sum() < N
     c.close(); d.close()
+
+
+def _check_logdiff(orc, geno, Q, T, P, ld_dev, ld_o, rep):
+    """The device's log ratios within the derived FP32 error bound of the
+    oracle's FP64 sums (conftest.metro_terms_and_bound), and the accept
+    decisions on the oracle's ratios equal to those on the device's outside
+    that band.  Returns the measured error relative to the bound."""
+    from conftest import check_metro_decisions, metro_terms_and_bound, metro_uniforms
+    ld64, mag, bound = metro_terms_and_bound(geno, Q, T, P)
+    np.testing.assert_allclose(ld64, ld_o, rtol=1e-9, atol=1e-9 * mag.max())
+    err = np.abs(ld_dev - ld_o)
+    assert (err <= bound).all(), (err / bound).max()
+    u = metro_uniforms(orc, geno.shape[0], SEED, rep)
+    inband, flips = check_metro_decisions(ld_dev, ld_o, bound, u)
+    assert flips <= inband
+    return float((err / bound).max())
 
 
 @pytest.mark.parametrize("K,layout", [(5, api.LAYOUT_B2G), (7, api.LAYOUT_B2G),
@@ -284,7 +304,7 @@ def test_metro_logdiff_across_k_classes(ctx, orc, K, layout):
     assert c.sync() == 0
     ld_dev = c.get(api.F_LOGDIFF)
     ld_o = orc.metro_logdiff(geno, Q, c.get(api.F_TESTQ), P)
-    np.testing.assert_allclose(ld_dev, ld_o, rtol=1e-5, atol=2e-3)
+    _check_logdiff(orc, geno, Q, c.get(api.F_TESTQ), P, ld_dev, ld_o, 20)
     Qo, _, _ = orc.metro_accept(ld_dev, SEED, 20, Q, lQ, c.get(api.F_TESTQ),
                                 c.get(api.F_LOGTESTQ))
     np.testing.assert_array_equal(c.get(api.F_Q), Qo)

@@ -47,11 +47,18 @@ def _state_and_reference(c):
     return Q, P, rep, n, m, like
 
 
-def test_noalloc_matches_chain_update_z_on_two_calls_in_a_row():
+@pytest.mark.parametrize("K,with_like", [(2, True), (5, True), (9, True), (20, False)])
+def test_noalloc_matches_chain_update_z_on_two_calls_in_a_row(orc, K, with_like):
+    """Two calls back to back on one stream, against the chain API's results
+    on the same state and against the oracle (Z drawn by the oracle from the
+    same Q, P and stream, then counted; ln P(D) of the same Q and P).  K=2 and
+    K=20 are even K classes (20 with two-warp CTAs), 5 and 9 odd ones with the
+    tail table; the K=20 case passes no ln P(D) output, which skips the
+    last-CTA reduction."""
     import torch
 
-    N, L, K = 700, 2600, 5
-    d = synth.snp_fmodel(N, L, K, np.linspace(0.05, 0.25, K), 0.4, 0.03, 21)
+    N, L = 700, 2600
+    d = synth.snp_fmodel(N, L, K, np.linspace(0.05, 0.25, K), 0.4, 0.03, 21 + K)
     packed, na = np.ascontiguousarray(d["packed"], np.uint32), d["numalleles"]
     wpr = (N + 15) // 16
     assert packed.shape == (L, wpr)
@@ -87,18 +94,30 @@ def test_noalloc_matches_chain_update_z_on_two_calls_in_a_row():
     # the two calls back to back on one stream, no host sync between them
     for (q, p), (n_o, m_o, like_o, err_o), s in zip(ins, outs, (s1, s2)):
         rc = f(0, g2.data_ptr(), wpr, N, L, K, q.data_ptr(), p.data_ptr(), SEED, s[2],
-               n_o.data_ptr(), m_o.data_ptr(), like_o.data_ptr(), err_o.data_ptr(),
-               C.c_void_p(stream.cuda_stream), C.byref(need))
+               n_o.data_ptr(), m_o.data_ptr(), like_o.data_ptr() if with_like else None,
+               err_o.data_ptr(), C.c_void_p(stream.cuda_stream), C.byref(need))
         assert rc == api.ST_OK, rc
         assert 0 < need.value <= NOALLOC_SCRATCH_BYTES
     torch.cuda.synchronize(dev)
 
-    for (n_o, m_o, like_o, err_o), (_, _, _, n_ref, m_ref, like_ref) in zip(outs, (s1, s2)):
+    geno = d["geno"]
+    for (n_o, m_o, like_o, err_o), (Q, P, rep, n_ref, m_ref, like_ref) in zip(outs, (s1, s2)):
         assert int(err_o.item()) == 0
         np.testing.assert_array_equal(n_o.cpu().numpy(), n_ref)
         np.testing.assert_array_equal(m_o.cpu().numpy(), m_ref)
-        like = float(like_o.item())
-        assert abs(like - like_ref) <= 1e-5 * abs(like_ref), (like, like_ref)
+        # the oracle: Z from the same Q, P and stream, then GetNumFromPops /
+        # GetNumLociPop on it
+        zo = orc.zupdate_f32(geno, Q, P, SEED, rep)
+        n_orc, m_orc = orc.counts(geno, zo, K, 2)
+        np.testing.assert_array_equal(n_o.cpu().numpy(), n_orc)
+        np.testing.assert_array_equal(m_o.cpu().numpy(), m_orc)
+        if with_like:
+            like = float(like_o.item())
+            assert abs(like - like_ref) <= 1e-5 * abs(like_ref), (like, like_ref)
+            like_orc = orc.calc_like(geno, Q, P)
+            assert abs(like - like_orc) <= 1e-5 * abs(like_orc), (like, like_orc)
+        else:
+            assert np.isnan(float(like_o.item()))   # not written
 
     # every observed allele copy is counted once in n and once in m
     copies = int(2 * N * L - 2 * np.count_nonzero(synth.unpack_int32(packed, N)[:, 0, :] < 0))
