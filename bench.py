@@ -607,6 +607,13 @@ def measure_config1(with_cpu=True):
     st = c.get(api.F_STATS)
     e2e_s = time.perf_counter() - t0
     assert c.sync() == 0
+    # per-kernel times from 200 more sweeps launch by launch (CUDA events)
+    ctx.profile(True)
+    ctx.profile_read()
+    b.sweep(200)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
     copies = int((geno >= 0).sum())
     sweeps = burn + reps
     out = {"workload": "config 1: N=200 L=100 microsatellites (2-10 alleles), K=3, "
@@ -617,6 +624,7 @@ def measure_config1(with_cpu=True):
                    "includes": "st_data_upload, st_chain_create, the whole run, QSum and "
                                "stats read back"},
            "gpu_launches": int(launches),
+           "kernel_us_per_sweep": {k: round(v[0] * 1e3 / 200, 2) for k, v in prof.items()},
            "mean_lnpd": round(st[api.ST_SUMLIKES] / max(1, st[api.ST_NLIKE]), 3),
            "roofline": {"bound": "launch", "achieved_us_per_sweep": round(ms * 1e3 / sweeps, 2),
                         "kernels_per_sweep": round(launches / sweeps, 2),
