@@ -23,7 +23,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <type_traits>
 
 #include "st_device.cuh"
 #include "st_kernels.h"
@@ -86,7 +85,7 @@ __device__ __forceinline__ void genotype_terms(uint32_t gt, T s0, T s1, T& w0, T
 
 template <typename T, int KT>
 __global__ void __launch_bounds__(kGradBlock) grad_ind_kernel(GradArgs a) {
-  __shared__ __align__(16) T sP[kLB][KT][2];
+  __shared__ T sP[kLB][KT][2];
   __shared__ uint32_t sW[kLB][kGradBlock / 16];
   const int N = a.N, L = a.L, K = a.K;
   const int i = blockIdx.x * kGradBlock + threadIdx.x;
@@ -94,16 +93,10 @@ __global__ void __launch_bounds__(kGradBlock) grad_ind_kernel(GradArgs a) {
   const T* Q = static_cast<const T*>(a.Q);
   const T* P = static_cast<const T*>(a.P);
   T q[KT], g[KT];
-  // FP32: (q_k, q_k) pairs and the packed gradient partials
-  float2 qq[std::is_same<T, float>::value ? KT : 1], g2[std::is_same<T, float>::value ? KT : 1];
 #pragma unroll
   for (int k = 0; k < KT; k++) {
     q[k] = (valid && k < K) ? Q[(size_t)i * K + k] : T(0);
     g[k] = T(0);
-    if constexpr (std::is_same<T, float>::value) {
-      qq[k] = make_float2(q[k], q[k]);
-      g2[k] = make_float2(0.0f, 0.0f);
-    }
   }
   double ll = 0.0;
   const int l0 = blockIdx.y * a.lchunk_len;
@@ -126,47 +119,23 @@ __global__ void __launch_bounds__(kGradBlock) grad_ind_kernel(GradArgs a) {
     __syncthreads();
     if (valid) {
       T llb = T(0);
-      if constexpr (std::is_same<T, float>::value) {
-        // FP32: both alleles' sums and both gradient terms as packed FP32x2
-        // (sm_100 FFMA2): (S0, S1) += (q_k, q_k) * (P_k0, P_k1) and
-        // (G_k, G'_k) += (w0, w1) * (P_k0, P_k1), G + G' added at the end
 #pragma unroll 4
-        for (int j = 0; j < nj; j++) {
-          const uint32_t gt = (sW[j][myc] >> sh) & 3u;
-          const float2* pj = reinterpret_cast<const float2*>(&sP[j][0][0]);
-          float2 S = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < nj; j++) {
+        const uint32_t gt = (sW[j][myc] >> sh) & 3u;
+        T s0 = T(0), s1 = T(0);
 #pragma unroll
-          for (int k = 0; k < KT; k++) S = fma2_rn(qq[k], pj[k], S);
-          T w0, w1, lt;
-          genotype_terms(gt, S.x, S.y, w0, w1, lt);
-          llb += lt;
-          const float2 W = make_float2(w0, w1);
-#pragma unroll
-          for (int k = 0; k < KT; k++) g2[k] = fma2_rn(W, pj[k], g2[k]);
+        for (int k = 0; k < KT; k++) {
+          s0 = fma_t(q[k], sP[j][k][0], s0);
+          s1 = fma_t(q[k], sP[j][k][1], s1);
         }
-      } else {
-#pragma unroll 4
-        for (int j = 0; j < nj; j++) {
-          const uint32_t gt = (sW[j][myc] >> sh) & 3u;
-          T s0 = T(0), s1 = T(0);
+        T w0, w1, lt;
+        genotype_terms(gt, s0, s1, w0, w1, lt);
+        llb += lt;
 #pragma unroll
-          for (int k = 0; k < KT; k++) {
-            s0 = fma_t(q[k], sP[j][k][0], s0);
-            s1 = fma_t(q[k], sP[j][k][1], s1);
-          }
-          T w0, w1, lt;
-          genotype_terms(gt, s0, s1, w0, w1, lt);
-          llb += lt;
-#pragma unroll
-          for (int k = 0; k < KT; k++) g[k] = fma_t(w0, sP[j][k][0], fma_t(w1, sP[j][k][1], g[k]));
-        }
+        for (int k = 0; k < KT; k++) g[k] = fma_t(w0, sP[j][k][0], fma_t(w1, sP[j][k][1], g[k]));
       }
       ll += (double)llb;
     }
-  }
-  if constexpr (std::is_same<T, float>::value) {
-#pragma unroll
-    for (int k = 0; k < KT; k++) g[k] = g2[k].x + g2[k].y;
   }
   if (valid) {
     T* gq = static_cast<T*>(a.gqpart) + ((size_t)blockIdx.y * N + i) * K;
@@ -179,28 +148,19 @@ __global__ void __launch_bounds__(kGradBlock) grad_ind_kernel(GradArgs a) {
 
 template <typename T, int KT>
 __global__ void __launch_bounds__(kGradBlock) grad_loc_kernel(GradArgs a) {
-  // Q rows of a stage; FP32 keeps each entry twice, (q, q), for the packed
-  // FP32x2 multiply-adds
-  constexpr int QW = std::is_same<T, float>::value ? 2 : 1;
-  __shared__ __align__(16) T sQ[kIB][KT * QW];
+  __shared__ T sQ[kIB][KT];
   const int N = a.N, L = a.L, K = a.K;
   const int l = blockIdx.x * kGradBlock + threadIdx.x;
   const bool valid = l < L;
   const T* Q = static_cast<const T*>(a.Q);
   const T* P = static_cast<const T*>(a.P);
   T p0[KT], p1[KT], g0[KT], g1[KT];
-  constexpr int KP = std::is_same<T, float>::value ? KT : 1;
-  float2 pp[KP], gg[KP];   // FP32: (p_k0, p_k1) and the packed gradient partials
 #pragma unroll
   for (int k = 0; k < KT; k++) {
     const bool in = valid && k < K;
     p0[k] = in ? P[((size_t)l * K + k) * 2] : T(0);
     p1[k] = in ? P[((size_t)l * K + k) * 2 + 1] : T(0);
     g0[k] = g1[k] = T(0);
-    if constexpr (std::is_same<T, float>::value) {
-      pp[k] = make_float2(p0[k], p1[k]);
-      gg[k] = make_float2(0.0f, 0.0f);
-    }
   }
   const int i0 = blockIdx.y * a.ichunk_len;   // a multiple of 16
   const int i1 = min(N, i0 + a.ichunk_len);
@@ -210,13 +170,7 @@ __global__ void __launch_bounds__(kGradBlock) grad_loc_kernel(GradArgs a) {
     __syncthreads();
     for (int idx = threadIdx.x; idx < kIB * KT; idx += kGradBlock) {
       const int r = idx / KT, k = idx - r * KT;
-      const T v = (r < ni && k < K) ? Q[(size_t)(ib + r) * K + k] : T(0);
-      if constexpr (QW == 2) {
-        sQ[r][2 * k] = v;
-        sQ[r][2 * k + 1] = v;
-      } else {
-        sQ[r][k] = v;
-      }
+      sQ[r][k] = (r < ni && k < K) ? Q[(size_t)(ib + r) * K + k] : T(0);
     }
     __syncthreads();
     if (!valid) continue;
@@ -227,41 +181,20 @@ __global__ void __launch_bounds__(kGradBlock) grad_loc_kernel(GradArgs a) {
       for (int h = 0; h < nh; h++) {
         const uint32_t gt = (w >> (2 * h)) & 3u;
         const T* q = sQ[wj + h];
-        if constexpr (std::is_same<T, float>::value) {
-          // FP32: (S0, S1) += (q_k, q_k) * (p_k0, p_k1) and
-          // (g_k0, g_k1) += (w0, w1) * (q_k, q_k) as packed FP32x2
-          const float2* q2 = reinterpret_cast<const float2*>(q);
-          float2 S = make_float2(0.0f, 0.0f);
+        T s0 = T(0), s1 = T(0);
 #pragma unroll
-          for (int k = 0; k < KT; k++) S = fma2_rn(q2[k], pp[k], S);
-          T w0, w1, lt;
-          genotype_terms(gt, S.x, S.y, w0, w1, lt);
-          const float2 W = make_float2(w0, w1);
+        for (int k = 0; k < KT; k++) {
+          s0 = fma_t(q[k], p0[k], s0);
+          s1 = fma_t(q[k], p1[k], s1);
+        }
+        T w0, w1, lt;
+        genotype_terms(gt, s0, s1, w0, w1, lt);
 #pragma unroll
-          for (int k = 0; k < KT; k++) gg[k] = fma2_rn(W, q2[k], gg[k]);
-        } else {
-          T s0 = T(0), s1 = T(0);
-#pragma unroll
-          for (int k = 0; k < KT; k++) {
-            s0 = fma_t(q[k], p0[k], s0);
-            s1 = fma_t(q[k], p1[k], s1);
-          }
-          T w0, w1, lt;
-          genotype_terms(gt, s0, s1, w0, w1, lt);
-#pragma unroll
-          for (int k = 0; k < KT; k++) {
-            g0[k] = fma_t(w0, q[k], g0[k]);
-            g1[k] = fma_t(w1, q[k], g1[k]);
-          }
+        for (int k = 0; k < KT; k++) {
+          g0[k] = fma_t(w0, q[k], g0[k]);
+          g1[k] = fma_t(w1, q[k], g1[k]);
         }
       }
-    }
-  }
-  if constexpr (std::is_same<T, float>::value) {
-#pragma unroll
-    for (int k = 0; k < KT; k++) {
-      g0[k] = gg[k].x;
-      g1[k] = gg[k].y;
     }
   }
   if (valid) {
