@@ -844,6 +844,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
   }
   h.g2 = data->g2; h.g8 = data->g8; h.numalleles = data->numalleles; h.popflags = data->popflags;
   h.g2t = data->g2t; h.nlw4 = data->nlw4;
+  h.loc_tpl = locus_lanes(L);
 
   c->fast = data->layout == kLayoutB2G && model->precision == 0 && fast_kt(K) > 0;
   if (data->layout == kLayoutB2G && !c->fast) {

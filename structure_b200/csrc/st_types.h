@@ -65,6 +65,7 @@ struct ChainDev {
   double alphamax, alphapropsd, alphapriora, alphapriorb;
   double fpriormean, fpriorsd, invsqrtnuminds;
   uint32_t key;             // seed32: low word of splitmix64(chain seed)
+  int loc_tpl;              // locus kernel: lanes per locus (power of two, 1..32)
   // Z-pass tiling: T individuals per chunk, W warps, R locus blocks per CTA
   int tileT, tileW, tileR, nchunks, ngroups;
   // count histogram slices summed by the consumers (1: every producer adds

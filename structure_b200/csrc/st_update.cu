@@ -50,12 +50,16 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   ChainDev& ch = chains[c];
   const int tile = blockIdx.x - prefix[c];
   const int L = ch.L, K = ch.K, A = ch.A;
-  const int l = tile * blockDim.x + threadIdx.x;
-  const bool lvalid = l < L;
+  // tpl lanes per locus (1 unless the chain has few loci): the P draws of a
+  // locus are spread over them; eps and F run on the first lane of each locus
+  const int tpl = ch.loc_tpl;
+  const int l = tile * ((int)blockDim.x / tpl) + (int)threadIdx.x / tpl;
+  const int sub = (int)threadIdx.x % tpl;
+  const bool lvalid = l < L && sub == 0;
   const int rep = *ch.rep;
   const uint32_t key = ch.key;
   const bool collect = (stages & kLocCollect) && (rep + 1 > ch.burnin);
-  const int na = lvalid ? ch.numalleles[l] : 0;
+  const int na = (l < L) ? ch.numalleles[l] : 0;
   const bool fstage = (stages & kLocFst) && ch.freqscorr;
   const int numfst = ch.onefst ? 1 : K;
   if (ch.freqscorr && (stages & (kLocP | kLocEps | kLocFst))) {
@@ -68,7 +72,63 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   int errb = 0;
 
   // ---- P ------------------------------------------------------------------
-  if ((stages & kLocP) && lvalid && na > 0) {
+  if ((stages & kLocP) && tpl > 1) {
+    // lanes (k, j) of the locus: population k (strided by tpl / J when K
+    // exceeds it), alleles a = j, j + J, ...; the Dirichlet's log-sum over the
+    // alleles of (l, k) is a width-J butterfly over contiguous lanes
+    int J = 1;
+    while (J * 2 * K <= tpl && J * 2 <= 32) J *= 2;
+    const int kslots = tpl / J;
+    const int j = sub % J, k0 = sub / J;
+    // lanes of a locus stay together through the loop: every lane runs the
+    // same number of rounds
+    for (int kb = 0; kb < K; kb += kslots) {
+      const int k = kb + k0;
+      const bool kv = l < L && na > 0 && k < K;
+      const size_t base = ((size_t)(l < L ? l : 0) * K + (k < K ? k : 0)) * A;
+      double lg[kMaxAlleles];
+      double M = -INFINITY;
+      int nmine = 0;
+      if (kv) {
+        for (int a = j; a < na && a < kMaxAlleles; a += J) {
+          int n = 0;
+          for (int cc = 0; cc < ch.cnt_chunks; cc++)
+            n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
+          const double shape = ch.freqscorr ? ch.eps[(size_t)l * A + a] * sFrac[k] + (double)n
+                                            : ch.lambda[k] + (double)n;
+          lg[nmine] = log_gamma_draw(shape, (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+          M = lg[nmine] > M ? lg[nmine] : M;
+          nmine++;
+        }
+      }
+      M = group_max(M, J);
+      double S = 0.0;
+      for (int t = 0; t < nmine; t++) S += exp(lg[t] - M);
+      S = group_sum(S, J);
+      const double ls = M + log(S);
+      const int nac = na < kMaxAlleles ? na : kMaxAlleles;
+      if (kv) {
+        if (na > kMaxAlleles) errb |= kErrBounds;
+        int t = 0;
+        for (int a = j; a < nac; a += J, t++) {
+          double lp, p;
+          if (ls < kLogUnderflo) {
+            p = 1.0 / (double)nac;
+            lp = -log((double)nac);
+          } else {
+            lp = lg[t] - ls;
+            p = exp(lp);
+          }
+          const float pf = (float)p;
+          ch.P[base + a] = pf;
+          ch.logP[base + a] = (float)lp;
+          if (collect) ch.PSum[base + a] += (double)pf;
+          if (!(pf == pf)) errb |= kErrNaN;
+        }
+      }
+    }
+  }
+  if ((stages & kLocP) && tpl == 1 && lvalid && na > 0) {
     for (int k = 0; k < K; k++) {
       const size_t base = ((size_t)l * K + k) * A;
       auto shape_of = [&](int a) {
@@ -188,7 +248,7 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
       if (lane == 0) sF[warp * numfst + j] = v;
     }
     __syncthreads();
-    const int nblocks = (L + blockDim.x - 1) / blockDim.x;
+    const int nblocks = (L * tpl + blockDim.x - 1) / blockDim.x;
     if (threadIdx.x < numfst) {
       double s = 0.0;
       for (int w = 0; w < nwarps; w++) s += sF[w * numfst + threadIdx.x];
@@ -231,7 +291,16 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   if (errb) set_err(ch.err, errb);
 }
 
-int ctas_locus(const ChainDev& c, int block) { return (c.L + block - 1) / block; }
+int ctas_locus(const ChainDev& c, int block) { return (c.L * c.loc_tpl + block - 1) / block; }
+
+// Lanes per locus of the locus kernel: 1 for most chains; with fewer loci
+// than about two waves of threads, up to 32 per locus (a power of two), so a
+// small chain's Dirichlet draws run in parallel over populations and alleles.
+int locus_lanes(int L) {
+  int t = 1;
+  while (t < 32 && (size_t)L * t * 2 <= (size_t)148 * 256 * 2) t *= 2;
+  return t;
+}
 
 cudaError_t launch_locus(const LaunchSet& ls, int stages, int block) {
   locus_kernel<<<ls.total_ctas, block, 0, ls.stream>>>(ls.chains, ls.prefix, ls.nchains, stages);
