@@ -18,8 +18,8 @@ LIB = os.path.join(HERE, "libstgpu.so")
 SOURCES = ["st_zpass.cu", "st_zpass_k1.cu", "st_zpass_k2.cu", "st_zpass_k3.cu",
            "st_zpass_k4.cu", "st_zpass_k5.cu", "st_zpass_k6.cu", "st_update.cu", "st_api.cu",
            "st_noalloc.cu", "st_grad.cu", "st_noadmix.cu",
-           "st_popinfo.cu", "st_locprior.cu", "st_injected.cu", "st_zpass_ind.cu"]
-HEADERS = ["st_device.cuh", "st_types.h", "st_kernels.h", "st_zpass_fast.cuh", "st_zpass_ind.cuh"]
+           "st_popinfo.cu", "st_locprior.cu", "st_injected.cu"]
+HEADERS = ["st_device.cuh", "st_types.h", "st_kernels.h", "st_zpass_fast.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",

@@ -41,8 +41,6 @@ struct st_data {
   st_ctx* ctx = nullptr;
   int N = 0, L = 0, A = 1, layout = kLayoutU8, wpr = 0, Leff = 0;
   uint32_t* g2 = nullptr;
-  uint32_t* g2t = nullptr;   // individual-major copy for the individual-lane Z pass
-  int nlw4 = 0;
   uint8_t* g8 = nullptr;
   int32_t* numalleles = nullptr;
   int32_t* popflags = nullptr;
@@ -301,14 +299,6 @@ void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R)
   *R = r;
 }
 
-// The Z update with counts (mode Normal) runs one lane per individual for K
-// classes up to kZIndMaxKT (st_zpass_ind.cuh) and one lane per locus above
-// (st_zpass_fast.cuh); the other modes keep the locus-lane pass.  Both draw
-// the same Z and counts.
-bool use_zind(const ChainDev& h, int KT) {
-  return KT <= kZIndMaxKT && h.g2t != nullptr && h.tileW == 8;
-}
-
 int zpass(st_chain* c, int mode, int flags) {
   Bracket br(c->ctx, mode == kZMetro ? ST_K_METRO : (mode == kZNormal ? ST_K_ZPASS : ST_K_OTHER));
   st_ctx* ctx = c->ctx;
@@ -318,8 +308,6 @@ int zpass(st_chain* c, int mode, int flags) {
   }
   if (c->fast) {
     LaunchSet ls = single(c, ctas_zpass_b2g(c->h));
-    if (mode == kZNormal && use_zind(c->h, c->KT))
-      return cuda_check(c->ctx, launch_zpass_ind(ls, c->KT, flags), "zpass_ind");
     return cuda_check(c->ctx, launch_zpass_b2g(ls, c->KT, c->h.tileW, mode, flags, c->zsmem),
                       "zpass_b2g");
   }
@@ -657,16 +645,6 @@ extern "C" int st_data_upload(st_ctx* ctx, const st_data_desc* d, st_data** out)
     if (!rc && d->packed)
       rc = count_b2g_device(ctx, s->g2, N, L, wpr, A, s->cnt_h.data(), s->tot_h.data());
     if (rc) { st_data_destroy(s); return rc; }
-    // the individual-major copy read by the individual-lane Z pass
-    s->nlw4 = (L + 63) / 64;
-    rc = ctx_alloc(ctx, (size_t)((N + 31) / 32) * s->nlw4 * 128 * sizeof(uint32_t), &p, nullptr,
-                   &s->bytes);
-    if (rc) { st_data_destroy(s); return rc; }
-    s->g2t = (uint32_t*)p;
-    ctx->launches++;
-    rc = cuda_check(ctx, launch_build_g2t(s->g2, wpr, N, L, s->g2t, 0), "individual-major genotypes");
-    if (!rc) rc = cuda_check(ctx, cudaDeviceSynchronize(), "individual-major genotypes");
-    if (rc) { st_data_destroy(s); return rc; }
   } else {
     const size_t n = (size_t)N * 2 * L;
     rc = ctx_alloc(ctx, n, &p, nullptr, &s->bytes);
@@ -697,8 +675,7 @@ extern "C" int st_data_destroy(st_data* s) {
   if (s->chains > 0) return seterr(s->ctx, ST_ERR_STATE, "data still used by %d chains", s->chains);
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
-  for (void* p : {(void*)s->g2, (void*)s->g2t, (void*)s->g8, (void*)s->numalleles,
-                  (void*)s->popflags})
+  for (void* p : {(void*)s->g2, (void*)s->g8, (void*)s->numalleles, (void*)s->popflags})
     ctx_free(s->ctx, p);
   delete s;
   return ST_OK;
@@ -843,7 +820,6 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     h.key = (uint32_t)z;
   }
   h.g2 = data->g2; h.g8 = data->g8; h.numalleles = data->numalleles; h.popflags = data->popflags;
-  h.g2t = data->g2t; h.nlw4 = data->nlw4;
   h.loc_tpl = locus_lanes(L);
 
   c->fast = data->layout == kLayoutB2G && model->precision == 0 && fast_kt(K) > 0;
@@ -1829,9 +1805,7 @@ extern "C" int st_batch_autotune(st_batch* b, int reps) {
           cudaMemsetAsync(h.mpart, 0, (size_t)h.N * h.K * 4, s);
         }
         cudaEventRecord(e0, s);
-        cudaError_t e = use_zind(b->table[g.first], g.KT)
-                            ? launch_zpass_ind(lg, g.KT, 0)
-                            : launch_zpass_b2g(lg, g.KT, g.W, kZNormal, 0, g.zsmem);
+        cudaError_t e = launch_zpass_b2g(lg, g.KT, g.W, kZNormal, 0, g.zsmem);
         cudaEventRecord(e1, s);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) rc = cuda_check(ctx, e, "autotune");
@@ -1902,10 +1876,7 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
       cudaStream_t gs = fork ? b->aux[gi] : s;
       if (fork) ST_CUDA(ctx, cudaStreamWaitEvent(gs, b->ev_fork, 0));
       LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, gs};
-      if (mode == kZNormal && use_zind(b->table[g.first], g.KT))
-        ST_CUDA(ctx, launch_zpass_ind(lg, g.KT, flags));
-      else
-        ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags, g.zsmem));
+      ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags, g.zsmem));
       if (fork) ST_CUDA(ctx, cudaEventRecord(b->ev_join[gi], gs));
     }
     if (fork)

@@ -39,13 +39,6 @@ int zpass_b2g_width(int KT);   // CTA width (warps) of the fast path for a K cla
 cudaError_t launch_zpass_b2g(const LaunchSet& ls, int KT, int W, int mode, int flags,
                              size_t smem);
 cudaError_t launch_zpass_u8(const LaunchSet& ls, int mode, int flags);
-// Individual-lane Z pass (mode Normal, K classes up to kZIndMaxKT) on the
-// chains' g2t copies; same tiles as the locus-lane pass.
-constexpr int kZIndMaxKT = 8;
-cudaError_t launch_zpass_ind(const LaunchSet& ls, int KT, int flags);
-// g2t [ceil(N/32)][ceil(L/64)][32][4] from the locus-major words g2 [L][wpr].
-cudaError_t launch_build_g2t(const uint32_t* g2, int wpr, int N, int L, uint32_t* g2t,
-                             cudaStream_t s);
 cudaError_t launch_locus(const LaunchSet& ls, int stages, int block);
 cudaError_t launch_ind(const LaunchSet& ls, int G, int mode, int stages, int block);
 cudaError_t launch_collect(const LaunchSet& ls, int block);

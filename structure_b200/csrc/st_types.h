@@ -73,11 +73,6 @@ struct ChainDev {
   int cnt_chunks, cnt_groups;
   // data
   const uint32_t* g2;
-  // the same 2-bit genotypes individual-major for the individual-lane Z pass:
-  // per 32 individuals and 64 loci one uint4 per individual (words of 16 loci,
-  // bits 2j..2j+1 = locus 16q+j), [ceil(N/32)][nlw4][32][4] words, padding 3
-  const uint32_t* g2t;
-  int nlw4;                 // ceil(L / 64)
   const uint8_t* g8;
   const int32_t* numalleles;
   const int32_t* popflags;
