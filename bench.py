@@ -359,10 +359,9 @@ def run_ours(args):
     sm_mhz = clk["sm_mhz"] or 1965.0
     alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e12
     # issue roofline of the same kernel, the limit it actually meets: warp
-    # instructions per 32 genotypes from the ncu capture of a burn-in launch
-    # (profiles/zpass_b2g_snp2000x50000_k5_batch20.txt); the timed launches also
-    # add the ln P(D) terms, so the fraction below is a lower bound
-    inst_per_32 = 115.6
+    # instructions per 32 genotypes from the ncu capture of a collecting launch
+    # (profiles/zpass_b2g_snp2000x50000_k5_batch20.txt), as the timed launches are
+    inst_per_32 = 120.0
     issue_achieved = B * N * L / 32 * inst_per_32 / (zavg / 1e3) / 1e12
     issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e12
     traffic = read_traffic()
@@ -412,9 +411,9 @@ def run_ours(args):
                            "peak": round(issue_peak, 4), "unit": "T warp-inst/s",
                            "frac": round(issue_achieved / issue_peak, 4),
                            "inst_per_32_genotypes": inst_per_32,
-                           "note": "instructions from an ncu capture of a burn-in launch "
-                                   "(no ln P(D) terms; lower bound); peak = 148 SM x 4 "
-                                   "schedulers x median SM clock"},
+                           "note": "instructions from an ncu capture of a collecting "
+                                   "launch (ln P(D) terms on, as in the timed sweeps); peak "
+                                   "= 148 SM x 4 schedulers x median SM clock"},
         "timed_path": "CUDA-graph replay of the batched sweep (st_batch_sweep, graphs on)",
         "profiled_pass": {"sweeps": PS, "ms_per_step": round(eager_ms, 4),
                           "note": "kernels_ms_per_step, kernel_share and the Z-pass launch "
