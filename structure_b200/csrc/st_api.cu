@@ -367,6 +367,15 @@ int check_model(st_ctx* ctx, const st_model* m) {
 
 }  // namespace
 
+// The Z-pass tile a chain of this shape gets by default (st_model tile fields
+// zero), for callers without a chain (st_update_z_noalloc).
+void st::default_zpass_tile(int N, int L, int K, int* T, int* W, int* R) {
+  st_model m{};
+  st_model_defaults(&m);
+  m.tile_t = m.tile_w = m.tile_r = 0;
+  choose_tile(&m, N, L, K, T, W, R);
+}
+
 // ===========================================================================
 // context
 // ===========================================================================

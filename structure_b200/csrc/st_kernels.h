@@ -35,6 +35,9 @@ enum : int { kIndGibbs = 0, kIndPropose = 1, kIndAccept = 2, kIndNone = 3 };
 enum : int { kIndAlpha = 0x1, kIndCollect = 0x2 };
 
 size_t zpass_b2g_smem(int KT, int K, int T, int W, int mode);
+// The default Z-pass tile (T individuals, W warps, R locus blocks) of a chain
+// of this shape (st_api.cu choose_tile).
+void default_zpass_tile(int N, int L, int K, int* T, int* W, int* R);
 int zpass_b2g_width(int KT);   // CTA width (warps) of the fast path for a K class
 cudaError_t launch_zpass_b2g(const LaunchSet& ls, int KT, int W, int mode, int flags,
                              size_t smem);

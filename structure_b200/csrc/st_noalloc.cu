@@ -67,38 +67,6 @@ int k_class(int K) {
   return 0;
 }
 
-// Same tile as a chain created with tile_t = tile_r = 0: T individuals per
-// chunk (shared memory of every Z-pass mode under 72 KB, or 110 KB where a
-// tile of 128 does not fit), the K class's width, and R locus blocks per CTA
-// for ~6 CTAs per SM.
-void pick_tile(int KT, int K, int N, int L, int* T, int* W, int* R) {
-  const int w = zpass_b2g_width(KT);
-  auto smem_all = [&](int t) {
-    size_t s = 0;
-    for (int mode : {kZNormal, kZMetro, kZInit, kZRecount, kZLike})
-      if (zpass_b2g_smem(KT, K, t, w, mode) > s) s = zpass_b2g_smem(KT, K, t, w, mode);
-    return s;
-  };
-  int t = 256;
-  const int np = (N + 15) & ~15;
-  if (t > np) t = np;
-  int t3 = t;
-  while (t3 > 128 && smem_all(t3) > 72 * 1024) t3 -= 16;
-  if (smem_all(t3) <= 72 * 1024) {
-    t = t3;
-  } else {
-    while (t > 32 && smem_all(t) > 110 * 1024) t -= 16;
-  }
-  const long lblocks = (L + 32 * w - 1) / (32 * w);
-  const long nch = (N + t - 1) / t;
-  long r = (lblocks * nch) / (148L * 3 * 2);
-  if (r < 1) r = 1;
-  if (r > 64) r = 64;
-  *T = t;
-  *W = w;
-  *R = (int)r;
-}
-
 // Copies the Z pass's histograms into the caller's layouts:
 // n_out[l][k][a] = npart[k][a][l], m_out[i][k] = mpart[i][k].
 __global__ void noalloc_sum_kernel(const Head* head, const int32_t* npart, const int32_t* mpart,
@@ -139,7 +107,7 @@ int run(int device, const uint32_t* g2, int wpr, int N, int L, int K, const floa
         double* like_out, int32_t* err_out, cudaStream_t stream, size_t* scratch_bytes) {
   const int KT = k_class(K);
   int T, W, R;
-  pick_tile(KT, K, N, L, &T, &W, &R);
+  default_zpass_tile(N, L, K, &T, &W, &R);   // the tile a chain of this shape gets
   const int nchunks = (N + T - 1) / T;
   const int lblocks = (L + 32 * W - 1) / (32 * W);
   const int ngroups = (lblocks + R - 1) / R;
