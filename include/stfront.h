@@ -103,6 +103,33 @@ int stf_write_results(stf_run *r, int rep, const double *QSum, const double *PSu
                       const double *sumlambda, const int32_t *AncestDist, double sumlikes,
                       double sumsqlikes);
 
+/* The screen trace printed every UPDATEFREQ sweeps (src/output.c:218-374
+ * PrintUpdate, called from src/structure.c:669-702 after sweep rep and once
+ * more after the last sweep when BURNIN + NUMREPS is not a multiple of
+ * UPDATEFREQ): the "BURNIN completed" and "Admixture Burnin complete" notes,
+ * the column heads every 10 * UPDATEFREQ sweeps (PrintBanner, output.c:377-454)
+ * preceded by the membership table of Q when PRINTQSUM=1 (PrintMembership),
+ * and the line of rep, lambda, alpha, F, r (LOCPRIOR), the net distances of
+ * P between clusters (PRINTNET or PRINTKLD) and Ln Like.  As in the
+ * reference, the Est Ln P(D) column of the line holds 0 outside the linkage
+ * model (output.c:258-279 evaluates it only there).  Q [N][K] and
+ * P [L][K][MAXALLELES] may be NULL when the line does not print them;
+ * alpha, F and lambda hold MAXPOPS values; locprior[0] is r (LOCPRIOR=1).
+ * The text goes to buf as snprintf would put it (NUL-terminated, cut to
+ * n - 1 bytes; buf may be NULL with n = 0); returns its full length, or a
+ * negative status (STF_ERR_UNSUPPORTED with LINKAGE=1).                   */
+int stf_format_update(const stf_run *r, int rep, const double *Q, const double *P,
+                      const double *alpha, const double *F, const double *lambda, double like,
+                      const double *locprior, char *buf, size_t n);
+
+/* ECHODATA=1: the start and end of the data as read (src/datain.c:514-571
+ * PrintSomeData, printed by ReadInputFile after the "Reading file" line):
+ * the first four individuals and the last two (all of them when there are
+ * six or fewer), each row with its label / population / popflag / phenotype
+ * columns, its first loci up to nine columns in all, and its last locus.
+ * Text as stf_format_update gives it.                                      */
+int stf_echo_data(const stf_run *r, char *buf, size_t n);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

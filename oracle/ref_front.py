@@ -11,12 +11,17 @@ process globals and exits on errors, so each scenario runs in its own process:
     python oracle/ref_front.py <workdir> <spec.json>
 
 spec: {"argv": [...], "read_data": bool, "sums": "<npz in workdir>" or null,
-       "rep": int}; with USEPOPINFO=1 the sums carry "usepop" [N][K][GENSBACK+1]
+       "rep": int, "trace": "<npz in workdir>" or null}; with USEPOPINFO=1 the sums carry "usepop" [N][K][GENSBACK+1]
 and CheckPopPriors (src/Init.c:15-70) runs before OutPutResults; with
 LOCPRIOR=1 they carry "sumLocPrior" (and sumAlpha of K * (locations + 1)
-values with admixture).  The working directory is <workdir> (the reference opens
-its files relative to it).  Results go to <workdir>/ref_out.json and
-<workdir>/ref_data.npz; OutPutResults writes OUTFILE_f (and OUTFILE_q).
+values with admixture).  "trace" holds, per screen-trace line, rep, like,
+alpha, F, lambda, locprior, Q and P, each passed to PrintUpdate
+(src/output.c:218-374) after the data are read.  The working directory is
+<workdir> (the reference opens its files relative to it).  Results go to
+<workdir>/ref_out.json and <workdir>/ref_data.npz; OutPutResults writes
+OUTFILE_f (and OUTFILE_q).  What the reference prints goes to
+<workdir>/ref_stdout.txt; ref_out.json gives the offsets in it where the data
+reading ("read_at", "read_end") and the trace ("trace_at") start and end.
 """
 import ctypes as C
 import json
@@ -49,6 +54,40 @@ class IND(C.Structure):
                 ("Phenotype", C.c_int), ("Location", C.c_int), ("myloc", C.c_int)]
 
 
+def _stdout_pos():
+    C.CDLL(None).fflush(None)
+    return os.lseek(1, 0, os.SEEK_CUR)
+
+
+def _trace(lib, g, spec, workdir, geno, na, inds, out):
+    """PrintUpdate for each line of the trace file (src/structure.c:681-702
+    passes the current Alpha, Fst, P, Q, like, sums, NumAlleles, R, lambda,
+    Individual and LocPrior)."""
+    z = np.load(os.path.join(workdir, spec["trace"]))
+    N = g("NUMINDS").value
+    if g("LOCDATA").value > 0 or g("LOCISPOP").value:
+        lib.GetNumLocations.argtypes = [C.c_void_p]
+        lib.GetNumLocations(inds)
+    if g("USEPOPINFO").value:
+        lib.CheckPopPriors.argtypes = [C.c_void_p]
+        lib.CheckPopPriors(inds)     # sets NOALPHA when every individual is flagged
+    vp = C.c_void_p
+    lib.PrintUpdate.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double,
+                                C.c_double, vp, vp, vp, vp, C.c_double, vp, vp, C.c_int]
+    R = np.zeros(N)
+    keep = []
+    out["trace_at"] = _stdout_pos()
+    for u in range(len(z["rep"])):
+        a = {k: np.ascontiguousarray(z[k][u], np.float64)
+             for k in ("alpha", "F", "lambda", "locprior", "Q", "P")}
+        keep.append(a)
+        P = lambda x: x.ctypes.data_as(vp)
+        lib.PrintUpdate(int(z["rep"][u]), geno, None, P(a["alpha"]), P(a["F"]), P(a["P"]),
+                        P(a["Q"]), float(z["like"][u]), 0.0, 0.0, na, P(R), P(a["lambda"]),
+                        inds, 0.0, None, P(a["locprior"]), a["locprior"].size)
+    out["trace_end"] = _stdout_pos()
+
+
 def main(workdir, specpath):
     with open(specpath) as f:
         spec = json.load(f)
@@ -70,7 +109,9 @@ def main(workdir, specpath):
         inds = (IND * N)()
         phase = (C.c_double * (N * L))()
         rec = (C.c_int * L)()
+        out["read_at"] = _stdout_pos()
         lib.ReadInputFile(geno, mapd, names, inds, phase, rec)
+        out["read_end"] = _stdout_pos()
         lib.FindMaxAlleles.restype = C.c_int
         A = lib.FindMaxAlleles(geno, rec)
         g("MAXALLELES").value = A
@@ -90,6 +131,8 @@ def main(workdir, specpath):
                  phenotype=np.array([x.Phenotype for x in inds]),
                  names=np.array([bytes(names[l * 15:(l + 1) * 15]).split(b"\0")[0].decode()
                                  for l in range(L)]))
+        if spec.get("trace"):
+            _trace(lib, g, spec, workdir, geno, na, inds, out)
         if spec.get("sums"):
             z = np.load(os.path.join(workdir, spec["sums"]))
             K = g("MAXPOPS").value
@@ -131,11 +174,14 @@ def main(workdir, specpath):
                               P(keep["sumlambda"]), P(slp) if slp is not None else None, lplen,
                               P(zeros["sil"]), P(zeros["iln"]),
                               len(argv), cargv)
+    C.CDLL(None).fflush(None)
     with open(os.path.join(workdir, "ref_out.json"), "w") as f:
         json.dump(out, f)
 
 
 if __name__ == "__main__":
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    os.dup2(devnull, 1)   # the reference prints progress on stdout
+    # the reference prints progress on stdout: keep it for the tests
+    fd = os.open(os.path.join(sys.argv[1], "ref_stdout.txt"),
+                 os.O_WRONLY | os.O_CREAT | os.O_TRUNC, 0o644)
+    os.dup2(fd, 1)
     main(sys.argv[1], sys.argv[2])

@@ -864,6 +864,48 @@ void net_table(const stf_run* r, Out& o, const double* P, int reps) {
   o.f("\n");
 }
 
+// The column heads of the screen trace (src/output.c:377-454 PrintBanner):
+// one head per printed column of trace_line, widened by a space per digit of
+// rep beyond five (and beyond nine before the likelihood heads).
+void trace_banner(const stf_run* r, Out& o, int rep) {
+  const int K = I(r, "MAXPOPS"), digits = (int)log10((double)rep);
+  o.f("\n");
+  for (int i = 4; i < digits; i++) o.f(" ");
+  o.f(" Rep#:   ");
+  if (I(r, "PRINTLAMBDA")) {
+    if (I(r, "POPSPECIFICLAMBDA"))
+      for (int k = 0; k < K; k++) o.f("Lambda%d ", k + 1);
+    else
+      o.f("Lambda  ");
+  }
+  if (!I(r, "NOADMIX") && !r->noalpha) {
+    o.f(" ");
+    if (I(r, "POPALPHAS"))
+      for (int k = 0; k < K; k++) o.f("Alpha%d ", k + 1);
+    else
+      o.f("Alpha  ");
+  }
+  if (I(r, "FREQSCORR")) {
+    o.f("   ");
+    if (I(r, "ONEFST")) o.f("Fst   ");
+    else
+      for (int k = 0; k < K; k++) o.f(" F%d   ", k + 1);
+    o.f(" ");
+  } else {
+    o.f(" ");
+  }
+  if (I(r, "LOCPRIOR")) o.f("  r     ");
+  if (I(r, "PRINTKLD") || I(r, "PRINTNET"))
+    for (int i = 0; i < K - 1; i++)
+      for (int j = i + 1; j < K; j++) o.f(" D%d,%d ", i + 1, j + 1);
+  if (I(r, "COMPUTEPROB")) {
+    o.f("   Ln Like ");
+    for (int i = 8; i < digits; i++) o.f(" ");
+    if (rep >= I(r, "BURNIN")) o.f(" Est Ln P(D)");
+  }
+  o.f("\n");
+}
+
 void sums(const stf_run* r, Out& o, const Sums& s) {
   const int K = I(r, "MAXPOPS"), reps = s.rep - I(r, "BURNIN");
   o.f("--------------------------------------------\n");
@@ -1164,4 +1206,131 @@ extern "C" int stf_write_results(stf_run* r, int rep, const double* QSum, const 
     if (!write_text(qn, q.s)) return fail(r, STF_ERR_IO, "Unable to open output file %s.", qn.c_str());
   }
   return STF_OK;
+}
+
+namespace {
+
+// Copies text into buf as snprintf would (NUL-terminated, truncated to n-1
+// bytes) and returns its full length.
+int give_text(const std::string& s, char* buf, size_t n) {
+  if (buf && n > 0) {
+    const size_t m = std::min(s.size(), n - 1);
+    memcpy(buf, s.data(), m);
+    buf[m] = '\0';
+  }
+  return (int)s.size();
+}
+
+}  // namespace
+
+extern "C" int stf_format_update(const stf_run* r, int rep, const double* Q, const double* P,
+                                 const double* alpha, const double* F, const double* lambda,
+                                 double like, const double* locprior, char* buf, size_t n) {
+  if (!r || !r->have_data || rep < 1 || !alpha || !F || !lambda) return STF_ERR_ARG;
+  const int K = I(r, "MAXPOPS"), burnin = I(r, "BURNIN"), every = I(r, "UPDATEFREQ");
+  const bool printnet = I(r, "PRINTKLD") || I(r, "PRINTNET");
+  const bool banner_now = rep == every || (rep < burnin && rep % (10 * every) == 0) ||
+                          (rep > burnin && (rep - burnin) % (10 * every) == 0);
+  const bool membership_now = banner_now && rep != burnin + I(r, "NUMREPS") && rep > 1 &&
+                              I(r, "PRINTQSUM") && K > 1;
+  if (I(r, "LINKAGE")) return STF_ERR_UNSUPPORTED;
+  if ((printnet && !P) || (membership_now && !Q) || (I(r, "LOCPRIOR") && !locprior))
+    return STF_ERR_ARG;
+  Out o;
+  if (rep > burnin && rep < burnin + every) o.f("\nBURNIN completed");
+  const int admburnin = I(r, "ADMBURNIN");
+  if (I(r, "NOADMIX") && admburnin > 0 && !I(r, "LOCPRIOR") && rep >= admburnin &&
+      rep < admburnin + every) {
+    o.f("\nAdmixture Burnin complete.  Current alpha");
+    if (I(r, "POPALPHAS")) {
+      o.f("s = ");
+      for (int k = 0; k < K; k++) o.f("%1.3f ", alpha[k]);
+    } else {
+      o.f(" = %1.3f ", alpha[0]);
+    }
+    o.f("\n\n");
+  }
+  if (banner_now && rep != burnin + I(r, "NUMREPS")) {
+    if (membership_now) membership(r, o, Q);
+    trace_banner(r, o, rep);
+  }
+  o.f("%5d:    ", rep);
+  if (I(r, "PRINTLAMBDA")) {
+    const int nl = I(r, "POPSPECIFICLAMBDA") ? K : 1;
+    for (int k = 0; k < nl; k++) o.f("%1.2f    ", lambda[k]);
+  }
+  if (!I(r, "NOADMIX") && !r->noalpha) {
+    if (I(r, "POPALPHAS"))
+      for (int k = 0; k < K; k++) o.f(k > 8 ? "%1.3f   " : "%1.3f  ", alpha[k]);
+    else
+      o.f("%1.3f  ", alpha[0]);
+  }
+  if (I(r, "FREQSCORR")) {
+    o.f("  ");
+    const int nf = I(r, "ONEFST") ? 1 : K;
+    for (int k = 0; k < nf; k++) o.f("%1.3f ", F[k]);
+    o.f("   ");
+  } else {
+    o.f("  ");
+  }
+  if (I(r, "LOCPRIOR")) o.f("%1.3f    ", locprior[0]);
+  if (printnet)
+    for (int i = 0; i < K - 1; i++)
+      for (int j = i + 1; j < K; j++) o.f("%1.3f ", net_d(r, i, j, P, 1));
+  if (I(r, "COMPUTEPROB")) {
+    // the reference evaluates Est Ln P(D) for this line only in its linkage
+    // branch (src/output.c:258-279), so outside it the column holds 0
+    if (rep > burnin + 2) o.f("  %.0f    %.0f ", like, 0.0);
+    else o.f("  --  ");
+  }
+  o.f("\n");
+  if (rep == burnin) {
+    o.f("\nBURNIN completed");
+    trace_banner(r, o, rep);
+  }
+  return give_text(o.s, buf, n);
+}
+
+extern "C" int stf_echo_data(const stf_run* r, char* buf, size_t n) {
+  if (!r || !r->have_data) return STF_ERR_ARG;
+  const int N = r->N, L = r->L, LINES = r->LINES, A = std::max(r->MAXALLELES, 1);
+  const bool label = I(r, "LABEL") != 0, popdata = I(r, "POPDATA") != 0;
+  const bool popflag = I(r, "POPFLAG") != 0, phenotype = I(r, "PHENOTYPE") != 0;
+  const int precols = (int)label + (int)popdata + (int)popflag + (int)phenotype;
+  Out o;
+  o.f("\n\nData file \"%s\" (truncated) --\n\n", S(r, "DATAFILE").c_str());
+  o.f("Ind:   ");
+  if (label) o.f("%5s ", "Label");
+  if (popdata) o.f("Pop ");
+  if (popflag) o.f("Flag ");
+  if (phenotype) o.f("Phen ");
+  if (precols > 1) o.f(": ");
+  o.f("Genotype_data . . . .\n");
+  // the values as the file gives them: codes back through the allele table
+  auto raw = [&](int i, int line, int l) {
+    const int v = r->geno[((size_t)i * LINES + line) * L + l];
+    return v == r->missing ? r->orig_missing : r->translation[(size_t)l * A + v];
+  };
+  // individuals 1..4 and the last two when there are more than 2 * LINES + 2
+  // (src/structure.h:15 MAXINDS = 3, src/datain.c:566-570)
+  const bool cut = N > 3 * LINES && N > 6;
+  const int shown = std::min(L, 9 - precols);
+  for (int i = 0; i < N; i++) {
+    if (cut && i > 3 && i < N - 2) continue;
+    for (int line = 0; line < LINES; line++) {
+      o.f("%3d: ", i + 1);
+      const Individual& d = r->ind[i];
+      if (label) o.f("%5s ", d.label.c_str());
+      if (popdata) o.f("%4d ", d.population);
+      if (popflag) o.f("%4d ", d.popflag);
+      if (phenotype) o.f("%4d ", d.phenotype);
+      if (precols > 1) o.f(" :");
+      for (int l = 0; l < shown; l++) o.f("%3d ", raw(i, line, l));
+      if (L > shown) o.f(" . . . . %3d\n", raw(i, line, L - 1));
+      else o.f("\n");
+    }
+    if (cut && i == 3) o.f("\n      *******   \n\n");
+  }
+  o.f("\n");
+  return give_text(o.s, buf, n);
 }

@@ -2,8 +2,9 @@
 // engine.  Reads mainparams / extraparams and the data file like the
 // reference program (src/structure.c:155-700, with the same -m -e -i -o -K
 // -L -N -D flags), runs BURNIN + NUMREPS sweeps of one chain on the GPU
-// through libstgpu (include/stgpu.h), prints progress every UPDATEFREQ
-// sweeps and writes OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
+// through libstgpu (include/stgpu.h), prints the reference's screen trace
+// every UPDATEFREQ sweeps (and the data echo with ECHODATA=1) and writes
+// OUTFILE_f (and OUTFILE_q with PRINTQHAT=1).
 //
 // USEPOPINFO=1 runs the migrant model for individuals with prior population
 // information and prints its posterior in OUTFILE_f (src/output.c:800-829);
@@ -59,6 +60,11 @@ int main(int argc, char** argv) {
   stf_param_str(r, "DATAFILE", datafile, sizeof datafile);
   printf("Reading file \"%s\".\n", datafile);
   if (stf_read_data(r) != STF_OK) return die("data", stf_last_error(r));
+  if (pi(r, "ECHODATA")) {
+    std::string echo((size_t)stf_echo_data(r, nullptr, 0) + 1, '\0');
+    stf_echo_data(r, &echo[0], echo.size());
+    fputs(echo.c_str(), stdout);
+  }
   int dims[4];
   stf_dims(r, dims);
   const int N = dims[0], L = dims[1], A = dims[3], K = pi(r, "MAXPOPS");
@@ -199,7 +205,42 @@ int main(int argc, char** argv) {
     if (savefreq * (pi(r, "INTERMEDSAVE") + 1) < m.numreps) savefreq++;
   }
   const bool printlikes = pi(r, "PRINTLIKES") != 0;
-  printf(" Rep#:   Alpha   %s Ln Like    Est Ln P(D)\n", m.freqscorr ? " F(mean)" : "");
+  // the screen trace of src/output.c:218-374 PrintUpdate after every
+  // UPDATEFREQ-th sweep and after the last one (src/structure.c:669-702),
+  // from the chain's current state
+  const size_t lp_n = m.locprior ? st_field_bytes(c, ST_F_LOCPRIOR) / 8 : 0;
+  std::vector<double> lambda(K), Qd, Pd, locp(lp_n > 0 ? lp_n : 1);
+  std::vector<float> Qf, Pf;
+  const bool trace_q = pi(r, "PRINTQSUM") && K > 1, trace_p = pi(r, "PRINTNET") || pi(r, "PRINTKLD");
+  std::string line;
+  auto print_update = [&](int rep) -> int {
+    alpha.assign(st_field_bytes(c, ST_F_ALPHA) / 8, 0.0);
+    st_get_state(c, ST_F_ALPHA, alpha.data(), alpha.size() * 8);
+    st_get_state(c, ST_F_F, F.data(), F.size() * 8);
+    st_get_state(c, ST_F_LAMBDA, lambda.data(), lambda.size() * 8);
+    if (lp_n > 0) st_get_state(c, ST_F_LOCPRIOR, locp.data(), lp_n * 8);
+    if (trace_q) {
+      Qf.resize(NK);
+      st_get_state(c, ST_F_Q, Qf.data(), NK * 4);
+      Qd.assign(Qf.begin(), Qf.end());
+    }
+    if (trace_p) {
+      Pf.resize(LKA);
+      st_get_state(c, ST_F_P, Pf.data(), LKA * 4);
+      Pd.assign(Pf.begin(), Pf.end());
+    }
+    const int len = stf_format_update(r, rep, trace_q ? Qd.data() : nullptr,
+                                      trace_p ? Pd.data() : nullptr, alpha.data(), F.data(),
+                                      lambda.data(), stats[0], locp.data(), nullptr, 0);
+    if (len < 0) return len;
+    line.assign((size_t)len + 1, '\0');
+    stf_format_update(r, rep, trace_q ? Qd.data() : nullptr, trace_p ? Pd.data() : nullptr,
+                      alpha.data(), F.data(), lambda.data(), stats[0], locp.data(), &line[0],
+                      line.size());
+    fputs(line.c_str(), stdout);
+    fflush(stdout);
+    return STF_OK;
+  };
   for (int done = 0; done < total;) {
     int next = std::min(total, (done / every + 1) * every);
     if (savefreq > 0 && savefreq <= m.numreps) {
@@ -220,22 +261,8 @@ int main(int argc, char** argv) {
       if (done <= m.burnin && st_calc_like(c, &like) != ST_OK) return die("GPU", st_last_error(ctx));
       printf("%6.0f\n", like);
     }
-    if (done % every == 0 || done == total) {
-      st_get_state(c, ST_F_ALPHA, alpha.data(), alpha.size() * 8);
-      st_get_state(c, ST_F_F, F.data(), F.size() * 8);
-      double fm = 0.0;
-      for (double v : F) fm += v / K;
-      printf("%5d:    %1.3f  ", done, alpha[0]);
-      if (m.freqscorr) printf("  %1.3f  ", fm);
-      if (done > m.burnin && m.computeprob) {
-        const double reps = done - m.burnin, mean = stats[1] / reps;
-        const double var = reps > 1 ? (stats[2] - stats[1] * stats[1] / reps) / (reps - 1) : 0.0;
-        printf("%9.0f  %9.0f", stats[0], mean - var / 2.0);
-      } else if (done == m.burnin) {
-        printf("\nBURNIN completed");
-      }
-      printf("\n");
-    }
+    if (done % every == 0 || done == total)
+      if (print_update(done) != STF_OK) return die("output", "screen trace");
     if (savefreq > 0 && done > m.burnin && (done - m.burnin) % savefreq == 0 && done != total)
       if (write_results(done, (done - m.burnin) / savefreq) != STF_OK)
         return die("output", stf_last_error(r));

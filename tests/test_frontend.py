@@ -52,6 +52,9 @@ def _front():
     L.stf_num_locations.argtypes = [vp]
     L.stf_set_locprior_sums.argtypes = [vp, vp, C.c_size_t]
     L.stf_set_usepopprobs.argtypes = [vp, vp]
+    L.stf_format_update.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp,
+                                    C.c_size_t]
+    L.stf_echo_data.argtypes = [vp, vp, C.c_size_t]
     L.stf_close.argtypes = [vp]
     return L
 
@@ -127,15 +130,36 @@ class Ours:
                                       float(z["sumlikes"]), float(z["sumsqlikes"]))
         assert rc == 0, self.L.stf_last_error(self.h)
 
+    def update(self, rep, a):
+        """stf_format_update of one trace line from the arrays of `a`."""
+        f = lambda x: np.ascontiguousarray(x, np.float64)
+        args = [f(a[k]) for k in ("Q", "P", "alpha", "F", "lambda")]
+        lp = f(a["locprior"])
+        call = lambda buf, n: self.L.stf_format_update(
+            self.h, rep, *[x.ctypes.data for x in args], float(a["like"]), lp.ctypes.data, buf, n)
+        n = call(None, 0)
+        assert n >= 0, n
+        buf = C.create_string_buffer(n + 1)
+        assert call(buf, n + 1) == n
+        return buf.value
+
+    def echo(self):
+        n = self.L.stf_echo_data(self.h, None, 0)
+        assert n >= 0
+        buf = C.create_string_buffer(n + 1)
+        self.L.stf_echo_data(self.h, buf, n + 1)
+        return buf.value
+
     def close(self):
         self.L.stf_close(self.h)
         os.chdir(self.cwd)
 
 
-def _ref(workdir, argv, read_data=False, sums=None, rep=0):
+def _ref(workdir, argv, read_data=False, sums=None, rep=0, trace=None):
     spec = os.path.join(workdir, "spec.json")
     with open(spec, "w") as f:
-        json.dump({"argv": argv, "read_data": read_data, "sums": sums, "rep": rep}, f)
+        json.dump({"argv": argv, "read_data": read_data, "sums": sums, "rep": rep,
+                   "trace": trace}, f)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "ref_front.py"), workdir,
                         spec], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -201,7 +225,12 @@ EXTRA_TMPL = """EXTRA PARAMS (written by the test)
 #define ANCESTDIST   {ancestdist}  // (B)
 #define NUMBOXES   {numboxes} // (int)
 #define ANCESTPINT 0.90 // (d)
-#define COMPUTEPROB 1     // (B)
+#define PRINTQSUM  {printqsum}  // (B)
+#define PRINTNET   {printnet}  // (B)
+#define PRINTLAMBDA {printlambda}  // (B)
+#define POPSPECIFICLAMBDA {popspecificlambda}  // (B)
+#define ECHODATA   {echodata}  // (B)
+#define COMPUTEPROB {computeprob}     // (B)
 #define METROFREQ    10   // (int)
 #define RANDOMIZE      0  // (B)
 #define SEED        {seed}  // (int)
@@ -216,7 +245,8 @@ def _scenario(d, **kw):
              mapdist=0, freqscorr=1, onefst=0, popalphas=0, updatefreq=0, printqhat=0,
              ancestdist=0, numboxes=100, seed=4242, noadmix=0, usepopinfo=0, migrprior=0.05,
              gensback=2, locdata=0, locprior=0, locispop=0, admburnin=50, intermedsave=0,
-             printlikes=0)
+             printlikes=0, printqsum=0, printnet=0, printlambda=0, popspecificlambda=0,
+             echodata=0, computeprob=1)
     p.update(kw)
     with open(os.path.join(d, "mainparams"), "w") as f:
         f.write(MAIN_TMPL.format(**p))
@@ -400,3 +430,69 @@ def test_front_end_reports_errors(tmp_path):
     assert ours.rc == 0
     assert ours.L.stf_read_data(ours.h) == -3
     ours.close()
+
+
+TRACES = [dict(), dict(printqsum=1, printnet=1, K=4), dict(freqscorr=0, popalphas=1, K=12),
+          dict(onefst=1, printlambda=1, popspecificlambda=1, printqsum=1, popdata=0),
+          dict(noadmix=1, admburnin=70, popalphas=1), dict(noadmix=1, admburnin=30),
+          dict(locprior=1, locdata=1, printlambda=1), dict(computeprob=0, burnin=150),
+          dict(usepopinfo=1, K=4), dict(burnin=130000, numreps=2000)]
+
+
+@needs_ref
+@pytest.mark.parametrize("opts", TRACES, ids=["default", "qsum-net", "popalphas-k12",
+                                               "onefst-lambda", "noadmix-admburnin",
+                                               "noadmix-early", "locprior", "noprob",
+                                               "usepop-noalpha", "six-digit-reps"])
+def test_screen_trace_matches_reference(tmp_path, opts):
+    """The screen trace of a run (src/output.c:218-454 PrintUpdate and
+    PrintBanner), line for line at the sweeps where the run loop prints it
+    (src/structure.c:669-702), from the same alpha, F, lambda, r, like, Q and
+    P: identical text."""
+    d = str(tmp_path)
+    p = _scenario(d, updatefreq=10, **opts)
+    argv = ["structure", "-K", str(p["K"])]
+    ours = Ours(d, argv)
+    o = ours.data()
+    ours.check_pop_priors()
+    K, A, N, L = p["K"], o["A"], p["N"], p["L"]
+    total = p["burnin"] + p["numreps"]
+    every = ours.int("UPDATEFREQ")
+    reps = list(range(every, total + 1, every))
+    if p["burnin"] > 1000:       # a few sweeps on each side of the banners
+        reps = [r for r in reps if r < 60 or abs(r - p["burnin"]) <= 30 or r > total - 120]
+    if total % every:
+        reps.append(total)
+    rng = np.random.default_rng(5)
+    U = len(reps)
+    z = dict(rep=np.array(reps), like=-rng.random(U) * 5000.0 - 1000.5,
+             alpha=rng.random((U, K)) * 3.0, F=rng.random((U, K)) * 0.5,
+             **{"lambda": rng.random((U, K)) * 2.0}, locprior=rng.random((U, 1)) * 4.0,
+             Q=rng.dirichlet(np.ones(K), (U, N)), P=rng.dirichlet(np.ones(A), (U, L, K)))
+    np.savez(os.path.join(d, "trace.npz"), **z)
+    mine = b"".join(ours.update(int(r), {k: z[k][u] for k in z}) for u, r in enumerate(reps))
+    ours.close()
+    out = _ref(d, argv, read_data=True, trace="trace.npz")
+    theirs = open(os.path.join(d, "ref_stdout.txt"), "rb").read()
+    theirs = theirs[out["trace_at"]:out["trace_end"]]
+    assert mine == theirs
+
+
+@needs_ref
+@pytest.mark.parametrize("layout", [dict(), dict(N=5, L=4, popflag=1), dict(label=0, popdata=0),
+                                    dict(missing=0, onerow=1, N=7)],
+                         ids=["default", "few", "bare", "onerow-missing0"])
+def test_echo_data_matches_reference(tmp_path, layout):
+    """ECHODATA=1: the data echo of src/datain.c:514-571 PrintSomeData."""
+    d = str(tmp_path)
+    p = _scenario(d, echodata=1, **layout)
+    argv = ["structure"]
+    ours = Ours(d, argv)
+    ours.data()
+    mine = ours.echo()
+    ours.close()
+    out = _ref(d, argv, read_data=True)
+    theirs = open(os.path.join(d, "ref_stdout.txt"), "rb").read()[out["read_at"]:out["read_end"]]
+    head = b'Reading file "%s".\n' % p["infile"].encode()
+    assert theirs.startswith(head)
+    assert mine == theirs[len(head):]

@@ -40,13 +40,24 @@ def test_cli_run_writes_results(tmp_path, kind):
     if kind == "intermedsave":
         return _intermedsave_run(d)
     if kind == "microsat":
-        p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200)
+        p = _scenario(d, N=60, L=30, burnin=200, numreps=600, updatefreq=200, echodata=1,
+                      printnet=1)
     else:
         p = _scenario(d, N=80, L=300, burnin=200, numreps=600, updatefreq=200, markernames=0)
         _snp_data(d, p)
     r = subprocess.run([CLI, "-D", "99"], cwd=d, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "Final results printed to file results_f" in r.stdout
+    # the screen trace: a line after every UPDATEFREQ-th sweep, Ln Like once
+    # collecting (the line format itself is pinned in tests/test_frontend.py)
+    lines = re.findall(r"^\s*(\d+):    (.*)$", r.stdout, re.M)
+    assert [int(x) for x, _ in lines] == [200, 400, 600, 800]
+    assert "BURNIN completed" in r.stdout and " Rep#:   " in r.stdout
+    like = [float(t.split()[-2]) for x, t in lines if int(x) > 202]
+    assert len(like) == 3 and all(np.isfinite(v) and v < 0 for v in like)
+    if kind == "microsat":
+        assert 'Data file "data file.str" (truncated) --' in r.stdout
+        assert lines[0][1].count(".") == 1 + 3 + 3    # alpha, F1..F3, D1,2 D1,3 D2,3
     text = open(os.path.join(d, "results_f")).read()
     for section in ("Run parameters:", "Proportion of membership", "Net nucleotide distance",
                     "Estimated Ln Prob of Data", "Inferred ancestry of individuals:",
