@@ -22,6 +22,8 @@
 // kernels sum the partials in a fixed order and apply the softmax Jacobian.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstdint>
 
 #include "st_device.cuh"
@@ -469,19 +471,38 @@ int grad_kclass(int K) {
   return K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : 16;
 }
 
-// Chunking: enough CTAs in both passes for ~4 per SM, partials kept small.
+// Chunks per pass: the smallest count c (1..cmax) whose grid takes at most
+// 5 % more waves per unit of work, ceil(tiles * c / wave) / c, than perfect
+// packing (tiles / wave), else the count with the fewest.  A grid just above
+// a whole number of waves (600 CTAs on 592 slots) would run a nearly empty
+// last wave as long as a full one; few chunks keep the partials small.
+int wave_chunks(int tiles, int wave, int cmax) {
+  const double ideal = (double)tiles / wave;
+  int best = 1;
+  double best_t = 1e300;
+  for (int c = 1; c <= cmax; c++) {
+    const double t = (double)((tiles * (long long)c + wave - 1) / wave) / c;
+    if (t <= 1.05 * ideal) return c;
+    if (t < best_t) {
+      best_t = t;
+      best = c;
+    }
+  }
+  return best;
+}
+
+// Chunking: each pass's grid sized against one wave of 4 CTAs per SM on 148
+// SMs (64 registers x 256 threads per CTA), chunks of at least 64 loci or
+// individuals so the partials stay small.
 void grad_plan(int N, int L, GradArgs* a) {
   const int tiles_i = (N + kGradBlock - 1) / kGradBlock;
   const int tiles_l = (L + kGradBlock - 1) / kGradBlock;
-  const int target = 148 * 4;
-  int lch = (target + tiles_i - 1) / tiles_i;
-  lch = lch < 1 ? 1 : lch;
-  int llen = (L + lch - 1) / lch;
-  if (llen < 64) llen = 64;
+  const int wave = 148 * 4;
+  const int lch = wave_chunks(tiles_i, wave, std::max(1, std::min(64, L / 64)));
+  const int llen = std::max(64, (L + lch - 1) / lch);
   a->lchunk_len = llen;
   a->lchunks = (L + llen - 1) / llen;
-  int ich = (target + tiles_l - 1) / tiles_l;
-  ich = ich < 1 ? 1 : ich;
+  const int ich = wave_chunks(tiles_l, wave, std::max(1, std::min(64, N / 64)));
   int ilen = (N + ich - 1) / ich;
   ilen = ((ilen + 15) / 16) * 16;
   if (ilen < 64) ilen = 64;
