@@ -822,7 +822,7 @@ def measure_config5(steps, warmup, with_cpu=True):
     ctx.set_stream(stream.cuda_stream)
     data = api.Data(ctx, d["numalleles"], packed=d["packed"], num_inds=N, num_loci=L,
                     layout=api.LAYOUT_B2G)
-    mk = dict(maxpops=K, burnin=warmup, numreps=steps + 20, freqscorr=1, inferalpha=1,
+    mk = dict(maxpops=K, burnin=warmup, numreps=steps + 40, freqscorr=1, inferalpha=1,
               popalphas=1, alpha=1.0, metrofreq=10, fpriormean=0.01, fpriorsd=0.05,
               computeprob=1)
     chains = [api.Chain(ctx, data, api.model_defaults(**mk), 5000 + r) for r in range(B)]
@@ -841,13 +841,25 @@ def measure_config5(steps, warmup, with_cpu=True):
     torch.cuda.synchronize()
     prof = ctx.profile_read()
     ctx.profile(False)
+    # plain: each chain alone, replaying its own graphs (captured by untimed
+    # sweeps first), ten sweeps each with one Metropolis sweep among them
+    singles = [api.Batch(ctx, [c]) for c in chains]
+    for sb in singles:
+        sb.sweep(10)
+    pms = _timed(stream, lambda: [sb.sweep(10) for sb in singles])
+    for sb in singles:
+        sb.close()
     for c in chains:
         assert c.sync() == 0
     copies = _observed_copies(d["packed"], N)
     value = B * steps / (ms / 1e3)
+    plain = B * 10 / (pms / 1e3)
     out = {"workload": "config 5: N=10000 L=500000 K=10 F model, POPALPHAS=1, 8 chains batched",
            "value": round(value, 3), "unit": METRIC, "steps": steps, "warmup": warmup,
            "ms_per_step": round(ms / steps, 3), "z_updates_per_s": round(value * copies, 1),
+           "plain": {"value": round(plain, 3), "unit": METRIC,
+                     "path": "each chain alone, replaying its own CUDA graphs"},
+           "batched_over_plain": round(value / plain, 3),
            "hbm_in_use_gb": round(used / 1e9, 2), "hbm_budget_gb": round(budget / 1e9, 2),
            "gpu_launches": int(launches),
            "kernel_share": _kernel_share(prof),
@@ -910,7 +922,7 @@ def other_configs(with_cpu):
     for key, fn in (("config1", lambda: measure_config1(with_cpu)),
                     ("config3", lambda: measure_config3(20, 3, with_cpu)),
                     ("config4", lambda: measure_config4(10, 3, with_cpu)),
-                    ("config5", lambda: measure_config5(5, 3, with_cpu))):
+                    ("config5", lambda: measure_config5(10, 3, with_cpu))):
         try:
             out[key] = fn()
         except Exception as e:  # reported in the line, never hides the headline
