@@ -39,6 +39,8 @@ __device__ __forceinline__ void warp_slot_sums(double v, int G, double* s, int n
 // lane busy whatever K is).  The per-population constants of the sweep --
 // (1-F_k)/F_k and the F proposals -- are formed once per CTA in shared memory.
 // ---------------------------------------------------------------------------
+constexpr int kStageKA = 16;   // populations x alleles staged per locus (P stage)
+
 __global__ void __launch_bounds__(256, 3)
 locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
              int stages) {
@@ -46,6 +48,10 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
   __shared__ double sTot[kMaxPops];
   __shared__ double sFrac[kMaxPops];   // (1 - F_k) / F_k
   __shared__ double sNF[kMaxPops];     // proposed F_j (F stage)
+  // P stage, one lane per locus and K * A <= kStageKA: the CTA's new P and
+  // log P, written to HBM (and added into PSum) row-contiguously afterwards
+  __shared__ float sPst[256 * kStageKA];
+  __shared__ float sLPst[256 * kStageKA];
   const int c = find_chain(prefix, nchains, blockIdx.x);
   ChainDev& ch = chains[c];
   const int tile = blockIdx.x - prefix[c];
@@ -128,6 +134,8 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
       }
     }
   }
+  // CTA-uniform (one chain per CTA): stage this CTA's P rows in shared memory
+  const bool pstage = (stages & kLocP) && tpl == 1 && K * A <= kStageKA && blockDim.x <= 256;
   if ((stages & kLocP) && tpl == 1 && lvalid && na > 0) {
     for (int k = 0; k < K; k++) {
       const size_t base = ((size_t)l * K + k) * A;
@@ -149,9 +157,14 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
           p = exp(lp);
         }
         const float pf = (float)p;
-        ch.P[base + a] = pf;
-        ch.logP[base + a] = (float)lp;
-        if (collect) ch.PSum[base + a] += (double)pf;
+        if (pstage) {
+          sPst[threadIdx.x * (K * A) + k * A + a] = pf;
+          sLPst[threadIdx.x * (K * A) + k * A + a] = (float)lp;
+        } else {
+          ch.P[base + a] = pf;
+          ch.logP[base + a] = (float)lp;
+          if (collect) ch.PSum[base + a] += (double)pf;
+        }
         if (!(pf == pf)) errb |= kErrNaN;
       };
       if (na <= 2) {
@@ -180,6 +193,27 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         for (int a = 0; a < nac; a++) emit(a, lg[a], ls, nac);
       }
     }
+  }
+
+  if (pstage) {
+    // rows l0 .. l0 + nl - 1 of P, log P and PSum are contiguous: [l][k][a]
+    __syncthreads();
+    const int KA = K * A;
+    const int l0 = tile * (int)blockDim.x;
+    const int nl = min((int)blockDim.x, L - l0);
+    const size_t g0 = (size_t)l0 * KA;
+    for (int idx = threadIdx.x; idx < nl * KA; idx += blockDim.x) {
+      const int li = idx / KA;
+      const int a = (idx - li * KA) % A;
+      const int nal = ch.numalleles[l0 + li];
+      if (a < (nal < kMaxAlleles ? nal : kMaxAlleles)) {
+        const float pf = sPst[idx];
+        ch.P[g0 + idx] = pf;
+        ch.logP[g0 + idx] = sLPst[idx];
+        if (collect) ch.PSum[g0 + idx] += (double)pf;
+      }
+    }
+    __syncthreads();   // the eps stage reads this CTA's log P rows
   }
 
   // ---- eps ----------------------------------------------------------------
