@@ -90,7 +90,8 @@ struct st_batch {
   std::vector<st_chain*> chains;   // sorted by K class
   ChainDev* d_table = nullptr;
   int* d_pz = nullptr;     // prefix: Z pass (restarting at 0 in every group)
-  int* d_pl = nullptr;     // prefix: locus kernel
+  int* d_pl = nullptr;     // prefix: locus kernel (over d_table_l)
+  ChainDev* d_table_l = nullptr;   // the table in the locus kernel's CTA order
   int* d_pi = nullptr;     // prefix: individual kernel
   int tz = 0, tl = 0, ti = 0;
   std::vector<ZGroup> zg;  // fast path: one Z launch per K class
@@ -101,6 +102,7 @@ struct st_batch {
   int glaunches[2] = {0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<ChainDev> table;             // host copies of the device tables
+  std::vector<ChainDev> table_l;
   std::vector<int> pz, pl, pi;
   std::vector<cudaStream_t> aux;           // one per K class (several classes only)
   cudaEvent_t ev_fork = nullptr;
@@ -829,7 +831,7 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     h.key = (uint32_t)z;
   }
   h.g2 = data->g2; h.g8 = data->g8; h.numalleles = data->numalleles; h.popflags = data->popflags;
-  h.loc_tpl = locus_lanes(L);
+  h.loc_tpl = locus_lanes(L, K, A);
 
   c->fast = data->layout == kLayoutB2G && model->precision == 0 && fast_kt(K) > 0;
   if (data->layout == kLayoutB2G && !c->fast) {
@@ -1601,10 +1603,31 @@ static int batch_layout(st_batch* b, bool keep_groups) {
       b->pz[j] = b->tz;
       b->tz += ctas_zpass_u8(b->table[j], 256);
     }
-    b->pl[j] = b->tl;
     b->pi[j] = b->ti;
-    b->tl += ctas_locus(b->table[j], kBlockLoc);
     b->ti += ctas_ind(b->table[j], kBlockInd);
+  }
+  // locus kernel: chains whose CTAs take longest first (longest-processing-
+  // time order), so a batch of uneven K does not end on a tail of its slowest
+  // chain's CTAs; a CTA's time is about its lanes' serial gamma draws
+  std::vector<int> order(n);
+  for (int j = 0; j < n; j++) order[j] = j;
+  auto lane_draws = [&](int j) {
+    const ChainDev& h = b->table[j];
+    const int tpl = h.loc_tpl;
+    if (tpl <= 1) return (long)h.K * h.A;
+    int J = 1;
+    while (J * 2 * h.K <= tpl && J * 2 <= 32) J *= 2;
+    const int kslots = tpl / J;
+    return (long)((h.K + kslots - 1) / kslots) * ((h.A + J - 1) / J);
+  };
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return lane_draws(x) > lane_draws(y); });
+  b->table_l.resize(n);
+  for (int q = 0; q < n; q++) {
+    const int j = order[q];
+    b->table_l[q] = b->table[j];
+    b->pl[q] = b->tl;
+    b->tl += ctas_locus(b->table[j], kBlockLoc);
   }
   return ST_OK;
 }
@@ -1614,6 +1637,7 @@ static void batch_upload(st_batch* b) {
   cudaMemcpy(b->d_table, b->table.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice);
   cudaMemcpy(b->d_pz, b->pz.data(), 4 * n, cudaMemcpyHostToDevice);
   cudaMemcpy(b->d_pl, b->pl.data(), 4 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_table_l, b->table_l.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice);
   cudaMemcpy(b->d_pi, b->pi.data(), 4 * n, cudaMemcpyHostToDevice);
 }
 
@@ -1716,7 +1740,8 @@ extern "C" int st_batch_create(st_ctx* ctx, st_chain** chains, int n, st_batch**
     return e == cudaSuccess ? ST_OK : seterr(ctx, ST_ERR_NOMEM, "batch table");
   };
   if (alloc((void**)&b->d_table, sizeof(ChainDev) * n) || alloc((void**)&b->d_pz, 4 * n) ||
-      alloc((void**)&b->d_pl, 4 * n) || alloc((void**)&b->d_pi, 4 * n)) {
+      alloc((void**)&b->d_pl, 4 * n) || alloc((void**)&b->d_pi, 4 * n) ||
+      alloc((void**)&b->d_table_l, sizeof(ChainDev) * n)) {
     st_batch_destroy(b);
     return ST_ERR_NOMEM;
   }
@@ -1850,7 +1875,8 @@ extern "C" int st_batch_autotune(st_batch* b, int reps) {
 extern "C" int st_batch_destroy(st_batch* b) {
   if (!b) return ST_ERR_ARG;
   cudaSetDevice(b->ctx->device);
-  for (void* p : {(void*)b->d_table, (void*)b->d_pz, (void*)b->d_pl, (void*)b->d_pi})
+  for (void* p : {(void*)b->d_table, (void*)b->d_pz, (void*)b->d_pl, (void*)b->d_pi,
+                  (void*)b->d_table_l})
     if (p) cudaFree(p);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -1894,7 +1920,7 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
     ctx->launches += (int64_t)b->zg.size() - 1;   // the bracket counted one
     return ST_OK;
   };
-  LaunchSet ll{b->d_table, b->d_pl, n, b->tl, s};
+  LaunchSet ll{b->d_table_l, b->d_pl, n, b->tl, s};
   LaunchSet li{b->d_table, b->d_pi, n, b->ti, s};
   const int zflags = (c0->h.computeprob ? kZfLikeIfCollect : 0) | kZfCollect | kZfAdvance |
                      (c0->model.store_z ? kZfStoreZ : 0);

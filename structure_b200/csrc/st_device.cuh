@@ -67,6 +67,20 @@ __device__ __forceinline__ float neg_one_plus_u23(uint32_t w) {
   return __uint_as_float(0xBF800000u | (w & 0x7FFFFFu));
 }
 
+// Neumaier's compensated summation (the Kahan-Babuska form, which also holds
+// when a term outweighs the running sum): s + c carries the sum of the terms
+// added so far to about twice the working precision.  Additions only, so
+// contraction flags do not change it.
+struct CompSum {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return s + c; }
+};
+
 constexpr double kTwoPi = 6.283185307179586;
 
 // Standard normal for MH proposals: Box-Muller on block {idx, 0, rep, stream}.

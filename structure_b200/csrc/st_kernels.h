@@ -72,7 +72,7 @@ cudaError_t launch_clear_counts(const ChainDev* d_table, int nchains, cudaStream
 int ctas_zpass_b2g(const ChainDev& c);
 int ctas_zpass_u8(const ChainDev& c, int block);
 int ctas_locus(const ChainDev& c, int block);
-int locus_lanes(int L);
+int locus_lanes(int L, int K, int A);
 int ctas_ind(const ChainDev& c, int block);
 int ctas_collect(const ChainDev& c, int block);
 int ctas_lambda(const ChainDev& c, int block);

@@ -329,11 +329,16 @@ int ctas_locus(const ChainDev& c, int block) { return (c.L * c.loc_tpl + block -
 
 // Lanes per locus of the locus kernel: 1 for most chains; with fewer loci
 // than about two waves of threads, up to 32 per locus (a power of two), so a
-// small chain's Dirichlet draws run in parallel over populations and alleles.
-int locus_lanes(int L) {
+// small chain's Dirichlet draws run in parallel over populations and alleles,
+// but no more lanes than there are (population, allele) draws to spread:
+// the lanes of a locus cover populations x alleles in powers of two.
+int locus_lanes(int L, int K, int A) {
   int t = 1;
   while (t < 32 && (size_t)L * t * 2 <= (size_t)148 * 256 * 2) t *= 2;
-  return t;
+  int kp = 1, ap = 1;
+  while (kp < K) kp *= 2;
+  while (ap < A) ap *= 2;
+  return t < kp * ap ? t : kp * ap;
 }
 
 cudaError_t launch_locus(const LaunchSet& ls, int stages, int block) {

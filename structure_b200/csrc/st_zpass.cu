@@ -42,12 +42,13 @@ __device__ __forceinline__ double block_sum_d(double v, double* sred) {
   return s;  // valid in thread 0
 }
 
-// Last CTA of a chain: sum the per-CTA ln-likelihood partials in order and
-// fold them into the chain's stats.
+// Last CTA of a chain: sum the per-CTA ln-likelihood partials in a fixed
+// order (each thread a compensated sum of a strided subset, then the block's
+// tree) and fold them into the chain's stats.
 static __device__ void finish_like(ChainDev& ch, int ntiles, bool collect, double* sred) {
-  double v = 0.0;
-  for (int j = threadIdx.x; j < ntiles; j += blockDim.x) v += ch.likepart[j];
-  double s = block_sum_d(v, sred);
+  CompSum v;
+  for (int j = threadIdx.x; j < ntiles; j += blockDim.x) v.add(ch.likepart[j]);
+  double s = block_sum_d(v.value(), sred);
   if (threadIdx.x == 0) {
     ch.stats[kStLike] = s;
     if (collect) {
