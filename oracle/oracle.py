@@ -66,6 +66,11 @@ class Oracle:
         lib.orc_lgamma.restype = _cd
         lib.orc_loggamma.argtypes = [_cd, _cu32, _cu32, _cu32, _cu64, C.POINTER(_ci)]
         lib.orc_loggamma.restype = _cd
+        lib.orc_loggamma_f32.argtypes = [C.c_float, _cu32, _cu32, _cu32, _cu64, C.POINTER(_ci)]
+        lib.orc_loggamma_f32.restype = C.c_float
+        lib.orc_ln_f32.argtypes = [C.c_float]
+        lib.orc_ln_f32.restype = C.c_float
+        lib.orc_sincos_2pi_f32.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         lib.orc_normal.argtypes = [_cu32, _cu32, _cu32, _cu64]
         lib.orc_normal.restype = _cd
         lib.orc_init_z.argtypes = [_ci, _ci, _ci, _i32p, _cu64, _i32p]
@@ -128,6 +133,20 @@ class Oracle:
         err = _ci(0)
         v = self.lib.orc_loggamma(a, e, rep, stream, key, C.byref(err))
         return v, err.value
+
+    def loggamma_f32(self, a, e, rep, stream, key):
+        """The FP32 draw the P update uses (ln of a Gamma(a, 1) variate)."""
+        err = _ci(0)
+        v = self.lib.orc_loggamma_f32(a, e, rep, stream, key, C.byref(err))
+        return v, err.value
+
+    def ln_f32(self, x):
+        return self.lib.orc_ln_f32(x)
+
+    def sincos_2pi_f32(self, u):
+        sn, cs = C.c_float(), C.c_float()
+        self.lib.orc_sincos_2pi_f32(u, C.byref(sn), C.byref(cs))
+        return sn.value, cs.value
 
     def normal(self, idx, rep, stream, key):
         return self.lib.orc_normal(idx, rep, stream, key)

@@ -167,6 +167,133 @@ double orc_loggamma(double a, uint32_t e, uint32_t rep, uint32_t stream,
     return lg;
 }
 
+/* ------------------------------------------------------------------------ */
+/* FP32 gamma draw for the Dirichlet of P: the device's log_gamma_draw_f32,  */
+/* operation for operation (IEEE float add, multiply, fmaf, divide, sqrtf;  */
+/* no contraction), so both give the same bits.  ln and sin/cos are series: */
+/* ln m = 2 atanh((m-1)/(m+1)) for m in [sqrt(1/2), sqrt(2)) plus e ln 2 in  */
+/* a Cody-Waite head and tail; sin and cos of theta in [-pi/4, pi/4] by      */
+/* Taylor series to theta^9 / theta^10 after the quadrant reduction of 4u.  */
+/* Marsaglia & Tsang (2000) with v - 1 = y (3 + y (3 + y)), y = c x, and     */
+/* 1 - v + ln v = ln(1 + w) - w summed as a series when |w| < 1/8.          */
+/* ------------------------------------------------------------------------ */
+static float u23c_f32(uint32_t w)
+{
+    return (float)(((w >> 9) << 1) | 1u) * 5.9604644775390625e-8f;
+}
+
+static float ln_f32(float x)
+{
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    int e = (int)((b >> 23) & 0xFFu) - 127;
+    uint32_t mb = (b & 0x7FFFFFu) | 0x3F800000u;
+    float m;
+    memcpy(&m, &mb, 4);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    float sv = (m - 1.0f) / (m + 1.0f);
+    float z = sv * sv;
+    float q = fmaf(z, 1.0f / 11.0f, 1.0f / 9.0f);
+    q = fmaf(z, q, 1.0f / 7.0f);
+    q = fmaf(z, q, 1.0f / 5.0f);
+    q = fmaf(z, q, 1.0f / 3.0f);
+    float t = 2.0f * sv;
+    float lm = fmaf(t * z, q, t);
+    float fe = (float)e;
+    return fe * 0.693145751953125f + fmaf(fe, 1.42860682e-6f, lm);
+}
+
+static void sincos_2pi_f32(float u, float *sn, float *cs)
+{
+    float q = u * 4.0f;
+    int n = (int)(q + 0.5f);
+    float r = q - (float)n;
+    float th = r * 1.57079637f;
+    float t2 = th * th;
+    float ps = fmaf(t2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+    ps = fmaf(t2, ps, 1.0f / 120.0f);
+    ps = fmaf(t2, ps, -1.0f / 6.0f);
+    float sv = fmaf(th * t2, ps, th);
+    float pc = fmaf(t2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+    pc = fmaf(t2, pc, -1.0f / 720.0f);
+    pc = fmaf(t2, pc, 1.0f / 24.0f);
+    pc = fmaf(t2, pc, -0.5f);
+    float cv = fmaf(t2, pc, 1.0f);
+    switch (n & 3) {
+    case 0: *sn = sv; *cs = cv; break;
+    case 1: *sn = cv; *cs = -sv; break;
+    case 2: *sn = -sv; *cs = -cv; break;
+    default: *sn = -cv; *cs = sv; break;
+    }
+}
+
+float orc_loggamma_f32(float a, uint32_t e, uint32_t rep, uint32_t stream, uint64_t key,
+                       int *err)
+{
+    float aa = a < 1.0f ? a + 1.0f : a;
+    float d = aa - 1.0f / 3.0f;
+    float c = 1.0f / sqrtf(9.0f * d);
+    float lg = 0.0f;
+    int done = 0;
+    for (uint32_t j = 0; j < GAMMA_MAX_BLOCKS && !done; j++) {
+        uint32_t b[4];
+        philox4(e, j, rep, stream, key, b);
+        float sn, cs;
+        sincos_2pi_f32(u23c_f32(b[1]), &sn, &cs);
+        float rad = sqrtf(-2.0f * ln_f32(u23c_f32(b[0])));
+        float xs[2] = {rad * cs, rad * sn};
+        float us[2] = {u23c_f32(b[2]), u23c_f32(b[3])};
+        for (int h = 0; h < 2 && !done; h++) {
+            float x = xs[h];
+            float y = c * x;
+            if (!(1.0f + y > 0.0f)) continue;
+            float w = y * fmaf(y, 3.0f + y, 3.0f);
+            float v = 1.0f + w;
+            if (!(v > 1e-30f)) continue;
+            float x2 = x * x;
+            float u = us[h];
+            int acc = u < 1.0f - (0.0331f * x2) * x2;
+            if (!acc) {
+                float g;
+                if (fabsf(w) < 0.125f) {
+                    float p = fmaf(w, 1.0f / 9.0f, -0.125f);
+                    p = fmaf(w, p, 1.0f / 7.0f);
+                    p = fmaf(w, p, -1.0f / 6.0f);
+                    p = fmaf(w, p, 0.2f);
+                    p = fmaf(w, p, -0.25f);
+                    p = fmaf(w, p, 1.0f / 3.0f);
+                    p = fmaf(w, p, -0.5f);
+                    g = (w * w) * p;
+                } else {
+                    g = ln_f32(v) - w;
+                }
+                acc = ln_f32(u) < fmaf(d, g, 0.5f * x2);
+            }
+            if (acc) {
+                lg = ln_f32(d * v);
+                done = 1;
+            }
+        }
+    }
+    if (!done) {
+        if (err) *err |= ERR_GAMMA_CAP;
+        lg = ln_f32(d);
+    }
+    if (a < 1.0f) {
+        uint32_t w[4];
+        philox4(e, 0xFFFFFFu, rep, stream, key, w);
+        lg = lg + ln_f32(u23c_f32(w[0])) / a;
+    }
+    return lg;
+}
+
+float orc_ln_f32(float x) { return ln_f32(x); }
+
+void orc_sincos_2pi_f32(float u, float *sn, float *cs) { sincos_2pi_f32(u, sn, cs); }
+
 /* Pairwise tree over G (power of two) slots, the order of a xor-butterfly. */
 static double tree_sum(double *v, int G)
 {
@@ -328,7 +455,8 @@ void orc_update_p(int L, int K, int A, const int32_t *numalleles, const int32_t 
                     shape = eps[(size_t)l * A + a] * (1.0 - F[k]) / F[k] + (double)n[base + a];
                 else
                     shape = lambda[k] + (double)n[base + a];
-                lg[a] = orc_loggamma(shape, (uint32_t)(base + a), rep, ORC_S_P, key, err);
+                lg[a] = (double)orc_loggamma_f32((float)shape, (uint32_t)(base + a), rep,
+                                                 ORC_S_P, key, err);
             }
             if (na > 0) dirichlet_seq(lg, na, 1, P + base, logP + base);
         }

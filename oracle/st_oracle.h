@@ -45,7 +45,12 @@ double orc_normal(uint32_t idx, uint32_t rep, uint32_t stream, uint64_t key);
 
 double orc_lgamma(double z);                   /* mymath.c:382 (Lanczos g=7, n=9) */
 double orc_loggamma(double a, uint32_t e, uint32_t rep, uint32_t stream,
-                    uint64_t key, int *err);   /* log of a Gamma(a,1) draw */
+                    uint64_t key, int *err);
+/* The FP32 draw of the Dirichlet of P, and its own ln and sin/cos of 2 pi u. */
+float orc_loggamma_f32(float a, uint32_t e, uint32_t rep, uint32_t stream, uint64_t key,
+                       int *err);
+float orc_ln_f32(float x);
+void orc_sincos_2pi_f32(float u, float *sn, float *cs);   /* log of a Gamma(a,1) draw */
 
 /* --- Z (Updates/UpdateZ.c:13-56, mymath.c:105-129) --------------------- */
 void orc_init_z(int N, int L, int K, const int32_t *geno, uint64_t key,

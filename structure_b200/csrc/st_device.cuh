@@ -177,6 +177,139 @@ static __device__ __noinline__ double log_gamma_draw(double a, uint32_t e, uint3
   return lg;
 }
 
+// ---------------------------------------------------------------------------
+// FP32 gamma draws for the Dirichlet of P.  Every operation below is an
+// IEEE-rounded add, multiply, fma, divide or square root written as an
+// explicit _rn intrinsic (never contracted, whatever -fmad says), so the
+// oracle's C restatement of the same sequence gives the same bits.  log and
+// sin/cos are this file's own: the atanh series of the logarithm and the
+// Taylor series of sine and cosine, after exact range reductions.
+// ---------------------------------------------------------------------------
+// Uniform in (0,1) from a word's top 23 bits k: (2k + 1) / 2^24, exact in
+// FP32 (the odd integer has at most 24 bits).
+__device__ __forceinline__ float u23c_f32(uint32_t w) {
+  return __fmul_rn((float)(((w >> 9) << 1) | 1u), 5.9604644775390625e-8f);
+}
+
+// ln x for a positive normal float: x = 2^e m with m in [sqrt(1/2), sqrt(2)),
+// s = (m - 1) / (m + 1) (m - 1 exact), ln m = 2 atanh s = 2s (1 + s^2/3 +
+// s^4/5 + ... + s^10/11) (|s| < 0.172, the next term below 2e-9 relative),
+// and e ln 2 split into a 15-bit head (e ln2_hi exact for |e| < 256) and a
+// tail (Cody and Waite's reduction).
+__device__ __forceinline__ float ln_f32(float x) {
+  const uint32_t b = __float_as_uint(x);
+  int e = (int)((b >> 23) & 0xFFu) - 127;
+  float m = __uint_as_float((b & 0x7FFFFFu) | 0x3F800000u);
+  if (m > 1.41421356f) {
+    m = __fmul_rn(m, 0.5f);
+    e += 1;
+  }
+  const float sv = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+  const float z = __fmul_rn(sv, sv);
+  float q = __fmaf_rn(z, 1.0f / 11.0f, 1.0f / 9.0f);
+  q = __fmaf_rn(z, q, 1.0f / 7.0f);
+  q = __fmaf_rn(z, q, 1.0f / 5.0f);
+  q = __fmaf_rn(z, q, 1.0f / 3.0f);
+  const float t = __fmul_rn(2.0f, sv);
+  const float lm = __fmaf_rn(__fmul_rn(t, z), q, t);
+  const float fe = (float)e;
+  return __fadd_rn(__fmul_rn(fe, 0.693145751953125f), __fmaf_rn(fe, 1.42860682e-6f, lm));
+}
+
+// sin and cos of 2 pi u for u in [0,1): q = 4u (exact), n = nearest integer,
+// r = q - n in [-1/2, 1/2] (exact), theta = r pi/2 in [-pi/4, pi/4], Taylor
+// series to theta^9 (sine) and theta^10 (cosine), then the quadrant n.
+__device__ __forceinline__ void sincos_2pi_f32(float u, float* sn, float* cs) {
+  const float q = __fmul_rn(u, 4.0f);
+  const int n = (int)__fadd_rn(q, 0.5f);
+  const float r = __fsub_rn(q, (float)n);
+  const float th = __fmul_rn(r, 1.57079637f);
+  const float t2 = __fmul_rn(th, th);
+  float ps = __fmaf_rn(t2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  ps = __fmaf_rn(t2, ps, 1.0f / 120.0f);
+  ps = __fmaf_rn(t2, ps, -1.0f / 6.0f);
+  const float sv = __fmaf_rn(__fmul_rn(th, t2), ps, th);
+  float pc = __fmaf_rn(t2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+  pc = __fmaf_rn(t2, pc, -1.0f / 720.0f);
+  pc = __fmaf_rn(t2, pc, 1.0f / 24.0f);
+  pc = __fmaf_rn(t2, pc, -0.5f);
+  const float cv = __fmaf_rn(t2, pc, 1.0f);
+  switch (n & 3) {
+    case 0: *sn = sv; *cs = cv; break;
+    case 1: *sn = cv; *cs = -sv; break;
+    case 2: *sn = -sv; *cs = -cv; break;
+    default: *sn = -cv; *cs = sv; break;
+  }
+}
+
+// ln of a Gamma(a, 1) draw in FP32 (Marsaglia and Tsang 2000).  Attempt pair
+// j takes Philox block j: words x, y give two Box-Muller normals, z and w the
+// two acceptance uniforms.  With y = c x, v - 1 = y (3 + y (3 + y)) is formed
+// without cancellation and 1 - v + ln v = ln(1 + w) - w by its series when
+// |w| < 1/8 (to w^9/9; the next term is below 3e-8 of the sum): at the
+// shapes of large counts the direct form would lose ~1e-4 of the test's
+// log density to cancellation.  Shape < 1: G(a) = G(a + 1) U^(1/a), U from
+// block 0xFFFFFF.
+static __device__ __noinline__ float log_gamma_draw_f32(float a, uint32_t e, uint32_t rep,
+                                                    uint32_t stream, uint32_t key,
+                                                    int* errbits) {
+  const float aa = a < 1.0f ? __fadd_rn(a, 1.0f) : a;
+  const float d = __fsub_rn(aa, 1.0f / 3.0f);
+  const float c = __fdiv_rn(1.0f, __fsqrt_rn(__fmul_rn(9.0f, d)));
+  float lg = 0.0f;
+  bool done = false;
+  for (uint32_t j = 0; j < kGammaMaxBlocks && !done; j++) {
+    const U4 b = philox_s(e, j, rep, stream, key);
+    float sn, cs;
+    sincos_2pi_f32(u23c_f32(b.y), &sn, &cs);
+    const float rad = __fsqrt_rn(__fmul_rn(-2.0f, ln_f32(u23c_f32(b.x))));
+    const float xs[2] = {__fmul_rn(rad, cs), __fmul_rn(rad, sn)};
+    const float us[2] = {u23c_f32(b.z), u23c_f32(b.w)};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (done) break;
+      const float x = xs[h];
+      const float y = __fmul_rn(c, x);
+      if (!(__fadd_rn(1.0f, y) > 0.0f)) continue;
+      const float w = __fmul_rn(y, __fmaf_rn(y, __fadd_rn(3.0f, y), 3.0f));
+      const float v = __fadd_rn(1.0f, w);
+      if (!(v > 1e-30f)) continue;
+      const float x2 = __fmul_rn(x, x);
+      const float u = us[h];
+      bool acc = u < __fsub_rn(1.0f, __fmul_rn(__fmul_rn(0.0331f, x2), x2));
+      if (!acc) {
+        float g;
+        if (fabsf(w) < 0.125f) {
+          float p = __fmaf_rn(w, 1.0f / 9.0f, -0.125f);
+          p = __fmaf_rn(w, p, 1.0f / 7.0f);
+          p = __fmaf_rn(w, p, -1.0f / 6.0f);
+          p = __fmaf_rn(w, p, 0.2f);
+          p = __fmaf_rn(w, p, -0.25f);
+          p = __fmaf_rn(w, p, 1.0f / 3.0f);
+          p = __fmaf_rn(w, p, -0.5f);
+          g = __fmul_rn(__fmul_rn(w, w), p);
+        } else {
+          g = __fsub_rn(ln_f32(v), w);
+        }
+        acc = ln_f32(u) < __fmaf_rn(d, g, __fmul_rn(0.5f, x2));
+      }
+      if (acc) {
+        lg = ln_f32(__fmul_rn(d, v));
+        done = true;
+      }
+    }
+  }
+  if (!done) {
+    *errbits |= kErrGammaCap;
+    lg = ln_f32(d);
+  }
+  if (a < 1.0f) {
+    const U4 w = philox_s(e, 0xFFFFFFu, rep, stream, key);
+    lg = __fadd_rn(lg, __fdiv_rn(ln_f32(u23c_f32(w.x)), a));
+  }
+  return lg;
+}
+
 // Butterfly over G lanes (G a power of two, width-G shuffles): every lane of
 // the group ends with the same pairwise-tree value.
 template <typename T>

@@ -102,7 +102,8 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
             n += ch.npart[(((size_t)cc * K + k) * A + a) * L + l];
           const double shape = ch.freqscorr ? ch.eps[(size_t)l * A + a] * sFrac[k] + (double)n
                                             : ch.lambda[k] + (double)n;
-          lg[nmine] = log_gamma_draw(shape, (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+          lg[nmine] = (double)log_gamma_draw_f32((float)shape, (uint32_t)(base + a),
+                                                 (uint32_t)rep, kSP, key, &errb);
           M = lg[nmine] > M ? lg[nmine] : M;
           nmine++;
         }
@@ -169,9 +170,11 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
       };
       if (na <= 2) {
         // biallelic (and monomorphic) loci stay in registers
-        const double lg0 = log_gamma_draw(shape_of(0), (uint32_t)base, (uint32_t)rep, kSP, key, &errb);
-        const double lg1 = na > 1 ? log_gamma_draw(shape_of(1), (uint32_t)(base + 1), (uint32_t)rep,
-                                                   kSP, key, &errb)
+        const double lg0 = (double)log_gamma_draw_f32((float)shape_of(0), (uint32_t)base,
+                                                      (uint32_t)rep, kSP, key, &errb);
+        const double lg1 = na > 1 ? (double)log_gamma_draw_f32((float)shape_of(1),
+                                                               (uint32_t)(base + 1),
+                                                               (uint32_t)rep, kSP, key, &errb)
                                   : -INFINITY;
         const double M = (na > 1 && lg1 > lg0) ? lg1 : lg0;
         double S = exp(lg0 - M);
@@ -184,7 +187,8 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
         const int nac = na < kMaxAlleles ? na : kMaxAlleles;
         if (na > kMaxAlleles) errb |= kErrBounds;
         for (int a = 0; a < nac; a++)
-          lg[a] = log_gamma_draw(shape_of(a), (uint32_t)(base + a), (uint32_t)rep, kSP, key, &errb);
+          lg[a] = (double)log_gamma_draw_f32((float)shape_of(a), (uint32_t)(base + a),
+                                             (uint32_t)rep, kSP, key, &errb);
         double M = lg[0];
         for (int a = 1; a < nac; a++) M = lg[a] > M ? lg[a] : M;
         double S = 0.0;

@@ -220,6 +220,14 @@ def test_updatep_matches_oracle(ctx, orc, freqscorr):
     Po, lPo, err = orc.update_p(na, n, freqscorr, eps, F, lam, SEED, 4)
     assert err == 0 and c.get(api.F_ERR) == 0
     np.testing.assert_allclose(Pd, Po, rtol=1e-5, atol=1e-30)
+    # the FP32 gamma draws are the same bits on both sides; only the FP64
+    # exp / log of the normalisation may differ in their last place, so the
+    # stored P agree to an ulp or two
+    live = np.arange(Pd.shape[2])[None, None, :] < na[:, None, None]
+    live = np.broadcast_to(live, Pd.shape)
+    ulps = np.abs(Pd.view(np.int32).astype(np.int64) - Po.view(np.int32).astype(np.int64))[live]
+    print("UpdateP: largest difference from the oracle in float ulps:", int(ulps.max()))
+    assert ulps.max() <= 2
     np.testing.assert_allclose(lPd, lPo, rtol=1e-5, atol=1e-5)
     for l in range(Pd.shape[0]):
         np.testing.assert_allclose(Pd[l, :, :na[l]].sum(1), 1.0, rtol=1e-5)

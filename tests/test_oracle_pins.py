@@ -8,6 +8,8 @@ normals and uniforms must make the same moves; the Dirichlet samplers differ in
 algorithm (reference: Ripley/Cheng-Feast gamma; build: Marsaglia-Tsang) and are
 compared in distribution.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -550,3 +552,39 @@ def test_q_updates_with_location_priors_match_reference(orc, ref):
     ref.rand_queue(None)
     np.testing.assert_array_equal(Qr.argmax(1), pick)
     assert (pick != pick0).any()
+
+
+def test_fp32_ln_and_sincos_series(orc):
+    """The FP32 logarithm and sine/cosine the P draws use (atanh and Taylor
+    series after exact range reductions) against libm in double: within
+    2 ulp (relative 2.4e-7) for ln away from 1, 1e-6 absolute near 1, and
+    1.2e-7 absolute for sin and cos of 2 pi u."""
+    xs = np.concatenate([np.geomspace(2.0 ** -24, 1.0, 4001), np.linspace(0.5, 2.0, 4001),
+                         np.geomspace(1.0, 1e6, 401)]).astype(np.float32)
+    for x in xs:
+        ref_v = math.log(float(x))
+        got = orc.ln_f32(float(x))
+        assert abs(got - ref_v) <= max(2.4e-7 * abs(ref_v), 1e-6), (x, got, ref_v)
+    for u in np.linspace(0.0, 1.0, 8001)[:-1].astype(np.float32):
+        sn, cs = orc.sincos_2pi_f32(float(u))
+        assert abs(sn - math.sin(2 * math.pi * float(u))) <= 1.2e-7
+        assert abs(cs - math.cos(2 * math.pi * float(u))) <= 1.2e-7
+
+
+@pytest.mark.parametrize("a", [0.05, 0.5, 1.0, 2.5, 10.0, 100.0, 4000.0])
+def test_fp32_gamma_draws_in_distribution(orc, a):
+    """The FP32 Marsaglia-Tsang draw of the P update against Gamma(a, 1):
+    Kolmogorov-Smirnov on the draws, and the mean and variance of their
+    logarithm (digamma and trigamma of a) with standard errors from the
+    sample's own fourth moment; from small shapes (the U^(1/a) boost) to the
+    counts of large samples (the series form of the acceptance test)."""
+    from scipy import special, stats
+    n = 20000
+    lg = np.array([orc.loggamma_f32(a, e, 3, 7, KEY + int(a * 1000))[0] for e in range(n)],
+                  np.float64)
+    assert stats.kstest(np.exp(lg), stats.gamma(a).cdf).pvalue > 1e-4
+    s2 = special.polygamma(1, a)
+    zm = (lg.mean() - special.digamma(a)) / math.sqrt(s2 / n)
+    d = lg - lg.mean()
+    zv = (lg.var() - s2) / math.sqrt((d ** 4).mean() / n - lg.var() ** 2 / n)
+    assert abs(zm) < 4.5 and abs(zv) < 4.5, (zm, zv)
