@@ -89,6 +89,10 @@ def test_config2_batch_sweeps_match_oracle(ctx, orc, ref, config2):
         assert err == 0
         P = c.get(api.F_P)
         np.testing.assert_allclose(P, Po, rtol=1e-5, atol=1e-30)
+        # the FP32 gamma draws (counts up to 2N = 4,000: the series form of the
+        # acceptance test) are the oracle's bits; P agrees to an ulp or two
+        ulps = np.abs(P.view(np.int32).astype(np.int64) - Po.view(np.int32).astype(np.int64))
+        assert ulps.max() <= 2, int(ulps.max())
         # the Metropolis step: log ratios of TestQ against the Q before the sweep
         T = c.get(api.F_TESTQ)
         ld_dev = c.get(api.F_LOGDIFF)
@@ -101,7 +105,8 @@ def test_config2_batch_sweeps_match_oracle(ctx, orc, ref, config2):
         report[j] = dict(lnpd_rel=rel, ld_abs_max=float(err_ld.max()),
                          ld_rel_max=float((err_ld / np.maximum(np.abs(ld_o), 1e-300)).max()),
                          ld_err_over_bound=float((err_ld / bound).max()), inband=inband,
-                         flips=flips, accepted=int((np.log(u) < ld_o).sum()))
+                         flips=flips, accepted=int((np.log(u) < ld_o).sum()),
+                         p_ulps_max=int(ulps.max()))
     # rep 11: a Gibbs sweep, Q drawn from the counts of rep 10
     before = {j: {f: chains[j].get(f) for f in (api.F_M, api.F_ALPHA)} for j in check}
     b.sweep(1)
