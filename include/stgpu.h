@@ -175,7 +175,10 @@ int st_model_defaults(st_model *m);
  * Creates device state and runs the reference's Initialization
  * (src/Init.c:329-444): alpha = ALPHA, lambda = LAMBDA, random Z
  * (InitializeZ, Init.c:125-169), epsilon/F (InitFreqPriors, Init.c:173-240),
- * Q = 1/K (src/structure.c:51-58), zeroed sums.                              */
+ * Q = 1/K (src/structure.c:51-58), zeroed sums.  The initialization is
+ * queued on the context's stream and the call returns without waiting for
+ * it; an error on the device surfaces at the next call that synchronizes
+ * (st_sync, st_get_state, ...).                                               */
 int st_chain_create(st_ctx *ctx, st_data *data, const st_model *model,
                     uint64_t seed, st_chain **out);
 int st_chain_destroy(st_chain *chain);

@@ -49,6 +49,11 @@ struct st_data {
   std::vector<int32_t> location_h;                 // empty: no location data
   std::vector<int64_t> cnt_h;    // [L][A] allele copies observed
   std::vector<int64_t> tot_h;    // [L] non-missing copies
+  // the initial eps of the data set's chains (src/Init.c:173-240) for one
+  // (FREQSCORR, LAMBDA), on the device: [L][A]
+  double* eps0 = nullptr;
+  int eps0_fc = -1;
+  double eps0_lambda = 0.0;
   size_t bytes = 0;
   int chains = 0;
 };
@@ -686,7 +691,8 @@ extern "C" int st_data_destroy(st_data* s) {
   if (s->chains > 0) return seterr(s->ctx, ST_ERR_STATE, "data still used by %d chains", s->chains);
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
-  for (void* p : {(void*)s->g2, (void*)s->g8, (void*)s->numalleles, (void*)s->popflags})
+  for (void* p : {(void*)s->g2, (void*)s->g8, (void*)s->numalleles, (void*)s->popflags,
+                  (void*)s->eps0})
     ctx_free(s->ctx, p);
   delete s;
   return ST_OK;
@@ -986,27 +992,27 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
 
   // ---- Initialization (src/Init.c:329-444, src/structure.c:51-58) ---------
   cudaStream_t s = ctx->stream;
-  std::vector<float> q(NK, (float)(1.0 / K)), lq(NK, (float)log(1.0 / K));
-  std::vector<double> kv(K);
-  std::vector<double> ev(LA, 0.0);
-  for (int l = 0; l < L; l++)
-    for (int a = 0; a < data->na_h[l]; a++) {
-      // src/Init.c:173-240 InitFreqPriors
-      ev[(size_t)l * A + a] = model->freqscorr
-          ? (((double)model->lambda + (double)data->cnt_h[(size_t)l * A + a]) /
-             ((double)data->na_h[l] * (double)model->lambda + (double)data->tot_h[l]))
-          : model->lambda;
-    }
-  cudaMemcpyAsync(h.Q, q.data(), NK * 4, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(h.logQ, lq.data(), NK * 4, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(h.eps, ev.data(), LA * 8, cudaMemcpyHostToDevice, s);
-  std::fill(kv.begin(), kv.end(), model->freqscorr ? model->fpriormean : 0.5);
-  cudaMemcpyAsync(h.F, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
-  // alpha = ALPHA, for every location row too (src/Init.c:350-368)
-  std::vector<double> av(arows * K, model->alpha);
-  cudaMemcpyAsync(h.alpha, av.data(), arows * K * 8, cudaMemcpyHostToDevice, s);
-  std::fill(kv.begin(), kv.end(), model->lambda);
-  cudaMemcpyAsync(h.lambda, kv.data(), K * 8, cudaMemcpyHostToDevice, s);
+  const int fc = model->freqscorr ? 1 : 0;
+  if (!data->eps0 || data->eps0_fc != fc || data->eps0_lambda != model->lambda) {
+    // src/Init.c:173-240 InitFreqPriors, once per data set and prior; a chain
+    // created earlier may still be reading the previous values
+    std::vector<double> ev(LA, 0.0);
+    for (int l = 0; l < L; l++)
+      for (int a = 0; a < data->na_h[l]; a++)
+        ev[(size_t)l * A + a] = fc
+            ? (((double)model->lambda + (double)data->cnt_h[(size_t)l * A + a]) /
+               ((double)data->na_h[l] * (double)model->lambda + (double)data->tot_h[l]))
+            : model->lambda;
+    rc = cuda_check(ctx, cudaStreamSynchronize(s), "chain init");
+    if (!rc && !data->eps0) rc = ctx_alloc(ctx, LA * 8, (void**)&data->eps0, nullptr, &data->bytes);
+    if (!rc)
+      rc = cuda_check(ctx, cudaMemcpyAsync(data->eps0, ev.data(), LA * 8, cudaMemcpyHostToDevice, s),
+                      "initial eps");
+    if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "initial eps");
+    if (rc) { st_chain_destroy(c); return rc; }
+    data->eps0_fc = fc;
+    data->eps0_lambda = model->lambda;
+  }
   cudaMemsetAsync(h.P, 0, LKA * 4, s);
   cudaMemsetAsync(h.logP, 0, LKA * 4, s);
   cudaMemsetAsync(h.TestQ, 0, NK * 4, s);
@@ -1048,11 +1054,15 @@ extern "C" int st_chain_create(st_ctx* ctx, st_data* data, const st_model* model
     cudaMemcpyAsync(pi_pop, pop1.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(pi_use, 0, (size_t)N * K * (h.gensback + 1) * 8, s);
   }
-  int zero = 0;
-  cudaMemcpyAsync(c->d_prefix, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
-  rc = upload_chain(c);
+  // descriptor, prefix, Q = 1/K, eps, F, alpha = ALPHA for every location row
+  // (src/Init.c:350-368), lambda: one kernel, no host copy to wait on
+  rc = cuda_check(ctx,
+                  launch_init_chain(h, c->d_chain, c->d_prefix, data->eps0, (int)arows,
+                                    (float)(1.0 / K), (float)log(1.0 / K),
+                                    fc ? model->fpriormean : 0.5, model->alpha, model->lambda, s),
+                  "chain init");
   if (!rc) rc = zpass(c, kZInit, model->store_z ? kZfStoreZ : 0);
-  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "chain init");
+  if (!rc) rc = cuda_check(ctx, cudaGetLastError(), "chain init");
   if (rc) { st_chain_destroy(c); return rc; }
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);

@@ -67,6 +67,9 @@ cudaError_t launch_inj_metro_accept(const ChainDev& h, ChainDev* d_chain, const 
                                     const int* taken, cudaStream_t s);
 cudaError_t launch_pack_u8(const int32_t* geno, uint8_t* g8, size_t n, cudaStream_t s);
 cudaError_t launch_clear_counts(const ChainDev* d_table, int nchains, cudaStream_t s);
+cudaError_t launch_init_chain(const ChainDev& h, ChainDev* d_chain, int* d_prefix,
+                              const double* eps0, int arows, float q0, float lq0, double f0,
+                              double alpha0, double lambda0, cudaStream_t s);
 
 // CTA counts per chain for each launch kind (host-side mirror of the tiling).
 int ctas_zpass_b2g(const ChainDev& c);

@@ -13,6 +13,8 @@
 //            test on alpha by the last CTA                    Updates/UpdateAlpha.c:12-253
 // Both fold their accumulators (PSum, SumEps, FstSum, QSum, AncestDist,
 // sumAlpha, sumlambda; output.c:654-707 UpdateSums) when the sweep collects.
+#include <algorithm>
+
 #include "st_device.cuh"
 #include "st_kernels.h"
 
@@ -327,6 +329,45 @@ locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int 
     for (int q = 0; q < K; q++) ch.FstSum[q] += ch.F[q];
   }
   if (errb) set_err(ch.err, errb);
+}
+
+// A new chain's start (src/Init.c:329-444): its descriptor and prefix, Q = 1/K,
+// the initial eps of its data set (computed once per data set and prior on the
+// host, kept on the device), F, alpha and lambda; the rest of the chain's arrays
+// are zeroed by memsets.  Written by a kernel rather than copied from host
+// memory, so creating a chain does not wait for the previous chain's initial
+// Z pass.
+__global__ void init_chain_kernel(ChainDev h, ChainDev* d_chain, int* d_prefix,
+                                  const double* __restrict__ eps0, size_t LA, size_t NK,
+                                  int arows, float q0, float lq0, double f0, double alpha0,
+                                  double lambda0) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  if (t == 0) {
+    *d_chain = h;
+    *d_prefix = 0;
+  }
+  for (size_t j = t; j < NK; j += stride) {
+    h.Q[j] = q0;
+    h.logQ[j] = lq0;
+  }
+  for (size_t j = t; j < LA; j += stride) h.eps[j] = eps0[j];
+  for (size_t j = t; j < (size_t)arows * h.K; j += stride) h.alpha[j] = alpha0;
+  if (t < (size_t)h.K) {
+    h.F[t] = f0;
+    h.lambda[t] = lambda0;
+  }
+}
+
+cudaError_t launch_init_chain(const ChainDev& h, ChainDev* d_chain, int* d_prefix,
+                              const double* eps0, int arows, float q0, float lq0, double f0,
+                              double alpha0, double lambda0, cudaStream_t s) {
+  const size_t LA = (size_t)h.L * h.A, NK = (size_t)h.N * h.K;
+  const size_t n = std::max(std::max(LA, NK), (size_t)arows * h.K);
+  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+  init_chain_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(h, d_chain, d_prefix, eps0, LA, NK, arows,
+                                                        q0, lq0, f0, alpha0, lambda0);
+  return cudaGetLastError();
 }
 
 int ctas_locus(const ChainDev& c, int block) { return (c.L * c.loc_tpl + block - 1) / block; }
