@@ -81,7 +81,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
   z.t2 = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * KT2 * 8);  // (t,t) pairs
   z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT * nw32 * 8);       // allele table
   z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * (nw32 / 32) * 4);   // per warp
-  z.inc = o; if (counts && KT <= 8) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * 8);
+  z.inc = o; if (counts && KT <= 12) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * (KT <= 8 ? 8 : 16));
   z.m = o;  if (counts) o = zalign16(o + (size_t)T * KT * 4);
   z.n = o;  if (counts) o = zalign16(o + (size_t)(2 * K + 1) * nw32 * 4);
   z.total = o;
@@ -172,7 +172,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   constexpr int NWM = (KT + 3) / 4;
   constexpr bool kUseP = (MODE == kZNormal || MODE == kZMetro || MODE == kZLike);
   constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
-  constexpr bool kLut = kCounts && KT <= 8;
+  constexpr bool kLut = kCounts && KT <= 12;
   constexpr bool kRegX = zregx(MODE, KT);
   ChainDev& ch = *za.chp;
   const uint32_t* grow = za.grow;
@@ -315,10 +315,18 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
             atomicAdd(&mycol[(ncnt ? 2 * z0 + (int)a0 : trash) * NW32], 1);
             atomicAdd(&mycol[(ncnt ? 2 * z1 + (int)a1 : trash) * NW32], 1);
             uint32_t s_lo, s_hi = 0;
-            if (kLut) {
+            [[maybe_unused]] uint32_t s_3 = 0;
+            if (kLut && KT <= 8) {
               const uint2 v = sInc[cnt ? z0 * (KT + 1) + z1 : KT * (KT + 1) + KT];
               s_lo = __reduce_add_sync(0xffffffffu, v.x);
               if (KT > 4) s_hi = __reduce_add_sync(0xffffffffu, v.y);
+            } else if (kLut) {
+              // K classes 9-12: three packed words per pair of copies
+              const uint4 v = reinterpret_cast<const uint4*>(sInc)[cnt ? z0 * (KT + 1) + z1
+                                                                       : KT * (KT + 1) + KT];
+              s_lo = __reduce_add_sync(0xffffffffu, v.x);
+              s_hi = __reduce_add_sync(0xffffffffu, v.y);
+              s_3 = __reduce_add_sync(0xffffffffu, v.z);
             } else {
               uint32_t mw[NWM];
 #pragma unroll
@@ -334,7 +342,9 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
 #pragma unroll
               for (int q = 0; q < NWM; q++) s_lo = my_word == q ? mw[q] : s_lo;
             }
-            const uint32_t s = kLut ? (my_word == 0 ? s_lo : s_hi) : s_lo;
+            uint32_t s = s_lo;
+            if constexpr (kLut && KT <= 8) s = my_word == 0 ? s_lo : s_hi;
+            else if constexpr (kLut) s = my_word == 0 ? s_lo : (my_word == 1 ? s_hi : s_3);
             const int f = (int)((s >> my_shift) & 127u);
             if (lane < K) atomicAdd(&sM[row * KT + lane], f);
           }
@@ -394,7 +404,7 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   constexpr int NWM = (KT + 3) / 4;
   constexpr bool kUseP = (MODE == kZNormal || MODE == kZMetro || MODE == kZLike);
   constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
-  constexpr bool kLut = kCounts && KT <= 8;
+  constexpr bool kLut = kCounts && KT <= 12;
 
   const int c = find_chain(prefix, nchains, blockIdx.x);
   ChainDev& ch = chains[c];
@@ -440,13 +450,15 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     for (int idx = threadIdx.x; idx < nT16 * KT; idx += NW32) sM[idx] = 0;
   if (kLut) {
     // packed one-hot increments of two copies: 7-bit field per population,
-    // four fields per 32-bit half; index KT = "no copy"
+    // four fields per 32-bit word; index KT = "no copy"
     for (int idx = threadIdx.x; idx < (KT + 1) * (KT + 1); idx += NW32) {
       const int za = idx / (KT + 1), zb = idx - za * (KT + 1);
-      uint64_t v = 0;
-      if (za < KT) v += 1ull << (7 * (za & 3) + 32 * (za >> 2));
-      if (zb < KT) v += 1ull << (7 * (zb & 3) + 32 * (zb >> 2));
-      sInc[idx] = make_uint2((uint32_t)v, (uint32_t)(v >> 32));
+      auto field = [&](int z, int q) -> uint32_t {
+        return (z < KT && (z >> 2) == q) ? (1u << (7 * (z & 3))) : 0u;
+      };
+      const uint32_t w0 = field(za, 0) + field(zb, 0), w1 = field(za, 1) + field(zb, 1);
+      if (KT <= 8) sInc[idx] = make_uint2(w0, w1);
+      else reinterpret_cast<uint4*>(sInc)[idx] = make_uint4(w0, w1, field(za, 2) + field(zb, 2), 0u);
     }
   }
   if (MODE == kZMetro)
