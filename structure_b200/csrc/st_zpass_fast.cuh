@@ -28,6 +28,11 @@ constexpr float kLikeTinyF = 1e-30f;
 // word holding a smaller product is recomputed exactly (word_like_exact).
 constexpr float kLikeFastMin = 1e-30f;
 
+// K classes 9-12 keep one (P[l][k][0], P[l][k][1]) pair per population and lane
+// and select each copy's allele per genotype: a third of the per-class table
+// (20 KB instead of 61 KB at K=10), so three CTAs fit on an SM instead of two.
+__host__ __device__ constexpr bool zsingles(int kt) { return kt >= 9 && kt <= 12; }
+
 // Deterministic block sum of one double per thread (fixed tree order).
 __device__ __forceinline__ double block_sum_d(double v, double* sred) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -79,7 +84,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
   size_t o = 0;
   z.q2 = o; if (useP) o = zalign16(o + (size_t)T * KT2 * 8);            // (q,q) pairs
   z.t2 = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * KT2 * 8);  // (t,t) pairs
-  z.x = o;  if (useP) o = zalign16(o + (size_t)3 * KT * nw32 * 8);       // allele table
+  z.x = o;  if (useP) o = zalign16(o + (size_t)(zsingles(KT) ? 1 : 3) * KT * nw32 * 8);
   z.ld = o; if (mode == kZMetro) o = zalign16(o + (size_t)T * (nw32 / 32) * 4);   // per warp
   z.inc = o; if (counts && KT <= 12) o = zalign16(o + (size_t)(KT + 1) * (KT + 1) * (KT <= 8 ? 8 : 16));
   z.m = o;  if (counts) o = zalign16(o + (size_t)T * KT * 4);
@@ -134,12 +139,17 @@ __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, cons
     if (g == 3u) continue;
     const float4* q4 = reinterpret_cast<const float4*>(sQ2 + (row_base + gi) * KT2);
     const float4* X4 = reinterpret_cast<const float4*>(Xlane) + g * (XP * NW32);
+    const uint32_t a0 = g >> 1, a1 = (g | (g >> 1)) & 1u;
     float2 C = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < KT2; k += 2) {
       const float4 v = q4[k >> 1];
       float4 xv;
-      if (k + 1 < KT) {
+      if (zsingles(KT)) {
+        const float2 p = Xlane[k * NW32];
+        const float2 pn = k + 1 < KT ? Xlane[(k + 1) * NW32] : make_float2(0.0f, 0.0f);
+        xv = make_float4(a0 ? p.y : p.x, a1 ? p.y : p.x, a0 ? pn.y : pn.x, a1 ? pn.y : pn.x);
+      } else if (k + 1 < KT) {
         xv = X4[(k >> 1) * NW32];
       } else {
         const float2 t = Xtail[g * NW32];
@@ -217,7 +227,19 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               const float4 v = q4[k >> 1];
               Q2[k] = make_float2(v.x, v.y);
               Q2[k + 1] = make_float2(v.z, v.w);
-              if (!kRegX) {
+              if (zsingles(KT)) {
+                // (P[a0][k], P[a1][k]) from the lane's pair; a missing genotype
+                // takes allele 1 and its terms are discarded below
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                  if (k + e < KT) {
+                    const float2 pv = Xlane[(k + e) * NW32];
+                    X[k + e] = make_float2(a0 ? pv.y : pv.x, a1 ? pv.y : pv.x);
+                  } else {
+                    X[k + e] = make_float2(0.0f, 0.0f);
+                  }
+                }
+              } else if (!kRegX) {
                 if (k + 1 < KT) {
                   const float4 xv = X4[(k >> 1) * NW32];
                   X[k] = make_float2(xv.x, xv.y);
@@ -505,7 +527,11 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
             p1r[kk < NP ? kk : 0] = p1[e];
           }
         }
-        if (k + 1 < KT) {
+        if (zsingles(KT)) {
+          float2* XSw = reinterpret_cast<float2*>(sX) + threadIdx.x;
+          XSw[k * NW32] = make_float2(p0[0], p1[0]);
+          if (k + 1 < KT) XSw[(k + 1) * NW32] = make_float2(p0[1], p1[1]);
+        } else if (k + 1 < KT) {
           X4w[(0 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
           X4w[(1 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
           X4w[(2 * XP + (k >> 1)) * NW32] = make_float4(p1[0], p1[0], p1[1], p1[1]);
@@ -520,7 +546,9 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
       for (int q = 0; q < 2 * K + 1; q++) mycol[q * NW32] = 0;   // row 2K: missing copies
     __syncwarp();
     const uint32_t* grow = ch.g2 + (size_t)(valid ? l : 0) * ch.wpr;
-    const float2* Xlane = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
+    const float2* Xlane =
+        zsingles(KT) ? reinterpret_cast<const float2*>(sX) + threadIdx.x
+                     : reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
     const float2* Xtail = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) +
                                                           3 * (KT / 2) * NW32) + threadIdx.x;
     {
