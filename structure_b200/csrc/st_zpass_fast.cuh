@@ -120,7 +120,7 @@ struct ZArgs {
   int* mycol;
   int i0, i1, nT16, l, K, L, lane, my_word, my_shift;
   uint32_t prep, key, stream;
-  bool valid, pfonly;
+  bool valid, pfonly, store_z;
 };
 
 // ln P(D) terms of one lane's 16 genotypes of a word in FP64 with the
@@ -173,7 +173,10 @@ __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, cons
 __host__ __device__ constexpr bool zregx(int mode, int kt) { return mode == kZMetro && kt <= 6; }
 __host__ __device__ constexpr int zregn(int mode, int kt) { return zregx(mode, kt) ? kt : 1; }
 
-template <int KT, int MODE, int W, bool LIKE, bool SZ>
+// EXT: the rare per-genotype features (a stored Z, PFROMPOPFLAGONLY counts),
+// tested at run time only in this instantiation, so the common one carries
+// neither their loads nor their branches.
+template <int KT, int MODE, int W, bool LIKE, bool EXT>
 __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, int& errb,
                                            const float (&p0r)[zregn(MODE, KT)],
                                            const float (&p1r)[zregn(MODE, KT)]) {
@@ -196,19 +199,25 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   int* mycol = za.mycol;
   const int i0 = za.i0, i1 = za.i1, nT16 = za.nT16, l = za.l, K = za.K, L = za.L;
   const int lane = za.lane, my_word = za.my_word, my_shift = za.my_shift;
+  [[maybe_unused]] const int moff = lane < K ? lane : lane - K + KT;
+  [[maybe_unused]] const bool second = lane >= K;
   const uint32_t prep = za.prep, key = za.key, stream = za.stream;
-  const bool valid = za.valid, pfonly = za.pfonly;
+  const bool valid = za.valid, pfonly = EXT && za.pfonly, store_z = EXT && za.store_z;
+    // Philox blocks of this lane's locus and sweep: b = individual pair.  i0 is
+    // a multiple of 16 (whole genotype words), so a word's first pair index is
+    // a multiple of 8 and pair j/2 of the word is that index ^ (j/2).
+    const PhiloxRun prun((uint32_t)l, prep, stream, key);
     for (int wi = 0; wi < (nT16 >> 4); wi++) {
       const uint32_t word = valid ? __ldg(grow + (i0 >> 4) + wi) : 0xFFFFFFFFu;
+      const uint32_t pw = prun.head ^ ((uint32_t)((i0 >> 1) + (wi << 3)) & 0xFFFFFFu);
       float wlike = 0.0f, wprod = 1.0f, wmin = 1.0f;
       float tr[MODE == kZMetro ? 16 : 1];   // Metropolis pass: this lane's term per row
 #pragma unroll
       for (int j = 0; j < 16; j += 2) {
         const int row0 = (wi << 4) + j;              // chunk-relative individual
-        const int ib = i0 + row0;
         U4 r4;
-        if (MODE == kZNormal || MODE == kZInit)
-          r4 = philox_s((uint32_t)l, (uint32_t)(ib >> 1), prep, stream, key);
+        if (MODE == kZNormal || MODE == kZInit) r4 = prun.block_r0(pw ^ (uint32_t)(j >> 1));
+        [[maybe_unused]] uint32_t pr_lo = 0, pr_hi = 0, pr_3 = 0;   // first row's reduced words
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int row = row0 + h;
@@ -332,7 +341,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
             bool cnt = !miss;
             if (MODE == kZRecount) cnt = cnt && z0 < K && z1 < K;
             bool ncnt = cnt;
-            if (pfonly) ncnt = ncnt && ch.popflags[i0 + row] == 1;
+            if (EXT && pfonly) ncnt = ncnt && ch.popflags[i0 + row] == 1;
             const int trash = 2 * K;
             atomicAdd(&mycol[(ncnt ? 2 * z0 + (int)a0 : trash) * NW32], 1);
             atomicAdd(&mycol[(ncnt ? 2 * z1 + (int)a1 : trash) * NW32], 1);
@@ -364,13 +373,35 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
 #pragma unroll
               for (int q = 0; q < NWM; q++) s_lo = my_word == q ? mw[q] : s_lo;
             }
-            uint32_t s = s_lo;
-            if constexpr (kLut && KT <= 8) s = my_word == 0 ? s_lo : s_hi;
-            else if constexpr (kLut) s = my_word == 0 ? s_lo : (my_word == 1 ? s_hi : s_3);
-            const int f = (int)((s >> my_shift) & 127u);
-            if (lane < K) atomicAdd(&sM[row * KT + lane], f);
+            if constexpr (kLut) {
+              // one shared atomic per pair of rows: lanes 0..K-1 add the first
+              // row's populations, lanes K..2K-1 the second's (my_word and
+              // my_shift name population lane mod K; moff its slot)
+              if (h == 0) {
+                pr_lo = s_lo;
+                pr_hi = s_hi;
+                pr_3 = s_3;
+              } else {
+                uint32_t s;
+                if constexpr (KT <= 4) {
+                  s = second ? s_lo : pr_lo;
+                } else if constexpr (KT <= 8) {
+                  const uint32_t a = my_word == 0 ? pr_lo : pr_hi, b = my_word == 0 ? s_lo : s_hi;
+                  s = second ? b : a;
+                } else {
+                  const uint32_t a = my_word == 0 ? pr_lo : (my_word == 1 ? pr_hi : pr_3);
+                  const uint32_t b = my_word == 0 ? s_lo : (my_word == 1 ? s_hi : s_3);
+                  s = second ? b : a;
+                }
+                const int f = (int)((s >> my_shift) & 127u);
+                if (lane < 2 * K) atomicAdd(&sM[(row - 1) * KT + moff], f);
+              }
+            } else {
+              const int f = (int)((s_lo >> my_shift) & 127u);
+              if (lane < K) atomicAdd(&sM[row * KT + lane], f);
+            }
           }
-          if (SZ && valid && i0 + row < i1) {
+          if (EXT && store_z && valid && i0 + row < i1) {
             const size_t zi = (size_t)(i0 + row) * 2 * L + l;
             ch.Z[zi] = miss ? kZMissing : (uint8_t)z0;
             ch.Z[zi + L] = miss ? kZMissing : (uint8_t)z1;
@@ -488,7 +519,11 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   __syncthreads();
 
   // lane k < K extracts population k's field from the reduced words
-  const int my_word = lane >> 2, my_shift = 7 * (lane & 3);
+  // (table classes: lanes K..2K-1 take population lane - K of the second row
+  // of a pair, stored at slot moff of the first row's)
+  const int mfield = (kLut && lane >= K) ? lane - K : lane;
+  const int my_word = mfield >> 2, my_shift = 7 * (mfield & 3);
+
 
   double like_acc = 0.0;
   int errb = 0;
@@ -554,12 +589,13 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
     {
       ZArgs za{&ch, grow, Xlane, Xtail, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
                K, L, lane,
-               my_word, my_shift, prep, key, stream, valid, pfonly};
+               my_word, my_shift, prep, key, stream, valid, pfonly, store_z};
+      const bool ext = store_z || pfonly;
       if (want_like) {
-        if (store_z) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb, p0r, p1r);
+        if (ext) zword_loop<KT, MODE, W, true, true>(za, like_acc, errb, p0r, p1r);
         else zword_loop<KT, MODE, W, true, false>(za, like_acc, errb, p0r, p1r);
       } else {
-        if (store_z) zword_loop<KT, MODE, W, false, true>(za, like_acc, errb, p0r, p1r);
+        if (ext) zword_loop<KT, MODE, W, false, true>(za, like_acc, errb, p0r, p1r);
         else zword_loop<KT, MODE, W, false, false>(za, like_acc, errb, p0r, p1r);
       }
     }
