@@ -33,6 +33,17 @@ constexpr float kLikeFastMin = 1e-30f;
 // (20 KB instead of 61 KB at K=10), so three CTAs fit on an SM instead of two.
 __host__ __device__ constexpr bool zsingles(int kt) { return kt >= 9 && kt <= 12; }
 
+// One 16-byte shared-memory load.  The Q rows are read by every lane of a warp
+// at once (a broadcast): as one 16-byte load that is one wavefront per two
+// populations, where the code generator otherwise splits it into 8-byte loads.
+__device__ __forceinline__ float4 lds_f4(const float4* p) {
+  float4 v;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+
 // Deterministic block sum of one double per thread (fixed tree order).
 __device__ __forceinline__ double block_sum_d(double v, double* sred) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -110,8 +121,7 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
 struct ZArgs {
   ChainDev* chp;
   const uint32_t* grow;
-  const float2* Xlane;   // this lane's allele-table column (pairs of pairs)
-  const float2* Xtail;   // odd K classes: this lane's last pair
+  const float2* Xlane;   // this lane's allele-table column: one pair per class and population
   const float2* sQ2;
   const float2* sT2;
   float* sLD;     // this warp's Metropolis log-ratio partials, one per row
@@ -129,16 +139,15 @@ struct ZArgs {
 // a term below kLikeFastMin.
 template <int KT, int W>
 __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, const float2* Xlane,
-                                               const float2* Xtail, const float2* sQ2) {
+                                               const float2* sQ2) {
   constexpr int NW32 = 32 * W;
   constexpr int KT2 = (KT + 1) & ~1;
-  constexpr int XP = KT / 2;
   double s = 0.0;
   for (int gi = 0; gi < 16; gi++) {
     const uint32_t g = (word >> (2 * gi)) & 3u;
     if (g == 3u) continue;
     const float4* q4 = reinterpret_cast<const float4*>(sQ2 + (row_base + gi) * KT2);
-    const float4* X4 = reinterpret_cast<const float4*>(Xlane) + g * (XP * NW32);
+    const float2* X2 = Xlane + g * (KT * NW32);
     const uint32_t a0 = g >> 1, a1 = (g | (g >> 1)) & 1u;
     float2 C = make_float2(0.0f, 0.0f);
 #pragma unroll
@@ -149,11 +158,10 @@ __device__ __noinline__ double word_like_exact(uint32_t word, int row_base, cons
         const float2 p = Xlane[k * NW32];
         const float2 pn = k + 1 < KT ? Xlane[(k + 1) * NW32] : make_float2(0.0f, 0.0f);
         xv = make_float4(a0 ? p.y : p.x, a1 ? p.y : p.x, a0 ? pn.y : pn.x, a1 ? pn.y : pn.x);
-      } else if (k + 1 < KT) {
-        xv = X4[(k >> 1) * NW32];
       } else {
-        const float2 t = Xtail[g * NW32];
-        xv = make_float4(t.x, t.y, 0.0f, 0.0f);
+        const float2 t = X2[k * NW32];
+        const float2 tn = k + 1 < KT ? X2[(k + 1) * NW32] : make_float2(0.0f, 0.0f);
+        xv = make_float4(t.x, t.y, tn.x, tn.y);
       }
       if (k == 0) C = mul2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y));
       else C = fma2_rn(make_float2(v.x, v.y), make_float2(xv.x, xv.y), C);
@@ -190,7 +198,6 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   ChainDev& ch = *za.chp;
   const uint32_t* grow = za.grow;
   const float2* Xlane = za.Xlane;
-  const float2* Xtail = za.Xtail;
   const float2* sQ2 = za.sQ2;
   const float2* sT2 = za.sT2;
   float* sLD = za.sLD;
@@ -228,12 +235,12 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
           if (kUseP) {
             const float4* q4 = reinterpret_cast<const float4*>(sQ2 + row * KT2);
             const uint32_t cls = miss ? 0u : g;
-            const float4* X4 = reinterpret_cast<const float4*>(Xlane) + cls * ((KT / 2) * NW32);
+            const float2* X2 = Xlane + cls * (KT * NW32);
             float2 Cs[KT];
             float2 Q2[KT2], X[KT2];
 #pragma unroll
             for (int k = 0; k < KT2; k += 2) {
-              const float4 v = q4[k >> 1];
+              const float4 v = lds_f4(q4 + (k >> 1));
               Q2[k] = make_float2(v.x, v.y);
               Q2[k + 1] = make_float2(v.z, v.w);
               if (zsingles(KT)) {
@@ -249,14 +256,9 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
                   }
                 }
               } else if (!kRegX) {
-                if (k + 1 < KT) {
-                  const float4 xv = X4[(k >> 1) * NW32];
-                  X[k] = make_float2(xv.x, xv.y);
-                  X[k + 1] = make_float2(xv.z, xv.w);
-                } else {   // odd K class: the last pair from its own 8-byte table
-                  X[k] = Xtail[cls * NW32];
-                  X[k + 1] = make_float2(0.0f, 0.0f);
-                }
+                // 8-byte pairs, lane-minor: a warp's load is two wavefronts
+                X[k] = X2[k * NW32];
+                X[k + 1] = k + 1 < KT ? X2[(k + 1) * NW32] : make_float2(0.0f, 0.0f);
               }
             }
             if (kRegX) {
@@ -296,7 +298,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
               float2 T2[KT2];
 #pragma unroll
               for (int k = 0; k < KT2; k += 2) {
-                const float4 v = t4[k >> 1];
+                const float4 v = lds_f4(t4 + (k >> 1));
                 T2[k] = make_float2(v.x, v.y);
                 T2[k + 1] = make_float2(v.z, v.w);
               }
@@ -439,7 +441,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
         double wl = (double)wlike;
         if (__any_sync(0xffffffffu, !(wmin > kLikeFastMin))) {   // once per word, rare
           if (!(wmin > kLikeFastMin))
-            wl = word_like_exact<KT, W>(word, wi << 4, Xlane, Xtail, sQ2);
+            wl = word_like_exact<KT, W>(word, wi << 4, Xlane, sQ2);
         }
         like_acc += wl;
       }
@@ -541,14 +543,12 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
 #pragma unroll
     for (int k = 0; k < NP; k++) p0r[k] = p1r[k] = 0.0f;
     if (kUseP) {
-      // allele table of this lane's locus, per class g in {0/0, 0/1, 1/1}:
-      // float4 (P[a0][k], P[a1][k], P[a0][k+1], P[a1][k+1]) per pair of k; for
-      // odd K classes the last (P[a0][k], P[a1][k]) goes to a float2 table, so
-      // the warp reads it in two shared-memory wavefronts instead of four
-      constexpr int XP = KT / 2;
-      float4* X4w = reinterpret_cast<float4*>(sX) + threadIdx.x;
-      float2* XTw = reinterpret_cast<float2*>(reinterpret_cast<float4*>(sX) + 3 * XP * NW32) +
-                    threadIdx.x;
+      // allele table of this lane's locus: for class g in {0/0, 0/1, 1/1} and
+      // population k the pair (P[a0][k], P[a1][k]) at [g][k][lane], 8 bytes per
+      // lane and lane-minor, so a warp reads one population's pairs in two
+      // shared-memory wavefronts (pairs of pairs in 16-byte slots took four
+      // per half once the loads were split into 8-byte ones)
+      float2* X2w = reinterpret_cast<float2*>(sX) + threadIdx.x;
 #pragma unroll
       for (int k = 0; k < KT2; k += 2) {
         float p0[2], p1[2];
@@ -566,14 +566,15 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
           float2* XSw = reinterpret_cast<float2*>(sX) + threadIdx.x;
           XSw[k * NW32] = make_float2(p0[0], p1[0]);
           if (k + 1 < KT) XSw[(k + 1) * NW32] = make_float2(p0[1], p1[1]);
-        } else if (k + 1 < KT) {
-          X4w[(0 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p0[0], p0[1], p0[1]);
-          X4w[(1 * XP + (k >> 1)) * NW32] = make_float4(p0[0], p1[0], p0[1], p1[1]);
-          X4w[(2 * XP + (k >> 1)) * NW32] = make_float4(p1[0], p1[0], p1[1], p1[1]);
         } else {
-          XTw[0 * NW32] = make_float2(p0[0], p0[0]);
-          XTw[1 * NW32] = make_float2(p0[0], p1[0]);
-          XTw[2 * NW32] = make_float2(p1[0], p1[0]);
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            if (k + e < KT) {
+              X2w[(0 * KT + k + e) * NW32] = make_float2(p0[e], p0[e]);
+              X2w[(1 * KT + k + e) * NW32] = make_float2(p0[e], p1[e]);
+              X2w[(2 * KT + k + e) * NW32] = make_float2(p1[e], p1[e]);
+            }
+          }
         }
       }
     }
@@ -581,13 +582,9 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
       for (int q = 0; q < 2 * K + 1; q++) mycol[q * NW32] = 0;   // row 2K: missing copies
     __syncwarp();
     const uint32_t* grow = ch.g2 + (size_t)(valid ? l : 0) * ch.wpr;
-    const float2* Xlane =
-        zsingles(KT) ? reinterpret_cast<const float2*>(sX) + threadIdx.x
-                     : reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) + threadIdx.x);
-    const float2* Xtail = reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(sX) +
-                                                          3 * (KT / 2) * NW32) + threadIdx.x;
+    const float2* Xlane = reinterpret_cast<const float2*>(sX) + threadIdx.x;
     {
-      ZArgs za{&ch, grow, Xlane, Xtail, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
+      ZArgs za{&ch, grow, Xlane, sQ2, sT2, sLD + warp * nT16, sInc, sM, mycol, i0, i1, nT16, l,
                K, L, lane,
                my_word, my_shift, prep, key, stream, valid, pfonly, store_z};
       const bool ext = store_z || pfonly;
