@@ -196,17 +196,23 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def read_traffic():
-    """DRAM bytes per Z-pass launch from the committed ncu summary, if any."""
+def read_profile_figure(key):
+    """A figure of the committed ncu summary of the Z pass (a line "key: value"),
+    if any."""
     path = os.path.join(ROOT, "profiles", "zpass_b2g_snp2000x50000_k5_batch20.txt")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
+                if line.startswith(key + ":"):
                     return float(line.split(":")[1])
     except Exception:
         pass
     return None
+
+
+def read_traffic():
+    """DRAM bytes per Z-pass launch from the committed ncu summary, if any."""
+    return read_profile_figure("dram_bytes_per_launch")
 
 
 # ---------------------------------------------------------------------------
@@ -361,8 +367,8 @@ def run_ours(args):
     # issue roofline of the same kernel, the limit it actually meets: warp
     # instructions per 32 genotypes from the ncu capture of a collecting launch
     # (profiles/zpass_b2g_snp2000x50000_k5_batch20.txt), as the timed launches are
-    inst_per_32 = 120.0
-    issue_achieved = B * N * L / 32 * inst_per_32 / (zavg / 1e3) / 1e12
+    inst_per_32 = read_profile_figure("inst_per_32_genotypes")
+    issue_achieved = (B * N * L / 32 * inst_per_32 / (zavg / 1e3) / 1e12) if inst_per_32 else None
     issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e12
     traffic = read_traffic()
     total_ms = sum(v[0] for v in prof.values())
@@ -407,9 +413,10 @@ def run_ours(args):
                          "ops_per_copy": ops_per_copy,
                          "note": "2K+2 FP32 + ~10 int (Philox/4) + 0.5 log per allele copy; "
                                  "peak = 148 SM x 128 lanes x median SM clock"},
-        "roofline_issue": {"bound": "issue", "achieved": round(issue_achieved, 4),
+        "roofline_issue": {"bound": "issue",
+                           "achieved": round(issue_achieved, 4) if issue_achieved else None,
                            "peak": round(issue_peak, 4), "unit": "T warp-inst/s",
-                           "frac": round(issue_achieved / issue_peak, 4),
+                           "frac": round(issue_achieved / issue_peak, 4) if issue_achieved else None,
                            "inst_per_32_genotypes": inst_per_32,
                            "note": "instructions from an ncu capture of a collecting "
                                    "launch (ln P(D) terms on, as in the timed sweeps); peak "

@@ -281,9 +281,9 @@ void choose_tile(const st_model* m, int N, int L, int K, int* T, int* W, int* R)
   if (t > np) t = np;
   if (m->tile_t <= 0) {
     // three CTAs per SM (72 KB each) if a tile of >= 128 individuals fits,
-    // else two (112 KB each; 226 KB with the per-CTA reserve): the per-lane
-    // allele table of K classes 9-12 alone takes 61 KB, and small tiles
-    // rebuild it for every 32 individuals
+    // else two (112 KB each; 226 KB with the per-CTA reserve) rather than
+    // tiles so small that the per-lane allele table is rebuilt every few
+    // rows (the wide classes' tables and Q rows take the most)
     auto fits = [&](int tt, size_t b) { return zpass_smem_all(KT, K, tt, w) <= b; };
     int t3 = t;
     while (t3 > 128 && !fits(t3, 72 * 1024)) t3 -= 16;
