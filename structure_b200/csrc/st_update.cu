@@ -43,7 +43,7 @@ __device__ __forceinline__ void warp_slot_sums(double v, int G, double* s, int n
 // ---------------------------------------------------------------------------
 constexpr int kStageKA = 16;   // populations x alleles staged per locus (P stage)
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 locus_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix, int nchains,
              int stages) {
   __shared__ double sF[8 * kMaxPops];

@@ -232,3 +232,39 @@ def test_packed_upload_counts_match_int32_upload(ctx, N):
     np.testing.assert_allclose(ea[two].sum(1), 1.0, rtol=1e-12)
     for x in (ca, cb, a, b):
         x.close()
+
+
+@pytest.mark.parametrize("layout", [api.LAYOUT_B2G, api.LAYOUT_U8])
+@pytest.mark.parametrize("K,store_z", [(3, 1), (5, 0), (10, 1), (13, 0)])
+def test_pfrompopflagonly_counts(orc, layout, K, store_z):
+    """PFROMPOPFLAGONLY (src/Updates/UpdateP.c GetNumFromPops): only individuals
+    whose POPFLAG is 1 add to the allele counts n; every individual adds to the
+    ancestry counts m.  One Z pass on a fixed state against the oracle's Z and
+    its counts with the same flags, with and without the stored Z."""
+    N, L = 203, 517
+    geno, na = _snp(N, L, K, seed=11 + K)
+    rng = np.random.default_rng(7 * K + store_z)
+    popflags = (rng.random(N) < 0.4).astype(np.int32)
+    ctx = api.Context(0)
+    d = api.Data(ctx, na, geno=geno, layout=layout, popflags=popflags)
+    m = api.model_defaults(maxpops=K, burnin=2, numreps=6, freqscorr=0, metrofreq=3,
+                           store_z=store_z, pfrompopflagonly=1)
+    c = api.Chain(ctx, d, m, SEED)
+    Q, P = _rand_state(np.random.default_rng(N + L + K), N, L, K, na)
+    c.set(api.F_Q, Q)
+    c.set(api.F_P, P)
+    rep = 4
+    c.set(api.F_REP, np.array([rep], np.int32))
+    c.UpdateZ()
+    assert c.sync() == 0
+    zo = orc.zupdate_f32(geno, Q, P, SEED, rep)
+    if store_z:
+        assert (_z(c) == zo).all()
+    n_o, m_o = orc.counts(geno, zo, K, c.A, popflags=popflags, pfrompopflagonly=1)
+    n_all, _ = orc.counts(geno, zo, K, c.A)
+    assert n_o.sum() < n_all.sum()          # the flags leave some copies out of n
+    assert (c.get(api.F_N) == n_o).all()
+    assert (c.get(api.F_M) == m_o).all()
+    c.close()
+    d.close()
+    ctx.close()
