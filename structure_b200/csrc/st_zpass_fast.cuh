@@ -195,6 +195,8 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
   constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
   constexpr bool kLut = kCounts && KT <= 12;
   constexpr bool kRegX = zregx(MODE, KT);
+  constexpr int kHalves = (zsingles(KT) && MODE != kZMetro) ? 2 : 1;
+  constexpr int kJN = 16 / kHalves;   // genotypes of a word per unrolled pass
   ChainDev& ch = *za.chp;
   const uint32_t* grow = za.grow;
   const float2* Xlane = za.Xlane;
@@ -219,16 +221,23 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
       const uint32_t pw = prun.head ^ ((uint32_t)((i0 >> 1) + (wi << 3)) & 0xFFFFFFu);
       float wlike = 0.0f, wprod = 1.0f, wmin = 1.0f;
       float tr[MODE == kZMetro ? 16 : 1];   // Metropolis pass: this lane's term per row
+      // the widest table classes walk a word in two halves of 8 genotypes, so
+      // the unrolled loop body stays within the instruction cache
+#pragma unroll 1
+      for (int hb = 0; hb < kHalves; hb++) {
+      const uint32_t hword = kHalves == 1 ? word : (word >> (16 * hb));
+      const uint32_t phw = kHalves == 1 ? pw : (pw ^ (uint32_t)(hb << 2));
+      const int rbase = (wi << 4) + hb * kJN;
 #pragma unroll
-      for (int j = 0; j < 16; j += 2) {
-        const int row0 = (wi << 4) + j;              // chunk-relative individual
+      for (int j = 0; j < kJN; j += 2) {
+        const int row0 = rbase + j;              // chunk-relative individual
         U4 r4;
-        if (MODE == kZNormal || MODE == kZInit) r4 = prun.block_r0(pw ^ (uint32_t)(j >> 1));
+        if (MODE == kZNormal || MODE == kZInit) r4 = prun.block_r0(phw ^ (uint32_t)(j >> 1));
         [[maybe_unused]] uint32_t pr_lo = 0, pr_hi = 0, pr_3 = 0;   // first row's reduced words
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int row = row0 + h;
-          const uint32_t g = (word >> (2 * (j + h))) & 3u;
+          const uint32_t g = (hword >> (2 * (j + h))) & 3u;
           const bool miss = (g == 3u);
           const uint32_t a0 = g >> 1, a1 = (g | (g >> 1)) & 1u;
           int z0 = 0, z1 = 0;
@@ -410,6 +419,7 @@ __device__ __forceinline__ void zword_loop(const ZArgs& za, double& like_acc, in
           }
         }
       }
+      }   // halves
       if constexpr (MODE == kZMetro) {
         // the word's 16 row sums over the warp's 32 loci by a transposed
         // butterfly: at the exchange across lane bit b a lane keeps the half
