@@ -814,13 +814,14 @@ def measure_config4(steps, warmup, with_cpu=True, data=None):
     return out
 
 
-def measure_config5(steps, warmup, with_cpu=True):
+def measure_config5(steps, warmup, with_cpu=True, loci=500000):
     """Config 5: N=10,000, L=500,000 (2-bit packed, 1.25 GB), 2% missing, K=10 F
     model with F_k ~ U[0.01, 0.3], POPALPHAS=1, Q ~ Dir(0.1); 8 replicate chains
-    batched on one GPU under the context's HBM admission budget."""
+    batched on one GPU under the context's HBM admission budget.  `loci` < 500,000
+    runs the same model on fewer loci (a shape small enough for a profiler capture)."""
     import torch
     from structure_b200 import api, synth
-    N, L, K, B = 10000, 500000, 10, 8
+    N, L, K, B = 10000, int(loci), 10, 8
     rng = np.random.default_rng(synth.DATA_SEED_BASE + 5)
     F = rng.uniform(0.01, 0.3, K)
     d = synth.snp_fmodel_device(N, L, K, F, 0.1, 0.02, synth.DATA_SEED_BASE + 5)
@@ -861,7 +862,7 @@ def measure_config5(steps, warmup, with_cpu=True):
     copies = _observed_copies(d["packed"], N)
     value = B * steps / (ms / 1e3)
     plain = B * 10 / (pms / 1e3)
-    out = {"workload": "config 5: N=10000 L=500000 K=10 F model, POPALPHAS=1, 8 chains batched",
+    out = {"workload": f"config 5: N=10000 L={L} K=10 F model, POPALPHAS=1, 8 chains batched",
            "value": round(value, 3), "unit": METRIC, "steps": steps, "warmup": warmup,
            "ms_per_step": round(ms / steps, 3), "z_updates_per_s": round(value * copies, 1),
            "plain": {"value": round(plain, 3), "unit": METRIC,
@@ -889,7 +890,7 @@ def measure_config5(steps, warmup, with_cpu=True):
         out["cpu_baseline"] = {"value": round(1.0 / (dt * L / sl), 6), "unit": METRIC,
                                "cores": 1, "kind": "reference",
                                "sample": "sweep 1 of one reference chain on a 1,000-locus slice "
-                                         "(N=10,000, K=10), scaled by 500,000/1,000 loci",
+                                         f"(N=10,000, K=10), scaled by {L:,}/1,000 loci",
                                "cpu_model": cpu_model()}
     return out
 
@@ -910,7 +911,8 @@ def run_grad(args):
 
 
 def run_scale(args):
-    _print_workload("scale", measure_config5(args.steps, args.warmup, not args.no_cpu_baseline),
+    _print_workload("scale", measure_config5(args.steps, args.warmup, not args.no_cpu_baseline,
+                                             args.scale_loci),
                     args.steps, args.warmup)
 
 
@@ -997,6 +999,9 @@ def main():
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the brief measurements of configs 1, 3, 4 and 5 that the "
                          "default line carries under other_configs")
+    ap.add_argument("--scale-loci", type=int, default=500000,
+                    help="loci of the scale workload (config 5 has 500,000; fewer for a "
+                         "profiler capture of the same model)")
     ap.add_argument("--workload", default="snp",
                     choices=["snp", "small", "grad", "mala", "scale", "uneven"],
                     help="snp: the headline (default); small: config 1 whole run; grad: "

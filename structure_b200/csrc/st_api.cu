@@ -88,6 +88,7 @@ struct ZGroup {
   int KT = 0, W = 8;
   size_t zsmem = 0;
   int tz = 0;              // CTAs of the slice
+  bool same = false;       // one data set and tile for the whole slice (kZfInterleave)
 };
 
 struct st_batch {
@@ -1617,6 +1618,16 @@ static int batch_layout(st_batch* b, bool keep_groups) {
     b->pi[j] = b->ti;
     b->ti += ctas_ind(b->table[j], kBlockInd);
   }
+  for (ZGroup& g : b->zg) {
+    const ChainDev& h0 = b->table[g.first];
+    g.same = g.n > 1;
+    for (int j = g.first + 1; j < g.first + g.n; j++) {
+      const ChainDev& h = b->table[j];
+      g.same = g.same && h.g2 == h0.g2 && h.N == h0.N && h.L == h0.L && h.wpr == h0.wpr &&
+               h.tileT == h0.tileT && h.tileR == h0.tileR && h.nchunks == h0.nchunks &&
+               h.ngroups == h0.ngroups;
+    }
+  }
   // locus kernel: chains whose CTAs take longest first (longest-processing-
   // time order), so a batch of uneven K does not end on a tail of its slowest
   // chain's CTAs; a CTA's time is about its lanes' serial gamma draws
@@ -1850,7 +1861,8 @@ extern "C" int st_batch_autotune(st_batch* b, int reps) {
           cudaMemsetAsync(h.mpart, 0, (size_t)h.N * h.K * 4, s);
         }
         cudaEventRecord(e0, s);
-        cudaError_t e = launch_zpass_b2g(lg, g.KT, g.W, kZNormal, 0, g.zsmem);
+        cudaError_t e = launch_zpass_b2g(lg, g.KT, g.W, kZNormal, g.same ? kZfInterleave : 0,
+                                         g.zsmem);
         cudaEventRecord(e1, s);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) rc = cuda_check(ctx, e, "autotune");
@@ -1922,7 +1934,8 @@ static int enqueue_batch_sweep(st_batch* b, bool metro) {
       cudaStream_t gs = fork ? b->aux[gi] : s;
       if (fork) ST_CUDA(ctx, cudaStreamWaitEvent(gs, b->ev_fork, 0));
       LaunchSet lg{b->d_table + g.first, b->d_pz + g.first, g.n, g.tz, gs};
-      ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags, g.zsmem));
+      ST_CUDA(ctx, launch_zpass_b2g(lg, g.KT, g.W, mode, flags | (g.same ? kZfInterleave : 0),
+                                    g.zsmem));
       if (fork) ST_CUDA(ctx, cudaEventRecord(b->ev_join[gi], gs));
     }
     if (fork)

@@ -25,7 +25,11 @@ enum : int {
   kZfCollect = 0x8,        // fold ln P(D) into sumlikes/sumsqlikes when collecting
   kZfAdvance = 0x10,       // bump the device sweep counter at the end
   kZfF64 = 0x20,           // generic path: FP64 arithmetic (reference bit-parity)
-  kZfInjected = 0x40       // generic path: uniforms from the injected array
+  kZfInjected = 0x40,      // generic path: uniforms from the injected array
+  kZfInterleave = 0x80     // fast path: the launch's chains share one data set and
+                           // tile, and block b runs tile b / nchains of chain
+                           // b % nchains, so the chains' CTAs over the same loci run
+                           // together and read the genotype words once from DRAM
 };
 
 // Locus-kernel stages.

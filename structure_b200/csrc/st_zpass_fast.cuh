@@ -471,9 +471,15 @@ zpass_b2g_kernel(ChainDev* __restrict__ chains, const int* __restrict__ prefix,
   constexpr bool kCounts = (MODE == kZNormal || MODE == kZInit || MODE == kZRecount);
   constexpr bool kLut = kCounts && KT <= 12;
 
-  const int c = find_chain(prefix, nchains, blockIdx.x);
+  int c, tile;
+  if (flags & kZfInterleave) {   // chains of one data set and tile, interleaved
+    c = (int)blockIdx.x % nchains;
+    tile = (int)blockIdx.x / nchains;
+  } else {
+    c = find_chain(prefix, nchains, blockIdx.x);
+    tile = blockIdx.x - prefix[c];
+  }
   ChainDev& ch = chains[c];
-  const int tile = blockIdx.x - prefix[c];
   const int T = ch.tileT, R = ch.tileR;
   const int ichunk = tile % ch.nchunks, grp = tile / ch.nchunks;
   const int N = ch.N, L = ch.L, A = ch.A, K = ch.K;
