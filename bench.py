@@ -404,7 +404,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
                      "peak_source": peak_kind,
-                     "kernel": "zpass_b2g_kernel<8,kZNormal> (batched, 20 chains)",
+                     "kernel": f"zpass_b2g_kernel<K class {api.fast_class(K)}, Normal, 8 warps> "
+                               f"(batched, {B} chains)",
                      "avg_launch_ms": round(zavg, 4),
                      "algorithmic_bytes_per_launch": int(alg_bytes)},
         "roofline_alu": {"bound": "alu", "achieved": round(alu_achieved, 3),
