@@ -52,9 +52,9 @@ def test_noalloc_matches_chain_update_z_on_two_calls_in_a_row(orc, K, with_like)
     """Two calls back to back on one stream, against the chain API's results
     on the same state and against the oracle (Z drawn by the oracle from the
     same Q, P and stream, then counted; ln P(D) of the same Q and P).  K=2 and
-    K=20 are even K classes (20 with two-warp CTAs), 5 and 9 odd ones with the
-    tail table; the K=20 case passes no ln P(D) output, which skips the
-    last-CTA reduction."""
+    5 read the per-class allele table, 9 the one-pair-per-population table and
+    its two-half word loop, 20 the two-warp CTAs of the wide classes; the K=20
+    case passes no ln P(D) output, which skips the last-CTA reduction."""
     import torch
 
     N, L = 700, 2600
