@@ -153,3 +153,20 @@ def test_bench_reference_arm_line(ref):
     assert d["config"]["workload"].startswith("snp-fmodel N=2000 L=50000 K=5")
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_bench_reads_the_committed_z_pass_profile():
+    """The bench's roofline keys take the Z pass's DRAM bytes per launch and its
+    warp instructions per 32 genotypes from the committed ncu summary; both
+    lines must be there and plausible (traffic at least the 25 MB genotype
+    array, fewer than 200 instructions per 32 genotypes)."""
+    import importlib.util
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    traffic = bench.read_traffic()
+    inst = bench.read_profile_figure("inst_per_32_genotypes")
+    assert traffic is not None and traffic >= 25e6
+    assert inst is not None and 32 < inst < 200
+    assert bench.read_profile_figure("no_such_figure") is None
