@@ -116,8 +116,9 @@ __host__ __device__ inline ZLayout zlayout(int KT, int K, int T, int nw32, int m
 // so z is the reference's "first k with r <= cumsum_k" on FP32 weights.
 // The genotype loop of one lane (one locus) over the chunk's individuals,
 // specialised on the likelihood and Z-store flags so no per-genotype branch
-// tests them; the 16 genotypes of a word are fully unrolled so every shift and
-// shared-memory offset is an immediate.
+// tests them; the 16 genotypes of a word are fully unrolled (8 at a time for K
+// classes 9-12, whose longer body would not fit the instruction cache) so every
+// shift and shared-memory offset is an immediate.
 struct ZArgs {
   ChainDev* chp;
   const uint32_t* grow;
